@@ -1,0 +1,141 @@
+"""CPU oracle loader -- TEST INFRASTRUCTURE, not product code.
+
+Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s cpu_baseline /
+reference arm may import this module, and only as the checker.  It wraps
+``oracle/_build/liboracle.so`` (built from oracle/*.c by oracle/Makefile):
+
+* ``dt(points)``            exact Delaunay triangulation (oracle/dt.c), the
+                            output contract of gpudtComputeDT (gpudt/gpudt.h:131)
+* ``alpha(points, v, n)``   alpha spectrum + intervals (oracle/alpha.c), the
+                            output of Alpha_Shapes_2D::computeAlphaShapes
+                            (gpudt/AlphaShape/Alpha_Shapes_2D.cu:206-727)
+* exact predicates for cross-checks.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class _AlphaOut(ctypes.Structure):
+    _fields_ = [
+        ("nspec", ctypes.c_int),
+        ("spectrum", _dp),
+        ("spectrum_ref", _dp),
+        ("tri_ro", _ip),
+        ("edge", _ip),
+        ("point", _ip),
+        ("exact_compares", ctypes.c_longlong),
+        ("exact_ties", ctypes.c_longlong),
+    ]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        L.oracle_dt.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip]
+        L.oracle_dt.restype = ctypes.c_int
+        L.oracle_orient2d.argtypes = [_dp, _dp, _dp]
+        L.oracle_incircle.argtypes = [_dp, _dp, _dp, _dp]
+        L.oracle_exact_counts.argtypes = [ctypes.c_int]
+        L.oracle_exact_counts.restype = ctypes.c_longlong
+        L.oracle_alpha_count_edges.argtypes = [ctypes.c_int, _ip, _ip]
+        L.oracle_alpha.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, ctypes.POINTER(_AlphaOut)]
+        L.oracle_compare_rho.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp]
+        L.oracle_is_attached.argtypes = [_dp, _dp, _dp]
+        L.oracle_rho_rounded.argtypes = [ctypes.c_int, _dp]
+        L.oracle_rho_rounded.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def dt(points):
+    """Exact DT.  Returns (vtx[T,3] int32, nbr[T,3] int32, n_distinct)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    n = pts.shape[0]
+    cap = max(2 * n, 8)
+    vtx = np.empty((cap, 3), dtype=np.int32)
+    nbr = np.empty((cap, 3), dtype=np.int32)
+    kept = np.zeros(1, dtype=np.int32)
+    nt = lib().oracle_dt(n, _d(pts), cap, _i(vtx), _i(nbr), _i(kept))
+    if nt < 0:
+        raise RuntimeError("oracle_dt failed with status %d" % nt)
+    return vtx[:nt].copy(), nbr[:nt].copy(), int(kept[0])
+
+
+def alpha(points, vtx, nbr):
+    """Alpha spectrum and intervals of triangulation (vtx, nbr)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    vtx = np.ascontiguousarray(vtx, dtype=np.int32)
+    nbr = np.ascontiguousarray(nbr, dtype=np.int32)
+    n, nt = pts.shape[0], vtx.shape[0]
+    L = lib()
+    ne = L.oracle_alpha_count_edges(nt, _i(vtx), _i(nbr))
+    spec = np.zeros(1 + nt + ne, dtype=np.float64)
+    spec_ref = np.zeros(1 + nt + ne, dtype=np.float64)
+    tri_ro = np.zeros(nt, dtype=np.int32)
+    edge = np.zeros((ne, 7), dtype=np.int32)
+    point = np.zeros((n, 2), dtype=np.int32)
+    out = _AlphaOut(0, _d(spec), _d(spec_ref), _i(tri_ro), _i(edge), _i(point), 0, 0)
+    st = L.oracle_alpha(n, _d(pts), nt, _i(vtx), _i(nbr), ctypes.byref(out))
+    if st != 0:
+        raise RuntimeError("oracle_alpha failed with status %d" % st)
+    k = out.nspec
+    return {
+        "spectrum": spec[:k].copy(),
+        "spectrum_ref": spec_ref[:k].copy(),
+        "tri_ro": tri_ro,
+        "edge": edge,  # p1, p2, ro, nu_min, nu_max, tIndex, vOpp
+        "point": point,
+        "exact_compares": out.exact_compares,
+        "exact_ties": out.exact_ties,
+    }
+
+
+def orient2d(a, b, c):
+    a, b, c = (np.asarray(x, dtype=np.float64) for x in (a, b, c))
+    return lib().oracle_orient2d(_d(a), _d(b), _d(c))
+
+
+def incircle(a, b, c, d):
+    a, b, c, d = (np.asarray(x, dtype=np.float64) for x in (a, b, c, d))
+    return lib().oracle_incircle(_d(a), _d(b), _d(c), _d(d))
+
+
+def compare_rho(kind1, p1, kind2, p2):
+    p1 = np.ascontiguousarray(p1, dtype=np.float64).ravel()
+    p2 = np.ascontiguousarray(p2, dtype=np.float64).ravel()
+    return lib().oracle_compare_rho(kind1, _d(p1), kind2, _d(p2))
+
+
+def is_attached(i, j, k):
+    i, j, k = (np.asarray(x, dtype=np.float64) for x in (i, j, k))
+    return lib().oracle_is_attached(_d(i), _d(j), _d(k))
+
+
+def rho_rounded(kind, p):
+    p = np.ascontiguousarray(p, dtype=np.float64).ravel()
+    return lib().oracle_rho_rounded(kind, _d(p))
