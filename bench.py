@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark: DT + alpha spectrum throughput (Mpoints/s) at 4M uniform points.
+
+Workload c2: 4,194,304 points i.i.d. uniform in [0,1]^2 (seeded splitmix64,
+FP64), discrete Voronoi texture 8192^2.  One step = one full Delaunay
+triangulation + alpha spectrum with per-simplex intervals.
+
+  value  device-resident: points already in HBM, results left in HBM
+         (galphaRunDevice), timed with CUDA events on the engine's stream.
+  e2e    the same through the public host API (galphaTriangulate +
+         galphaComputeResident): pinned host points in, triangles and all alpha
+         arrays back to host memory, inside the timed region.
+
+Between timed steps a 512 MiB buffer is written (L2 flush); the step's own
+working set (~3.5 GB) is far larger than L2 as well.
+
+Multi-GPU: a single DT does not shard (the flip, insertion and sort stages are
+global), so N GPUs run N independent replicas of the workload ("replicas
+only", weak scaling); value = all points triangulated / max time over ranks.
+
+--impl reference times the reference's CPU path on the host cores: the C
+oracle port (oracle/, a CPU restatement of the path) on bounded samples of the
+same workload, one process per core.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DT+alpha-spectrum Mpoints/s at 4M pts"
+UNIT = "Mpoints/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="galpha", choices=["galpha", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--n", type=int, default=None, help="override the point count")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() in ("active", "1", "0x1"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU oracle
+def _oracle_job(args):
+    n, seed = args
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from galpha_b200 import datasets as D
+    from oracle import oracle as O
+
+    pts = D.uniform_points(n, seed)
+    t = time.perf_counter()
+    v, nb, _ = O.dt(pts)
+    O.alpha(pts, v, nb)
+    return n, time.perf_counter() - t
+
+
+def cpu_baseline(sample_n=1 << 20):
+    """Single-core oracle port on a bounded sample (same distribution as c2)."""
+    n, dt = _oracle_job((sample_n, 2))
+    return {"value": n / dt / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "%d uniform points of the c2 distribution, oracle DT + alpha spectrum, 1 thread, %.1f s"
+                      % (n, dt)}
+
+
+def reference_arm(a):
+    import multiprocessing as mp
+
+    procs = max(1, os.cpu_count() or 1)
+    per = a.n if a.n else (1 << 18)  # points per process per step
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(procs) as pool:
+        for it in range(a.warmup + a.steps):
+            t = time.perf_counter()
+            res = pool.map(_oracle_job, [(per, 1000 + it * procs + k) for k in range(procs)])
+            el = time.perf_counter() - t
+            if it >= a.warmup:
+                times.append(el)
+    tot = sum(times)
+    value = a.steps * procs * per / tot / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * tot / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "c2 uniform [0,1]^2 (bounded CPU sample per step)", "points_per_process": per,
+                   "processes": procs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": "%d processes x %d uniform points per step, oracle DT + alpha" % (procs, per)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ GPU arm
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        if rank == 0:
+            reference_arm(a)
+        return
+
+    import numpy as np
+    import torch
+
+    import galpha_b200 as G
+    from galpha_b200 import datasets as D
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    pts, fbo = D.make(a.config, a.n)
+    n = len(pts)
+    lo, hi = pts.min(axis=0), pts.max(axis=0)
+    bounds = (float(lo[0]), float(lo[1]), float(hi[0]), float(hi[1]))
+    d_xy = torch.from_numpy(pts).cuda()
+    eng = G.Engine(device=local)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    L = G.load()
+
+    def step():
+        return eng.run_device(d_xy.data_ptr(), n, bounds, fbo, True)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    stages, kernels = [], []
+    launches0 = L.galphaLaunchCount()
+    torch.cuda.synchronize()
+    for k in range(a.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 255)
+            ev[k][0].record(stream)
+        st = step()
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+        stages.append(list(st.ms))
+        kernels.append(list(st.kernelMs))
+    torch.cuda.synchronize()
+    launches = L.galphaLaunchCount() - launches0
+    clk = clocks.stop()
+    ms = [s.elapsed_time(e) for s, e in ev]
+    mean_ms = sum(ms) / len(ms)
+    t = torch.tensor([mean_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    nt, ne, ns = eng.counts()
+    value = world * n / (max_ms / 1e3) / 1e6
+
+    # roofline of the dominant texture kernel (row pass: envelope + colouring)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    T = fbo
+    row_ms = sum(k[0] for k in kernels) / len(kernels)
+    row_bytes = 6.0 * T * T  # per launch: read the int16 column-candidate texture, write the int32 colour texture
+    col_ms = sum(k[1] for k in kernels) / len(kernels)
+    stage_mean = [sum(s[i] for s in stages) / len(stages) for i in range(12)]
+    # whole-pipeline algorithmic byte model (SURVEY-style compulsory traffic)
+    n_spec = ns
+    b_alg = 28.0 * T * T + 16.0 * n + 36.0 * nt + 8.0 * n_spec + 24.0 * n_spec + 12.0 * ne + 4.0 * nt + 8.0 * n
+    roof = {
+        "bound": "hbm", "kernel": "k_row_pass (per-row lower envelope + colouring)",
+        "achieved": row_bytes / (row_ms / 1e3) / 1e9 if row_ms > 0 else None, "peak": peak, "unit": "GB/s",
+        "frac": (row_bytes / (row_ms / 1e3) / 1e9) / peak if row_ms > 0 else None,
+        "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650",
+        "algorithmic_bytes_per_launch": row_bytes, "launch_ms": row_ms,
+        "pipeline": {"algorithmic_bytes": b_alg, "achieved_gbs": b_alg / (max_ms / 1e3) / 1e9,
+                     "frac": b_alg / (max_ms / 1e3) / 1e9 / peak},
+    }
+
+    # end to end through the host API
+    e2e = None
+    if not a.no_e2e:
+        pinned = torch.from_numpy(pts).pin_memory()
+        params = G.GPUDTParams(pinned.numpy(), fboSize=fbo, minX=bounds[0], minY=bounds[1], maxX=bounds[2],
+                               maxY=bounds[3])
+        tms = []
+        for k in range(a.warmup + a.steps):
+            torch.cuda.synchronize()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            dt = eng.triangulate(params)
+            al = eng.alpha_resident()
+            s1.record(stream)
+            s1.synchronize()
+            if k >= a.warmup:
+                tms.append(s0.elapsed_time(s1))
+        h2d = 16 * n
+        d2h = (36 * dt.nTris + al["spectrum"].nbytes + al["point_list"].nbytes + al["edge_list"].nbytes
+               + al["tri_list"].nbytes)
+        em = sum(tms) / len(tms)
+        te = torch.tensor([em], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * n / (float(te.item()) / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": float(te.item())}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": max_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "%s: %d points uniform [0,1]^2, FP64, texture %d^2, DT + alpha spectrum + intervals"
+                                   % (a.config, n, fbo), "points": n, "fboSize": fbo,
+                       "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
+                       "l2": "512 MiB write between timed steps; working set > L2"},
+            "e2e": e2e, "gpu_launches": int(launches // max(1, a.steps)), "gpu_launches_total": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "stages_ms": {nm: stage_mean[i] for i, nm in enumerate(
+                ["upload", "voronoi", "triangles", "shift", "missing", "boundary", "flip", "compact", "alpha",
+                 "download", "total"]) if i < 11},
+            "kernels_ms": {"row_pass": row_ms, "column_pass": col_ms,
+                           "emit": sum(k[2] for k in kernels) / len(kernels)},
+            "counts": {"triangles": nt, "edges": ne, "spectrum": ns},
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

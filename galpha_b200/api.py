@@ -1,0 +1,348 @@
+"""Python mirror of the reference's DT + alpha-shape interface over libgalpha's C ABI.
+
+Reference interface                               here
+------------------------------------------------  --------------------------------------------
+``GPUDTPARAMS`` / ``GPUDTOUTPUT`` (gpudt.h:105-128)  :class:`GPUDTParams`, :class:`DTOutput`
+``gpudtComputeDT`` (gpudt.h:131)                    :func:`gpudt_compute_dt`
+``gpudtReleaseDTOutput`` (gpudt.h:132)              (automatic: arrays are copied out)
+``Alpha_Shapes_2D(pInput, pDT)``,                   :class:`AlphaShapes2D` with
+``computeAlphaShapes()`` and the public /           ``compute_alpha_shapes()``, ``spectrum``,
+friend members (Alpha_Shapes_2D.h:43-121)            ``point_list``, ``edge_list``, ``tri_list``
+``ReadDataFromFileBinary`` (main.cu:117-161)        :func:`read_points_file`
+
+Errors raise :class:`GpudtError` with the C status code instead of exiting the
+process as the reference does (common.h:55-93).  Every call goes to the CUDA
+library; when it is missing or no sm_100 device is present the calls raise --
+there is no CPU path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_LIB = os.path.join(_HERE, "lib", "libgalpha.so")
+
+STATUS_TEXT = {
+    0: "ok",
+    -1: "bad argument",
+    -2: "CUDA error",
+    -3: "out of memory / budget",
+    -4: "mesh topology invariant violated",
+    -5: "iteration cap reached",
+    -6: "exact arithmetic scratch overflow",
+    -7: "no sm_100 device",
+}
+
+
+class GpudtError(RuntimeError):
+    def __init__(self, code, where=""):
+        self.code = code
+        msg = "%s failed: %d (%s)" % (where, code, STATUS_TEXT.get(code, "?"))
+        extra = _last_error()
+        if extra:
+            msg += " -- " + extra
+        super().__init__(msg)
+
+
+class _Vertex(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_double), ("y", ctypes.c_double)]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("minX", ctypes.c_double), ("minY", ctypes.c_double),
+        ("maxX", ctypes.c_double), ("maxY", ctypes.c_double),
+        ("nPoints", ctypes.c_int), ("points", ctypes.c_void_p),
+        ("nConstraints", ctypes.c_int), ("constraints", ctypes.c_void_p),
+        ("fboSize", ctypes.c_int),
+    ]
+
+
+class _Output(ctypes.Structure):
+    _fields_ = [("triangles", ctypes.c_void_p), ("nTris", ctypes.c_int)]
+
+
+class Status(ctypes.Structure):
+    """gpudtStatus: per-call statistics of the triangulation."""
+    _fields_ = [
+        ("status", ctypes.c_int), ("nVerts", ctypes.c_int), ("nFake", ctypes.c_int),
+        ("nDuplicates", ctypes.c_int), ("nMissing", ctypes.c_int), ("nBadShift", ctypes.c_int),
+        ("nIslandPixels", ctypes.c_int), ("nFlips", ctypes.c_int), ("flipRounds", ctypes.c_int),
+        ("shiftRounds", ctypes.c_int), ("missingRounds", ctypes.c_int),
+        ("exactOrient", ctypes.c_longlong), ("exactIncircle", ctypes.c_longlong),
+        ("filteredIncircle", ctypes.c_longlong),
+        ("ms", ctypes.c_float * 12),
+        ("kernelMs", ctypes.c_float * 4),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("ms", "kernelMs")}
+        d["ms"] = list(self.ms)
+        d["kernelMs"] = list(self.kernelMs)
+        return d
+
+
+class _AlphaOut(ctypes.Structure):
+    _fields_ = [
+        ("nSpectrum", ctypes.c_int), ("spectrum", ctypes.c_void_p),
+        ("nPoints", ctypes.c_int), ("point_list", ctypes.c_void_p),
+        ("nEdges", ctypes.c_int), ("edge_list", ctypes.c_void_p),
+        ("nTris", ctypes.c_int), ("tri_list", ctypes.c_void_p),
+        ("exactCompares", ctypes.c_longlong), ("exactTies", ctypes.c_longlong),
+        ("exactAttached", ctypes.c_longlong),
+    ]
+
+
+# numpy views of the C element layouts (gpudt.h:97-102, headers.h:48-64)
+TRIANGLE_DTYPE = np.dtype([("tri", np.int32, 3), ("vtx", np.int32, 3), ("tmp", np.int32, 3)])
+POINT_INTERVAL_DTYPE = np.dtype([("nu_min_rank", np.int32), ("nu_max_rank", np.int32)])
+EDGE_INTERVAL_DTYPE = np.dtype([
+    ("ro_rank", np.int32), ("nu_min_rank", np.int32), ("nu_max_rank", np.int32),
+    ("sc", np.int32), ("tIndex", np.int32), ("vOpp", np.int32),
+])
+TRIANGLE_INTERVAL_DTYPE = np.dtype([("ro_rank", np.int32)])
+
+_lib = None
+_lib_path = None
+
+
+def load(path=None):
+    """Load libgalpha (default: the in-tree galpha_b200/lib/libgalpha.so)."""
+    global _lib, _lib_path
+    path = path or DEFAULT_LIB
+    if _lib is not None and _lib_path == path:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError("libgalpha not built: %s (run galpha_b200.build.build())" % path)
+    L = ctypes.CDLL(path)
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.galphaCreate.argtypes = [ip, ctypes.c_longlong, ctypes.POINTER(vp)]
+    L.galphaDestroy.argtypes = [vp]
+    L.galphaSetStream.argtypes = [vp, vp]
+    L.galphaTriangulate.argtypes = [vp, ctypes.POINTER(_Params), ctypes.POINTER(_Output), ctypes.POINTER(Status)]
+    L.galphaComputeResident.argtypes = [vp, ctypes.POINTER(_AlphaOut)]
+    L.galphaCompute.argtypes = [vp, ctypes.POINTER(_Params), ctypes.POINTER(_Output), ctypes.POINTER(_AlphaOut)]
+    L.galphaRunDevice.argtypes = [vp, vp, ip, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ip, ip, ctypes.POINTER(Status)]
+    L.galphaGetCounts.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.galphaCopyTriangles.argtypes = [vp, vp, ip]
+    L.galphaReleaseOutput.argtypes = [ctypes.POINTER(_AlphaOut)]
+    L.galphaLastError.restype = ctypes.c_char_p
+    L.galphaVersion.restype = ctypes.c_char_p
+    L.galphaLaunchCount.restype = ctypes.c_ulonglong
+    L.gpudtComputeDTEx.argtypes = [ctypes.POINTER(_Params), ctypes.POINTER(_Output), ctypes.POINTER(Status)]
+    L.gpudt_release_dt_output.argtypes = [ctypes.POINTER(_Output)]
+    _lib, _lib_path = L, path
+    return L
+
+
+def _last_error():
+    if _lib is None:
+        return ""
+    s = _lib.galphaLastError()
+    return s.decode() if s else ""
+
+
+def _check(code, where):
+    if code != 0:
+        raise GpudtError(code, where)
+
+
+class GPUDTParams:
+    """GPUDTPARAMS (gpudt.h:105-118).  points: (N, 2) float64."""
+
+    def __init__(self, points, fboSize=2048, minX=None, minY=None, maxX=None, maxY=None, constraints=None):
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+        self.points = pts
+        self.nPoints = pts.shape[0]
+        self.fboSize = int(fboSize)
+        lo = pts.min(axis=0) if len(pts) else np.zeros(2)
+        hi = pts.max(axis=0) if len(pts) else np.ones(2)
+        self.minX = float(lo[0] if minX is None else minX)
+        self.minY = float(lo[1] if minY is None else minY)
+        self.maxX = float(hi[0] if maxX is None else maxX)
+        self.maxY = float(hi[1] if maxY is None else maxY)
+        self.constraints = constraints
+        self.nConstraints = 0 if constraints is None else len(constraints)
+
+    def _c(self):
+        p = _Params()
+        p.minX, p.minY, p.maxX, p.maxY = self.minX, self.minY, self.maxX, self.maxY
+        p.nPoints = self.nPoints
+        p.points = self.points.ctypes.data if self.nPoints else None
+        p.nConstraints = self.nConstraints
+        p.constraints = None
+        p.fboSize = self.fboSize
+        return p
+
+
+class DTOutput:
+    """GPUDTOUTPUT (gpudt.h:124-128): ``triangles`` is a TRIANGLE_DTYPE array."""
+
+    def __init__(self, triangles, status=None):
+        self.triangles = triangles
+        self.nTris = len(triangles)
+        self.status = status
+
+    @property
+    def vtx(self):
+        return self.triangles["vtx"]
+
+    @property
+    def tri(self):
+        return self.triangles["tri"]
+
+
+class Engine:
+    """A libgalpha handle: one CUDA stream and one device arena, reused across calls."""
+
+    def __init__(self, device=-1, budget_bytes=0, lib=None):
+        self._L = load(lib)
+        h = ctypes.c_void_p()
+        _check(self._L.galphaCreate(device, budget_bytes, ctypes.byref(h)), "galphaCreate")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.galphaDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def triangulate(self, params):
+        """Delaunay triangulation of params (gpudtComputeDT semantics)."""
+        cp = params._c()
+        out = _Output()
+        st = Status()
+        _check(self._L.galphaTriangulate(self._h, ctypes.byref(cp), ctypes.byref(out), ctypes.byref(st)),
+               "galphaTriangulate")
+        n = out.nTris
+        arr = np.empty(n, dtype=TRIANGLE_DTYPE)
+        if n:
+            ctypes.memmove(arr.ctypes.data, out.triangles, n * TRIANGLE_DTYPE.itemsize)
+        self._L.gpudt_release_dt_output(ctypes.byref(out))
+        return DTOutput(arr, st)
+
+    def alpha_resident(self):
+        """Alpha spectrum + intervals of the mesh left on the device by triangulate()."""
+        out = _AlphaOut()
+        _check(self._L.galphaComputeResident(self._h, ctypes.byref(out)), "galphaComputeResident")
+        return _alpha_arrays(self._L, out)
+
+    def alpha_of(self, params, dt):
+        """Alpha spectrum + intervals of a given triangulation (Alpha_Shapes_2D(pInput, pDT))."""
+        cp = params._c()
+        tri = np.ascontiguousarray(dt.triangles)
+        o = _Output()
+        o.triangles = tri.ctypes.data if len(tri) else None
+        o.nTris = len(tri)
+        out = _AlphaOut()
+        _check(self._L.galphaCompute(self._h, ctypes.byref(cp), ctypes.byref(o), ctypes.byref(out)),
+               "galphaCompute")
+        return _alpha_arrays(self._L, out)
+
+    def run_device(self, d_xy_ptr, n, bounds, fbo_size, with_alpha=True):
+        """Hot path on device-resident points (d_xy_ptr: device address of 2n doubles)."""
+        st = Status()
+        _check(self._L.galphaRunDevice(self._h, ctypes.c_void_p(d_xy_ptr), n, bounds[0], bounds[1], bounds[2],
+                                       bounds[3], fbo_size, 1 if with_alpha else 0, ctypes.byref(st)),
+               "galphaRunDevice")
+        return st
+
+    def counts(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._L.galphaGetCounts(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+    def set_stream(self, stream_ptr):
+        _check(self._L.galphaSetStream(self._h, ctypes.c_void_p(stream_ptr)), "galphaSetStream")
+
+
+def _alpha_arrays(L, out):
+    def take(ptr, n, dtype):
+        a = np.empty(n, dtype=dtype)
+        if n:
+            ctypes.memmove(a.ctypes.data, ptr, n * np.dtype(dtype).itemsize)
+        return a
+
+    res = {
+        "spectrum": take(out.spectrum, out.nSpectrum, np.float64),
+        "point_list": take(out.point_list, out.nPoints, POINT_INTERVAL_DTYPE),
+        "edge_list": take(out.edge_list, out.nEdges, EDGE_INTERVAL_DTYPE),
+        "tri_list": take(out.tri_list, out.nTris, TRIANGLE_INTERVAL_DTYPE),
+        "exactCompares": out.exactCompares,
+        "exactTies": out.exactTies,
+        "exactAttached": out.exactAttached,
+    }
+    L.galphaReleaseOutput(ctypes.byref(out))
+    return res
+
+
+_default_engine = None
+
+
+def _engine():
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine()
+    return _default_engine
+
+
+def gpudt_compute_dt(params):
+    """gpudtComputeDT(pParam) (gpudt.h:131): returns a DTOutput."""
+    return _engine().triangulate(params)
+
+
+class AlphaShapes2D:
+    """Alpha_Shapes_2D(pInput, pDT) + computeAlphaShapes() (Alpha_Shapes_2D.h:43-121).
+
+    After compute_alpha_shapes(): ``spectrum`` (float64, [0] = 0 sentinel),
+    ``point_list`` / ``edge_list`` / ``tri_list`` (structured arrays with the
+    reference's field names), ``alpha`` and ``alpha_index`` as in the reference.
+    """
+
+    def __init__(self, params, dt, engine=None):
+        self.pInput = params
+        self.pDT = dt
+        self._engine = engine
+        self.spectrum = None
+        self.point_list = None
+        self.edge_list = None
+        self.tri_list = None
+        self.alpha = 0.0
+        self.alpha_index = 0
+
+    def compute_alpha_shapes(self):
+        eng = self._engine or _engine()
+        r = eng.alpha_of(self.pInput, self.pDT)
+        self.spectrum = r["spectrum"]
+        self.point_list = r["point_list"]
+        self.edge_list = r["edge_list"]
+        self.tri_list = r["tri_list"]
+        self.stats = {k: r[k] for k in ("exactCompares", "exactTies", "exactAttached")}
+        return self
+
+    computeAlphaShapes = compute_alpha_shapes
+
+    def set_alpha(self, index):
+        """setAlpha (Alpha_Shapes_2D.cu): select the alpha value spectrum[index]."""
+        self.alpha_index = int(index)
+        self.alpha = float(self.spectrum[self.alpha_index]) if self.spectrum is not None else 0.0
+
+    setAlpha = set_alpha
+
+
+def read_points_file(path):
+    """The reference's input format (main.cu:117-161): first line N, then 'index x y' lines."""
+    with open(path) as f:
+        n = int(f.readline().split()[0])
+        pts = np.zeros((n, 2), dtype=np.float64)
+        for _ in range(n):
+            parts = f.readline().split()
+            pts[int(parts[0])] = (float(parts[1]), float(parts[2]))
+    return pts

@@ -1,0 +1,484 @@
+// alpha.cu -- alpha spectrum and per-simplex intervals on the device.
+//
+// Stage map (reference -> here):
+//   computeTriEdgeCount + exclusive_scan +          k_edge_count + scan: the reference's
+//   computeEdgeTriMap (kernel.cu:138-217)           ownership and numbering rule
+//   computeTriangleRo / computeEdgeRo /             k_tri_keys / k_edge_keys: birth times in
+//   processAttached (kernel.cu:219-358,             double-double (<= 1 ulp, certified),
+//   predicates.h:1297-1444)                         slivers recomputed exactly; attached test
+//                                                   filtered then exact (closed disc)
+//   thrust::remove_if x2 (Alpha_Shapes_2D.cu:       unattached edges compacted by a scan
+//   276-281)
+//   thrust::sort_by_key (Alpha_Shapes_2D.cu:317)    radix_sort: LSD radix sort of the FP64
+//                                                   bit patterns with an int payload
+//   markSpectrum + sorT odd-even rounds +           k_mark_runs / k_resolve_runs: every run
+//   CPU_insertion_sort (kernel.cu:785-1102,         of keys within 2 ulp is sorted with the
+//   Alpha_Shapes_2D.cu:344-610)                     exact comparator on the device; exact
+//                                                   ties share a rank
+//   processSpectrum / remove_if / UpdateBackRefs    scan of "new rank" flags + k_scatter_ranks
+//   (kernel.cu:360-401, Alpha_Shapes_2D.cu:483-512)
+//   edgeIntervals / computeVertexIntervals          k_edge_intervals / k_vertex_intervals:
+//   (kernel.cu:427-624)                             vertex min/max by atomics over edges
+#include <cstdio>
+#include <algorithm>
+#include "internal.cuh"
+#include "exact.cuh"
+
+namespace galpha {
+
+// ------------------------------------------------------------ double-double
+struct dd {
+    double h, l;
+};
+
+__device__ __forceinline__ dd dd_from_diff(double a, double b)
+{
+    dd r;
+    two_sum(a, -b, r.h, r.l);
+    return r;
+}
+
+__device__ __forceinline__ dd dd_mul(dd a, dd b)
+{
+    double p, e;
+    two_prod(a.h, b.h, p, e);
+    e = fma(a.h, b.l, e);
+    e = fma(a.l, b.h, e);
+    dd r;
+    fast_two_sum(p, e, r.h, r.l);
+    return r;
+}
+
+__device__ __forceinline__ dd dd_add(dd a, dd b)
+{
+    double s, e;
+    two_sum(a.h, b.h, s, e);
+    e += a.l + b.l;
+    dd r;
+    fast_two_sum(s, e, r.h, r.l);
+    return r;
+}
+
+__device__ __forceinline__ dd dd_sub(dd a, dd b)
+{
+    b.h = -b.h;
+    b.l = -b.l;
+    return dd_add(a, b);
+}
+
+__device__ __forceinline__ double dd_div_to_double(dd a, dd b)
+{
+    double q1 = a.h / b.h;
+    dd qb = dd_mul(dd{q1, 0.0}, b);
+    dd r = dd_sub(a, qb);
+    double q2 = r.h / b.h;
+    return q1 + q2;
+}
+
+__device__ __forceinline__ dd dd_sqdist(double2 p, double2 q)
+{
+    dd dx = dd_from_diff(p.x, q.x), dy = dd_from_diff(p.y, q.y);
+    return dd_add(dd_mul(dx, dx), dd_mul(dy, dy));
+}
+
+// Edge birth time (|pq|/2)^2.
+__device__ __forceinline__ double rho_edge(double2 p, double2 q)
+{
+    dd s = dd_sqdist(p, q);
+    return (s.h + s.l) * 0.25;
+}
+
+// Triangle birth time R^2 = abc / (4 ar^2); *sliver set when ar is too
+// cancelled for the double-double evaluation to certify 1 ulp.
+__device__ __forceinline__ double rho_tri(double2 A, double2 B, double2 C, bool *sliver)
+{
+    dd a = dd_sqdist(A, B), b = dd_sqdist(B, C), c = dd_sqdist(C, A);
+    dd N = dd_mul(dd_mul(a, b), c);
+    dd ux = dd_from_diff(B.x, A.x), vy = dd_from_diff(C.y, A.y);
+    dd vx = dd_from_diff(C.x, A.x), uy = dd_from_diff(B.y, A.y);
+    dd P1 = dd_mul(ux, vy), P2 = dd_mul(vx, uy);
+    dd ar = dd_sub(P1, P2);
+    double mag = fabs(P1.h) + fabs(P2.h);
+    *sliver = !(fabs(ar.h) >= ldexp(mag, -48));
+    dd D = dd_mul(ar, ar);
+    D.h *= 4.0;
+    D.l *= 4.0;
+    return dd_div_to_double(N, D);
+}
+
+// ------------------------------------------------------------------ kernels
+struct EdgeCount {
+    const int4 *cv, *cn;
+    int *cnt;
+    __device__ void operator()(long long ii) const
+    {
+        int t = (int)ii;
+        int4 v = cv[t], n = cn[t];
+        int k = 0;
+        for (int i = 0; i < 3; i++)
+            if (geti(v, p1(i)) < geti(v, m1(i)) || geti(n, i) == -1) k++;
+        cnt[t] = k;
+    }
+};
+
+// Triangle keys + owned edges + attached test.
+struct TriKeys {
+    const int4 *cv, *cn;
+    const double2 *P;
+    const int *e_off;
+    unsigned long long *keys;
+    int *vals;
+    int4 *edges;    // p1, p2, tIndex, vOpp
+    int *unatt;     // 1 if the edge enters the spectrum
+    int *edge_ro;
+    int *slivers;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int t = (int)ii;
+        int4 v = cv[t], n = cn[t];
+        double2 A = P[v.x], B = P[v.y], C = P[v.z];
+        bool sl;
+        double r = rho_tri(A, B, C, &sl);
+        keys[1 + t] = (unsigned long long)__double_as_longlong(r);
+        vals[1 + t] = t;
+        if (sl) {
+            int k = atomicAdd(&ct->nlist2, 1);
+            slivers[k] = t;
+        }
+        int e = e_off[t];
+        for (int i = 0; i < 3; i++) {
+            int a = geti(v, p1(i)), b = geti(v, m1(i));
+            int nb = geti(n, i);
+            if (!(a < b || nb == -1)) continue;
+            edges[e] = make_int4(a, b, t, i);
+            double2 pa = P[a], pb = P[b], pk = P[geti(v, i)];
+            double qa[2] = {pa.x, pa.y}, qb[2] = {pb.x, pb.y}, qk[2] = {pk.x, pk.y};
+            int att = attached_filter(qa, qb, qk);
+            if (att == 2) {
+                atomicAdd(&ct->exact_attached, 1ull);
+                att = attached_exact(qa, qb, qk);
+            }
+            if (att == 0 && nb >= 0) {
+                double2 po = P[geti(cv[dtri(nb)], dori(nb))];
+                double qo[2] = {po.x, po.y};
+                att = attached_filter(qa, qb, qo);
+                if (att == 2) {
+                    atomicAdd(&ct->exact_attached, 1ull);
+                    att = attached_exact(qa, qb, qo);
+                }
+            }
+            if (att == EXACT_OVERFLOW) set_err(ct, GPUDT_ERR_EXACT, 100);
+            unatt[e] = att ? 0 : 1;
+            if (att) edge_ro[e] = 0;
+            e++;
+        }
+    }
+};
+
+struct SliverKeys {
+    const int4 *cv;
+    const double2 *P;
+    const int *slivers;
+    unsigned long long *keys;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int t = slivers[ii];
+        int4 v = cv[t];
+        double p[6] = {P[v.x].x, P[v.x].y, P[v.y].x, P[v.y].y, P[v.z].x, P[v.z].y};
+        double r = rho_rounded_exact(3, p);
+        if (r != r) set_err(ct, GPUDT_ERR_EXACT, 101);
+        keys[1 + t] = (unsigned long long)__double_as_longlong(r);
+    }
+};
+
+struct EdgeKeys {
+    const int4 *edges;
+    const double2 *P;
+    const int *unatt, *spos;
+    unsigned long long *keys;
+    int *vals;
+    int base, nT;
+    __device__ void operator()(long long ii) const
+    {
+        int e = (int)ii;
+        if (!unatt[e]) return;
+        int4 E = edges[e];
+        int k = base + spos[e];
+        keys[k] = (unsigned long long)__double_as_longlong(rho_edge(P[E.x], P[E.y]));
+        vals[k] = nT + e;
+    }
+};
+
+// --------------------------------------------------------- ranks and runs
+__device__ __forceinline__ bool near_equal(unsigned long long ka, unsigned long long kb)
+{
+    // kb >= ka (sorted); keys carry <= 1 ulp of error each
+    double a = __longlong_as_double((long long)ka), b = __longlong_as_double((long long)kb);
+    double u = __longlong_as_double((long long)kb + 1) - b;  // ulp of the positive key b
+    return (b - a) <= 2.0 * u;
+}
+
+// nr[i] = 1 when entry i certainly starts a new rank.  Links within 2 ulp are
+// listed for one exact comparison each.
+struct MarkRuns {
+    const unsigned long long *keys;
+    int *nr;
+    int *unc;
+    int n;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int i = (int)ii;
+        if (i == 0) {
+            nr[0] = 0;
+            return;
+        }
+        if (i >= 2 && near_equal(keys[i - 1], keys[i])) {
+            nr[i] = 0;
+            int k = atomicAdd(&ct->nlist, 1);
+            unc[k] = i;
+        } else {
+            nr[i] = 1;
+        }
+    }
+};
+
+__device__ __forceinline__ void entry_points(int val, int nT, const int4 *cv, const int4 *edges,
+                                             const double2 *P, int *kind, double *p)
+{
+    if (val < nT) {
+        int4 v = cv[val];
+        double2 a = P[v.x], b = P[v.y], c = P[v.z];
+        p[0] = a.x; p[1] = a.y; p[2] = b.x; p[3] = b.y; p[4] = c.x; p[5] = c.y;
+        *kind = 3;
+    } else {
+        int4 E = edges[val - nT];
+        double2 a = P[E.x], b = P[E.y];
+        p[0] = a.x; p[1] = a.y; p[2] = b.x; p[3] = b.y;
+        *kind = 2;
+    }
+}
+
+__device__ __forceinline__ int exact_cmp_vals(int va, int vb, int nT, const int4 *cv, const int4 *edges,
+                                              const double2 *P)
+{
+    int ka, kb;
+    double pa[6], pb[6];
+    entry_points(va, nT, cv, edges, P, &ka, pa);
+    entry_points(vb, nT, cv, edges, P, &kb, pb);
+    return compare_rho_exact(ka, pa, kb, pb);
+}
+
+// One exact comparison per uncertain adjacent pair (parallel over pairs): a
+// smaller left value starts a new rank, an exact tie shares the rank, and an
+// order violation sends the whole run to k_resolve (rare: it needs two distinct
+// values within one ulp whose keys rounded the wrong way).
+struct ExactAdjacent {
+    const unsigned long long *keys;
+    const int *vals;
+    int *nr, *slow, *slowflag;
+    const int *unc;
+    const int4 *cv, *edges;
+    const double2 *P;
+    int nT;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int i = unc[ii];
+        int cmp = exact_cmp_vals(vals[i - 1], vals[i], nT, cv, edges, P);
+        atomicAdd(&ct->exact_compares, 1ull);
+        if (cmp == EXACT_OVERFLOW) {
+            set_err(ct, GPUDT_ERR_EXACT, 110);
+            return;
+        }
+        if (cmp < 0) {
+            nr[i] = 1;
+        } else if (cmp == 0) {
+            nr[i] = 0;
+            atomicAdd(&ct->nties, 1);
+        } else {
+            int s = i - 1;
+            while (s >= 2 && near_equal(keys[s - 1], keys[s])) s--;
+            if (atomicCAS(&slowflag[s], 0, 1) == 0) {
+                int k = atomicAdd(&ct->nlist2, 1);
+                slow[k] = s;
+            }
+        }
+    }
+};
+
+// Rare path: one thread sorts a whole run with the exact comparator and
+// recomputes its rank-start flags.  Runs longer than kMaxSlowRun are refused
+// (GPUDT_ERR_EXACT) rather than sorted in quadratic time.
+constexpr int kMaxSlowRun = 16384;
+struct ResolveRuns {
+    unsigned long long *keys;
+    int *vals, *nr;
+    const int *runs;
+    const int4 *cv, *edges;
+    const double2 *P;
+    int n, nT;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int s = runs[ii];
+        int e = s;
+        while (e + 1 < n && near_equal(keys[e], keys[e + 1])) e++;
+        if (e - s > kMaxSlowRun) {
+            set_err(ct, GPUDT_ERR_EXACT, 113);
+            return;
+        }
+        for (int a = s + 1; a <= e; a++) {
+            unsigned long long kc = keys[a];
+            int vc = vals[a];
+            int b = a - 1;
+            for (; b >= s; b--) {
+                int cmp = exact_cmp_vals(vals[b], vc, nT, cv, edges, P);
+                if (cmp == EXACT_OVERFLOW) {
+                    set_err(ct, GPUDT_ERR_EXACT, 111);
+                    return;
+                }
+                if (cmp <= 0) break;
+                keys[b + 1] = keys[b];
+                vals[b + 1] = vals[b];
+            }
+            keys[b + 1] = kc;
+            vals[b + 1] = vc;
+        }
+        for (int a = s + 1; a <= e; a++) {
+            int cmp = exact_cmp_vals(vals[a - 1], vals[a], nT, cv, edges, P);
+            if (cmp == EXACT_OVERFLOW) {
+                set_err(ct, GPUDT_ERR_EXACT, 112);
+                return;
+            }
+            nr[a] = cmp != 0 ? 1 : 0;
+        }
+    }
+};
+
+struct ScatterRanks {
+    const unsigned long long *keys;
+    const int *vals, *nr, *excl;
+    int *tri_ro, *edge_ro;
+    double *spectrum;
+    int nT;
+    __device__ void operator()(long long ii) const
+    {
+        int i = (int)ii;
+        int r = excl[i] + nr[i];
+        if (i == 0) {
+            spectrum[0] = 0.0;
+            return;
+        }
+        int v = vals[i];
+        if (v < nT) tri_ro[v] = r;
+        else edge_ro[v - nT] = r;
+        if (nr[i]) spectrum[r] = __longlong_as_double((long long)keys[i]);
+    }
+};
+
+struct EdgeIntervals {
+    const int4 *edges, *cn;
+    const int *tri_ro, *edge_ro;
+    int2 *edge_nu;
+    int2 *pt;  // (min, max) accumulators
+    __device__ void operator()(long long ii) const
+    {
+        int e = (int)ii;
+        int4 E = edges[e];
+        int nb = geti(cn[E.z], E.w);
+        int tr = tri_ro[E.z];
+        int2 nu;
+        if (nb == -1) {
+            nu = make_int2(tr, 0);
+        } else {
+            int o = tri_ro[dtri(nb)];
+            nu = tr <= o ? make_int2(tr, o) : make_int2(o, tr);
+        }
+        edge_nu[e] = nu;
+        int ro = edge_ro[e];
+        int vmin = ro != 0 ? ro : nu.x;
+        atomicMin(&pt[E.x].x, vmin);
+        atomicMax(&pt[E.x].y, nu.y);
+        atomicMin(&pt[E.y].x, vmin);
+        atomicMax(&pt[E.y].y, nu.y);
+    }
+};
+
+struct InitPt {
+    int2 *pt;
+    __device__ void operator()(long long i) const { pt[i] = make_int2(0x7fffffff, -1); }
+};
+
+struct FixPt {
+    int2 *pt;
+    __device__ void operator()(long long i) const
+    {
+        if (pt[i].x == 0x7fffffff) pt[i] = make_int2(-1, -1);
+    }
+};
+
+// ------------------------------------------------------------------ stage
+int stage_alpha(Ctx &c)
+{
+    int r;
+    const int nT = c.nT_out;
+    int *cnt = c.aux, *e_off = c.e_off;
+    launch_n(c, EdgeCount{c.cv, c.cn, cnt}, nT);
+    r = exclusive_scan_int(c, cnt, e_off, nT, &c.ctr->nlist);
+    if (r) return r;
+    r = read_counters(c);
+    if (r) return r;
+    const int nE = c.hctr->nlist;
+    c.nE = nE;
+    int *unatt = c.aux2, *spos = c.rank;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.keys, 0, sizeof(unsigned long long), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.vals, 0, sizeof(int), c.stream));
+    launch_n(c, TriKeys{c.cv, c.cn, c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->err) return c.hctr->err;
+    if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{c.cv, c.opos, c.list, c.keys, c.ctr}, c.hctr->nlist2);
+    r = exclusive_scan_int(c, unatt, spos, nE, &c.ctr->nlist);
+    if (r) return r;
+    launch_n(c, EdgeKeys{c.edges, c.opos, unatt, spos, c.keys, c.vals, 1 + nT, nT}, nE);
+    r = read_counters(c);
+    if (r) return r;
+    const int nIn = 1 + nT + c.hctr->nlist;
+    c.nSpecIn = nIn;
+    r = radix_sort(c, c.keys + 1, c.vals + 1, c.keys2, c.vals2, nIn - 1);
+    if (r) return r;
+    // ranks
+    int *nr = c.aux, *unc = c.list, *slow = c.list2, *slowflag = c.stamp;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int), c.stream));
+    launch_n(c, MarkRuns{c.keys, nr, unc, nIn, c.ctr}, nIn);
+    r = read_counters(c);
+    if (r) return r;
+    int nunc = c.hctr->nlist;
+    if (nunc > 0) {
+        GALPHA_CUDA(cudaMemsetAsync(slowflag, 0, sizeof(int) * (size_t)nIn, c.stream));
+        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, c.cv, c.edges, c.opos, nT, c.ctr}, nunc);
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        if (c.hctr->nlist2 > 0)
+            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, c.cv, c.edges, c.opos, nIn, nT, c.ctr}, c.hctr->nlist2);
+    }
+    r = exclusive_scan_int(c, nr, c.rank, nIn, &c.ctr->nlist);
+    if (r) return r;
+    launch_n(c, ScatterRanks{c.keys, c.vals, nr, c.rank, c.tri_ro, c.edge_ro, c.spectrum, nT}, nIn);
+    launch_n(c, InitPt{c.pt_nu}, c.N);
+    launch_n(c, EdgeIntervals{c.edges, c.cn, c.tri_ro, c.edge_ro, c.edge_nu, c.pt_nu}, nE);
+    launch_n(c, FixPt{c.pt_nu}, c.N);
+    GALPHA_CUDA(cudaGetLastError());
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->err) return c.hctr->err;
+    c.nSpec = c.hctr->nlist + 1;  // distinct ranks incl. the sentinel
+    return GPUDT_OK;
+}
+
+}  // namespace galpha

@@ -1,0 +1,646 @@
+// api.cu -- C ABI of libgalpha: handles, device arena, stage orchestration.
+//
+// Entry points and the reference interfaces they replace are listed in
+// include/gpudt.h and include/galpha.h.  The reference keeps global host and
+// device state and exits on any CUDA error (gpudt.cpp:64-77, cudaMain.cu:69-92,
+// common.h:55-93); here each handle owns its stream and buffers, every entry
+// point returns a GPUDT_* status, and device-side errors (topology, iteration
+// caps, exact-arithmetic scratch) are reported through the counter block.
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <mutex>
+#include <new>
+#include "internal.cuh"
+
+namespace galpha {
+
+static thread_local std::string g_err;
+unsigned long long g_launches = 0;
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? GPUDT_ERR_NOMEM : GPUDT_ERR_CUDA;
+}
+
+const char *last_error_text() { return g_err.c_str(); }
+
+int read_counters(Ctx &c)
+{
+    GALPHA_CUDA(cudaMemcpyAsync(c.hctr, c.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    return GPUDT_OK;
+}
+
+// One arena per handle; carve() hands out 256-byte aligned pieces.
+struct Arena {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+    void *carve(size_t bytes)
+    {
+        size_t off = (used + 255) & ~(size_t)255;
+        if (off + bytes > cap) return nullptr;
+        used = off + bytes;
+        return base + off;
+    }
+};
+
+struct Sizes {
+    size_t V, T2, cap, lists, ntiles;
+};
+
+static size_t plan(const Sizes &z, Ctx *c, Arena *A)
+{
+    size_t total = 0;
+    auto take = [&](size_t bytes) -> void * {
+        size_t off = (total + 255) & ~(size_t)255;
+        total = off + bytes;
+        return A ? A->carve(bytes) : nullptr;
+    };
+    size_t V = z.V, cap = z.cap, T2 = z.T2, L = z.lists;
+    size_t T = (size_t)std::llround(std::sqrt((double)T2));
+    size_t W2 = ((T >> 6) + 31) / 32;
+#define TAKE(field, type, count) \
+    {                            \
+        void *p_ = take(sizeof(type) * (size_t)(count)); \
+        if (c) c->field = (type *)p_; \
+    }
+    TAKE(opos, double2, V);
+    TAKE(pos, double2, V);
+    TAKE(gpix, short2, V);
+    TAKE(idmap, int, T2);
+    TAKE(occ, uint32_t, T * (T / 32));
+    TAKE(bandocc, uint32_t, T * W2);
+    TAKE(ycol, int16_t, T2);
+    TAKE(colour, int, T2);
+    TAKE(list, int, L);
+    TAKE(list2, int, L);
+    TAKE(aux, int, L);
+    TAKE(aux2, int, L);
+    TAKE(tv, int4, cap);
+    TAKE(tn, int4, cap);
+    TAKE(fwd, int4, cap);
+    TAKE(cv, int4, cap);
+    TAKE(cn, int4, cap);
+    TAKE(epoch, int, cap);
+    TAKE(vote, int, cap);
+    TAKE(stamp, int, L);
+    TAKE(freelist, int, cap);
+    TAKE(rec, Relink, 3 * cap);
+    TAKE(vtri, int, V);
+    TAKE(vstate, int8_t, V);
+    TAKE(vround, int, V);
+    TAKE(anchor, int, V);
+    TAKE(deg, int, V + 1);
+    TAKE(inc, int, 3 * cap);
+    TAKE(tilecount, int, z.ntiles + 1);
+    TAKE(hist, int, 65536);
+    TAKE(rhist, int, 256 * (3 * cap / 4096 + 2) + 16);
+    TAKE(e_off, int, cap + 1);
+    TAKE(edges, int4, 2 * cap);
+    TAKE(edge_ro, int, 2 * cap);
+    TAKE(edge_nu, int2, 2 * cap);
+    TAKE(tri_ro, int, cap);
+    TAKE(pt_nu, int2, V);
+    TAKE(keys, unsigned long long, 3 * cap);
+    TAKE(keys2, unsigned long long, 3 * cap);
+    TAKE(vals, int, 3 * cap);
+    TAKE(vals2, int, 3 * cap);
+    TAKE(rank, int, 3 * cap);
+    TAKE(spectrum, double, 3 * cap);
+    TAKE(outtri, gpudtTriangle, cap);
+    TAKE(ctr, Counters, 1);
+#undef TAKE
+    return total + 4096;
+}
+
+struct HandleState {
+    Ctx c;
+    Arena arena;
+    double *d_xy = nullptr;
+    size_t d_xy_cap = 0;
+};
+
+static int ensure(HandleState &H, int V, int T, long long nExtraTris)
+{
+    Ctx &c = H.c;
+    Sizes z;
+    z.V = (size_t)V;
+    z.T2 = (size_t)T * T;
+    z.cap = (size_t)2 * V + 64 + (size_t)(nExtraTris > 0 ? nExtraTris : 0);
+    z.lists = std::max(z.cap * 3, z.V + 1);
+    z.ntiles = ((size_t)(T - 1) * (T - 1) + 255) / 256 + 1;
+    size_t need = plan(z, nullptr, nullptr);
+    if (c.budget > 0 && (long long)need > c.budget) {
+        g_err = "device memory budget exceeded";
+        return GPUDT_ERR_NOMEM;
+    }
+    if (need > H.arena.cap) {
+        if (H.arena.base) cudaFree(H.arena.base);
+        H.arena.base = nullptr;
+        H.arena.cap = 0;
+        void *p = nullptr;
+        GALPHA_CUDA(cudaMalloc(&p, need));
+        H.arena.base = (char *)p;
+        H.arena.cap = need;
+        c.reserved = (long long)need;
+        GALPHA_CUDA(cudaMemsetAsync(p, 0, need, c.stream));
+    }
+    H.arena.used = 0;
+    plan(z, &c, &H.arena);
+    c.cap_tris = (int)z.cap;
+    // per-call initialisation of the slot state
+    GALPHA_CUDA(cudaMemsetAsync(c.epoch, 0, sizeof(int) * z.cap, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.vote, 0x7f, sizeof(int) * z.cap, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.ctr, 0, sizeof(Counters), c.stream));
+    return GPUDT_OK;
+}
+
+static void ev_record(Ctx &c, int k)
+{
+    if (c.events) cudaEventRecord(c.ev[k], c.stream);
+}
+
+static int fbo_ok(int T) { return T >= 256 && T <= 16384 && (T & (T - 1)) == 0; }
+
+// Records which stage failed and the device-side detail code.
+static int stage_fail(Ctx &c, int r, const char *stage)
+{
+    if (r == GPUDT_ERR_CUDA || r == GPUDT_ERR_NOMEM) {
+        if (g_err.find(stage) == std::string::npos) g_err = std::string(stage) + ": " + g_err;
+        return r;
+    }
+    read_counters(c);
+    char buf[160];
+    snprintf(buf, sizeof(buf), "stage %s: device error %d, detail %d", stage, c.hctr->err, c.hctr->errinfo);
+    g_err = buf;
+    return r;
+}
+
+// DT of n device points (interleaved xy).  Leaves the compacted mesh in c.cv/c.cn.
+static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double minY, double maxX, double maxY,
+                  int T)
+{
+    Ctx &c = H.c;
+    int r;
+    int nside = (T - 1 + kFakeSpacing - 1) / kFakeSpacing;
+    int V = n + 4 * nside;
+    r = ensure(H, V, T, 0);
+    if (r) return r;
+    memset(&c.st, 0, sizeof(c.st));
+    c.have_mesh = c.have_alpha = false;
+    ev_record(c, 1);
+    int nonempty = has_triangles(c, d_xy, n);
+    if (nonempty < 0) return stage_fail(c, nonempty, "precheck");
+    if (nonempty == 0) {
+        // fewer than three distinct points, or all collinear: no triangle
+        // (the reference has no defined output here; this returns an empty mesh)
+        c.N = n;
+        c.nT_out = 0;
+        c.have_mesh = true;
+        for (int k = 2; k <= 8; k++) ev_record(c, k);
+        return GPUDT_OK;
+    }
+    const char *stage = "setup";
+#define STAGE(name, call)        \
+    stage = name;                \
+    r = (call);                  \
+    if (r) return stage_fail(c, r, stage)
+    STAGE("setup", stage_setup(c, d_xy, n, minX, minY, maxX, maxY, T));
+    STAGE("voronoi", stage_voronoi(c));
+    ev_record(c, 2);
+    STAGE("triangles", stage_triangles(c));
+    STAGE("links", stage_links(c));
+    ev_record(c, 3);
+    STAGE("shift", stage_shift(c));
+    ev_record(c, 4);
+    STAGE("missing", stage_missing(c));
+    ev_record(c, 5);
+    STAGE("boundary", stage_boundary(c));
+    ev_record(c, 6);
+    STAGE("flip", stage_flip(c));
+    ev_record(c, 7);
+    STAGE("compact", stage_compact(c));
+#undef STAGE
+    ev_record(c, 8);
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->err) return stage_fail(c, c.hctr->err, "final");
+    c.st.nVerts = c.V;
+    c.st.nFake = c.F;
+    c.st.exactOrient = (long long)c.hctr->exact_orient;
+    c.st.exactIncircle = (long long)c.hctr->exact_incircle;
+    c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
+    c.have_mesh = true;
+    return GPUDT_OK;
+}
+
+static void fill_times(Ctx &c, int last)
+{
+    if (!c.events) return;
+    cudaEventSynchronize(c.ev[last]);
+    for (int k = 1; k < last; k++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c.ev[k], c.ev[k + 1]) == cudaSuccess && k < 12) c.st.ms[k] = ms;
+    }
+    float tot = 0.f;
+    if (cudaEventElapsedTime(&tot, c.ev[0], c.ev[last]) == cudaSuccess) c.st.ms[GALPHA_STAGE_TOTAL] = tot;
+    if (c.have_mesh && c.nT_out > 0) {
+        float a = 0.f, b = 0.f;
+        if (cudaEventElapsedTime(&a, c.kev[0], c.kev[1]) == cudaSuccess) c.st.kernelMs[0] = a;
+        if (cudaEventElapsedTime(&a, c.kev[2], c.kev[3]) == cudaSuccess) c.st.kernelMs[1] = a;
+        if (cudaEventElapsedTime(&a, c.kev[4], c.kev[5]) == cudaSuccess &&
+            cudaEventElapsedTime(&b, c.kev[6], c.kev[7]) == cudaSuccess)
+            c.st.kernelMs[2] = a + b;
+    }
+}
+
+static int upload_points(HandleState &H, const gpudtVertex *pts, int n)
+{
+    Ctx &c = H.c;
+    size_t bytes = sizeof(double) * 2 * (size_t)(n > 0 ? n : 1);
+    if (bytes > H.d_xy_cap) {
+        if (H.d_xy) cudaFree(H.d_xy);
+        H.d_xy = nullptr;
+        H.d_xy_cap = 0;
+        GALPHA_CUDA(cudaMalloc(&H.d_xy, bytes));
+        H.d_xy_cap = bytes;
+    }
+    if (n > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(H.d_xy, pts, sizeof(double) * 2 * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    return GPUDT_OK;
+}
+
+static int check_params(const GPUDTPARAMS *p)
+{
+    if (!p) return GPUDT_ERR_ARG;
+    if (p->nPoints < 0 || (p->nPoints > 0 && !p->points)) return GPUDT_ERR_ARG;
+    if (p->nConstraints != 0) return GPUDT_ERR_ARG;
+    if (!fbo_ok(p->fboSize)) return GPUDT_ERR_ARG;
+    if (p->nPoints >= (1 << 28)) return GPUDT_ERR_ARG;
+    if (!(std::isfinite(p->minX) && std::isfinite(p->minY) && std::isfinite(p->maxX) && std::isfinite(p->maxY)))
+        return GPUDT_ERR_ARG;
+    if (p->minX > p->maxX || p->minY > p->maxY) return GPUDT_ERR_ARG;
+    return GPUDT_OK;
+}
+
+}  // namespace galpha
+
+using namespace galpha;
+
+struct galpha_ctx {
+    HandleState H;
+    std::mutex mu;
+};
+
+static int handle_init(galpha_ctx *h, int device, long long budget)
+{
+    Ctx &c = h->H.c;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_err = "no CUDA device";
+        return GPUDT_ERR_NODEVICE;
+    }
+    if (device < 0) GALPHA_CUDA(cudaGetDevice(&device));
+    GALPHA_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    GALPHA_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        g_err = "libgalpha is built for sm_100a";
+        return GPUDT_ERR_NODEVICE;
+    }
+    c.device = device;
+    c.sm_count = prop.multiProcessorCount;
+    c.budget = budget;
+    GALPHA_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.own_stream = true;
+    GALPHA_CUDA(cudaMallocHost(&c.hctr, sizeof(Counters)));
+    memset(c.hctr, 0, sizeof(Counters));
+    for (int k = 0; k < GALPHA_STAGE_TOTAL + 2; k++) GALPHA_CUDA(cudaEventCreate(&c.ev[k]));
+    for (int k = 0; k < 8; k++) GALPHA_CUDA(cudaEventCreate(&c.kev[k]));
+    c.events = true;
+    // exact fall-back paths keep expansion arrays on the per-thread stack
+    GALPHA_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 18432));  // largest kernel frame is ~16 KB
+    return GPUDT_OK;
+}
+
+extern "C" {
+
+const char *galphaVersion(void) { return "galpha-b200 0.1 (sm_100a)"; }
+
+unsigned long long galphaLaunchCount(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+const char *galphaLastError(void) { return last_error_text(); }
+
+int galphaCreate(int device, long long budgetBytes, galphaHandle *out)
+{
+    if (!out) return GPUDT_ERR_ARG;
+    galpha_ctx *h = new (std::nothrow) galpha_ctx;
+    if (!h) return GPUDT_ERR_NOMEM;
+    int r = handle_init(h, device, budgetBytes);
+    if (r) {
+        delete h;
+        *out = nullptr;
+        return r;
+    }
+    *out = h;
+    return GPUDT_OK;
+}
+
+int galphaDestroy(galphaHandle h)
+{
+    if (!h) return GPUDT_OK;
+    Ctx &c = h->H.c;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    if (h->H.arena.base) cudaFree(h->H.arena.base);
+    if (h->H.d_xy) cudaFree(h->H.d_xy);
+    if (c.hctr) cudaFreeHost(c.hctr);
+    for (int k = 0; k < GALPHA_STAGE_TOTAL + 2 && c.events; k++) cudaEventDestroy(c.ev[k]);
+    for (int k = 0; k < 8 && c.events; k++) cudaEventDestroy(c.kev[k]);
+    if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+    delete h;
+    return GPUDT_OK;
+}
+
+int galphaSetStream(galphaHandle h, void *stream)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    if (stream) {
+        if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+        c.stream = (cudaStream_t)stream;
+        c.own_stream = false;
+    }
+    return GPUDT_OK;
+}
+
+int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY, double maxX, double maxY,
+                    int fboSize, int withAlpha, gpudtStatus *st)
+{
+    if (!h || n < 0 || !fbo_ok(fboSize)) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    cudaSetDevice(c.device);
+    ev_record(c, 0);
+    int r = run_dt(h->H, d_xy, n, minX, minY, maxX, maxY, fboSize);
+    if (!r && withAlpha) {
+        ev_record(c, 8);
+        r = stage_alpha(c);
+        if (!r) c.have_alpha = true;
+        ev_record(c, 9);
+        if (!r) fill_times(c, 9);
+    } else if (!r) {
+        fill_times(c, 8);
+    }
+    c.st.status = r;
+    if (st) *st = c.st;
+    return r;
+}
+
+int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *out, gpudtStatus *st)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    int r = check_params(params);
+    if (r) return r;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    cudaSetDevice(c.device);
+    ev_record(c, 0);
+    r = upload_points(h->H, params->points, params->nPoints);
+    if (!r)
+        r = run_dt(h->H, h->H.d_xy, params->nPoints, params->minX, params->minY, params->maxX, params->maxY,
+                   params->fboSize);
+    if (!r && out) {
+        int n = params->nPoints;
+        int nv = n + std::max(4, (int)(std::sqrt((double)n) / 10));
+        int capacity = std::max(2 * nv, c.nT_out);
+        gpudtTriangle *tris = new (std::nothrow) gpudtTriangle[capacity > 0 ? capacity : 1];
+        if (!tris) r = GPUDT_ERR_NOMEM;
+        else {
+            if (c.nT_out > 0) {
+                cudaError_t e = cudaMemcpyAsync(tris, c.outtri, sizeof(gpudtTriangle) * (size_t)c.nT_out,
+                                                cudaMemcpyDeviceToHost, c.stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+                if (e != cudaSuccess) r = cuda_fail(e, "download triangles");
+            }
+            out->triangles = tris;
+            out->nTris = c.nT_out;
+        }
+    }
+    if (!r) fill_times(c, 8);
+    c.st.status = r;
+    if (st) *st = c.st;
+    return r;
+}
+
+int galphaGetCounts(galphaHandle h, int *nTris, int *nEdges, int *nSpectrum)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    Ctx &c = h->H.c;
+    if (nTris) *nTris = c.have_mesh ? c.nT_out : 0;
+    if (nEdges) *nEdges = c.have_alpha ? c.nE : 0;
+    if (nSpectrum) *nSpectrum = c.have_alpha ? c.nSpec : 0;
+    return GPUDT_OK;
+}
+
+int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap)
+{
+    if (!h || !dst) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    if (!c.have_mesh) return GPUDT_ERR_ARG;
+    int n = std::min(cap, c.nT_out);
+    if (n > 0) {
+        GALPHA_CUDA(cudaMemcpyAsync(dst, c.outtri, sizeof(gpudtTriangle) * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
+        GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    return GPUDT_OK;
+}
+
+static int download_alpha(Ctx &c, GAlphaOutput *out)
+{
+    memset(out, 0, sizeof(*out));
+    out->nSpectrum = c.nSpec;
+    out->nPoints = c.N;
+    out->nEdges = c.nE;
+    out->nTris = c.nT_out;
+    out->spectrum = (double *)malloc(sizeof(double) * (size_t)std::max(1, c.nSpec));
+    out->point_list = (galphaPointInterval *)malloc(sizeof(galphaPointInterval) * (size_t)std::max(1, c.N));
+    out->edge_list = (galphaEdgeInterval *)malloc(sizeof(galphaEdgeInterval) * (size_t)std::max(1, c.nE));
+    out->tri_list = (galphaTriangleInterval *)malloc(sizeof(galphaTriangleInterval) * (size_t)std::max(1, c.nT_out));
+    int4 *edges = (int4 *)malloc(sizeof(int4) * (size_t)std::max(1, c.nE));
+    int *ero = (int *)malloc(sizeof(int) * (size_t)std::max(1, c.nE));
+    int2 *enu = (int2 *)malloc(sizeof(int2) * (size_t)std::max(1, c.nE));
+    if (!out->spectrum || !out->point_list || !out->edge_list || !out->tri_list || !edges || !ero || !enu) {
+        free(edges);
+        free(ero);
+        free(enu);
+        galphaReleaseOutput(out);
+        return GPUDT_ERR_NOMEM;
+    }
+    cudaStream_t s = c.stream;
+    GALPHA_CUDA(cudaMemcpyAsync(out->spectrum, c.spectrum, sizeof(double) * (size_t)c.nSpec, cudaMemcpyDeviceToHost, s));
+    if (c.N > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(out->point_list, c.pt_nu, sizeof(int2) * (size_t)c.N, cudaMemcpyDeviceToHost, s));
+    if (c.nT_out > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(out->tri_list, c.tri_ro, sizeof(int) * (size_t)c.nT_out, cudaMemcpyDeviceToHost, s));
+    if (c.nE > 0) {
+        GALPHA_CUDA(cudaMemcpyAsync(edges, c.edges, sizeof(int4) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
+        GALPHA_CUDA(cudaMemcpyAsync(ero, c.edge_ro, sizeof(int) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
+        GALPHA_CUDA(cudaMemcpyAsync(enu, c.edge_nu, sizeof(int2) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
+    }
+    GALPHA_CUDA(cudaStreamSynchronize(s));
+    for (int e = 0; e < c.nE; e++) {
+        galphaEdgeInterval &E = out->edge_list[e];
+        E.ro_rank = ero[e];
+        E.nu_min_rank = enu[e].x;
+        E.nu_max_rank = enu[e].y;
+        E.sc = ero[e] == 0 ? 0 : 1;
+        E.tIndex = edges[e].z;
+        E.vOpp = edges[e].w;
+    }
+    out->exactCompares = (long long)c.hctr->exact_compares;
+    out->exactTies = c.hctr->nties;
+    out->exactAttached = (long long)c.hctr->exact_attached;
+    free(edges);
+    free(ero);
+    free(enu);
+    return GPUDT_OK;
+}
+
+int galphaComputeResident(galphaHandle h, GAlphaOutput *out)
+{
+    if (!h || !out) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    if (!c.have_mesh) return GPUDT_ERR_ARG;
+    cudaSetDevice(c.device);
+    int r = GPUDT_OK;
+    if (!c.have_alpha) {
+        r = stage_alpha(c);
+        if (r) return r;
+        c.have_alpha = true;
+    }
+    return download_alpha(c, out);
+}
+
+// Alpha of a host triangulation: the points and triangles are uploaded into
+// the handle's mesh arrays, then the same device stage runs.
+struct AosToSoa {
+    const gpudtTriangle *in;
+    int4 *cv, *cn;
+    __device__ void operator()(long long i) const
+    {
+        gpudtTriangle g = in[i];
+        cv[i] = make_int4(g.vtx[0], g.vtx[1], g.vtx[2], 0);
+        cn[i] = make_int4(g.tri[0], g.tri[1], g.tri[2], 0);
+    }
+};
+
+int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *dt, GAlphaOutput *out)
+{
+    if (!h || !params || !dt || !out || params->nPoints < 0 || dt->nTris < 0) return GPUDT_ERR_ARG;
+    if (dt->nTris > 0 && !dt->triangles) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    cudaSetDevice(c.device);
+    int n = params->nPoints;
+    int r = ensure(h->H, n + 4, 256, (long long)dt->nTris);
+    if (r) return r;
+    r = upload_points(h->H, params->points, n);
+    if (r) return r;
+    c.N = n;
+    c.V = n;
+    GALPHA_CUDA(cudaMemcpyAsync(c.opos, h->H.d_xy, sizeof(double2) * (size_t)n, cudaMemcpyDeviceToDevice, c.stream));
+    GALPHA_CUDA(cudaMemcpyAsync(c.outtri, dt->triangles, sizeof(gpudtTriangle) * (size_t)dt->nTris,
+                                cudaMemcpyHostToDevice, c.stream));
+    launch_n(c, AosToSoa{c.outtri, c.cv, c.cn}, dt->nTris);
+    c.nT_out = dt->nTris;
+    c.have_mesh = true;
+    c.have_alpha = false;
+    r = stage_alpha(c);
+    if (r) return r;
+    c.have_alpha = true;
+    return download_alpha(c, out);
+}
+
+void galphaReleaseOutput(GAlphaOutput *out)
+{
+    if (!out) return;
+    free(out->spectrum);
+    free(out->point_list);
+    free(out->edge_list);
+    free(out->tri_list);
+    memset(out, 0, sizeof(*out));
+}
+
+// ------------------------------------------------------ reference entry points
+static galpha_ctx *g_default = nullptr;
+static std::mutex g_default_mu;
+
+static galpha_ctx *default_handle(int *status)
+{
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (!g_default) {
+        galphaHandle h = nullptr;
+        int r = galphaCreate(-1, 0, &h);
+        if (r) {
+            if (status) *status = r;
+            return nullptr;
+        }
+        g_default = h;
+    }
+    return g_default;
+}
+
+int gpudtComputeDTEx(const GPUDTPARAMS *pParam, GPUDTOUTPUT *pOutput, gpudtStatus *status)
+{
+    int r = GPUDT_OK;
+    galpha_ctx *h = default_handle(&r);
+    if (!h) {
+        if (status) {
+            memset(status, 0, sizeof(*status));
+            status->status = r;
+        }
+        return r;
+    }
+    if (!pOutput) return GPUDT_ERR_ARG;
+    pOutput->triangles = nullptr;
+    pOutput->nTris = 0;
+    return galphaTriangulate(h, pParam, pOutput, status);
+}
+
+PGPUDTOUTPUT gpudt_compute_dt(PGPUDTPARAMS pParam)
+{
+    PGPUDTOUTPUT out = new (std::nothrow) GPUDTOUTPUT;
+    if (!out) return nullptr;
+    out->triangles = nullptr;
+    out->nTris = 0;
+    gpudtStatus st;
+    int r = gpudtComputeDTEx(pParam, out, &st);
+    if (r) {
+        fprintf(stderr, "gpudtComputeDT failed: status %d (%s)\n", r, last_error_text());
+        delete[] out->triangles;
+        out->triangles = nullptr;
+        out->nTris = 0;
+    }
+    return out;
+}
+
+// As gpudt.cpp:926-929: frees the triangle array only.
+void gpudt_release_dt_output(PGPUDTOUTPUT pGpudtOutput)
+{
+    if (!pGpudtOutput) return;
+    delete[] pGpudtOutput->triangles;
+    pGpudtOutput->triangles = nullptr;
+}
+
+}  // extern "C"
+
+// C++-linkage symbols of the reference header (gpudt.h:131-132).
+PGPUDTOUTPUT gpudtComputeDT(PGPUDTPARAMS pParam) { return gpudt_compute_dt(pParam); }
+void gpudtReleaseDTOutput(PGPUDTOUTPUT pGpudtOutput) { gpudt_release_dt_output(pGpudtOutput); }

@@ -1,0 +1,419 @@
+// dt_grid.cu -- discrete Voronoi diagram and its dual triangles.
+//
+// Stage map (reference -> here):
+//   computeScalingFactors (gpudt.cpp:722-769)      grid_scaling: power-of-two aligned
+//                                                  scale/shift so every snapped
+//                                                  coordinate shift + g*scale is exact
+//   fake boundary circle (gpudt.cpp:810-832) and   fake ring: sites every <= 32 pixels on
+//   gpudtFixConvexHull (gpudt.cpp:349-647)          the texture border, inside the texture,
+//                                                  so the dual is closed by construction
+//                                                  and no host hull walk is needed
+//   kernelMapping / kernelMapPointsToTexture       SetupSites: snap, scatter the
+//   (cudaMain.cu:160-176, kernelVoronoi.h:56-74)    lowest index into an id map and a
+//                                                  column-major occupancy bitmap
+//   PBA phase 1 (pba2DKernel.h:90-206)             k_column_pass: nearest site per
+//                                                  column from 64-bit band masks
+//   PBA phases 2+3 + transposes                    k_row_pass: one CTA per row builds the
+//   (pba2DKernel.h:48-88, 209-478)                  lower envelope of the column candidates
+//                                                  in shared memory (exact integer
+//                                                  dominance) and colours the row
+//   cudaIslandDetection (cudaVoronoi.cu:220-307,   k_island_*: isolated pixels, iterated
+//   kernelVoronoi.h:82-191)                         on a work list, recoloured on device
+//   kernelFindRealVoronoiVertices + kernelFlood1D  k_emit_*: 2x2 windows with 3-4 colours
+//   + kernelCountRow/GenerateTriangles               give 1-2 counterclockwise triangles,
+//   (kernelVoronoi.h:196-270,                        written in window order through a
+//    cudaReconstruction.cu:134-208)                  tile-count scan (no host prefix sum)
+#include <cstdio>
+#include <cmath>
+#include <algorithm>
+#include "internal.cuh"
+#include "exact.cuh"
+
+namespace galpha {
+
+// ---------------------------------------------------------------- scaling
+// scale and shift are multiples of u = 2^e with scale/u < 2^37 and
+// |coordinate|/u < 2^51, so shift + g*scale is exact for |g| < 2^15.
+static void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale,
+                         double &sx, double &sy)
+{
+    int D = T - 2 * kMargin;  // usable pixels [kMargin, T-1-kMargin]
+    double range = std::max(maxX - minX, maxY - minY);
+    if (!(range > 0.0)) range = std::max(1.0, std::fabs(minX) + std::fabs(minY));
+    double scale0 = range / (D - 2);
+    double maxabs = std::max(std::max(std::fabs(minX), std::fabs(minY)), std::max(std::fabs(maxX), std::fabs(maxY)));
+    int es = std::ilogb(scale0) - 36;
+    int eb = maxabs > 0.0 ? std::ilogb(maxabs) - 50 : es;
+    int e = std::max(es, eb);
+    double u = std::ldexp(1.0, e);
+    scale = std::ceil(scale0 / u) * u;
+    sx = std::floor(minX / u) * u;
+    sy = std::floor(minY / u) * u;
+}
+
+struct RingPix {
+    int T, nside;
+    __host__ __device__ short2 operator()(int k) const
+    {
+        int side = k / nside, i = k % nside;
+        int off = (int)(((long long)i * (T - 1)) / nside);
+        switch (side) {
+        case 0: return make_short2((short)off, 0);
+        case 1: return make_short2((short)(T - 1), (short)off);
+        case 2: return make_short2((short)(T - 1 - off), (short)(T - 1));
+        default: return make_short2(0, (short)(T - 1 - off));
+        }
+    }
+};
+
+struct SetupSites {
+    const double *xy;
+    double2 *opos, *pos;
+    short2 *gpix;
+    int *idmap;
+    uint32_t *occ, *bandocc;
+    int8_t *vstate;
+    int *vtri, *vround, *anchor;
+    int N, T, logT, W2;
+    double scale, sx, sy, minX, minY, maxX, maxY;
+    RingPix ring;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        int v = (int)i;
+        double2 o, p;
+        int px, py;
+        if (v < N) {
+            o = make_double2(xy[2 * v], xy[2 * v + 1]);
+            if (!(o.x >= minX && o.x <= maxX && o.y >= minY && o.y <= maxY)) set_err(ct, GPUDT_ERR_ARG, v);
+            int D = T - 2 * kMargin;
+            double gx = floor((o.x - sx) / scale), gy = floor((o.y - sy) / scale);
+            int ix = (int)fmin(fmax(gx, 0.0), (double)(D - 1));
+            int iy = (int)fmin(fmax(gy, 0.0), (double)(D - 1));
+            p = make_double2(sx + ix * scale, sy + iy * scale);
+            px = ix + kMargin;
+            py = iy + kMargin;
+            vstate[v] = VS_UNDECIDED;
+        } else {
+            short2 q = ring(v - N);
+            px = q.x;
+            py = q.y;
+            p = make_double2(sx + (px - kMargin) * scale, sy + (py - kMargin) * scale);
+            o = p;
+            vstate[v] = VS_FAKE;
+        }
+        opos[v] = o;
+        pos[v] = p;
+        gpix[v] = make_short2((short)px, (short)py);
+        vtri[v] = -1;
+        vround[v] = v < N ? 0 : 1;  // fake ring sites never move: decided before round 2
+        anchor[v] = -1;
+        size_t pix = ((size_t)py << logT) + px;
+        idmap[pix] = v;
+        atomicOr(&occ[(size_t)px * (T >> 5) + (py >> 5)], 1u << (py & 31));
+        atomicOr(&bandocc[(size_t)px * W2 + (py >> 11)], 1u << ((py >> 6) & 31));
+    }
+};
+
+struct MinId {
+    const short2 *gpix;
+    int *idmap;
+    int logT;
+    __device__ void operator()(long long i) const
+    {
+        int v = (int)i;
+        short2 g = gpix[v];
+        int *slot = &idmap[((size_t)g.y << logT) + g.x];
+        if (*slot > v) atomicMin(slot, v);
+    }
+};
+
+struct ClassifySites {
+    const short2 *gpix;
+    const int *idmap;
+    int8_t *vstate;
+    int *anchor;
+    int logT;
+    __device__ void operator()(long long i) const
+    {
+        int v = (int)i;
+        short2 g = gpix[v];
+        int w = idmap[((size_t)g.y << logT) + g.x];
+        if (w != v) {
+            vstate[v] = VS_MISSING;
+            anchor[v] = w;
+        }
+    }
+};
+
+// ----------------------------------------------------------------- islands
+// A pixel is isolated when none of the (up to three) neighbours in the
+// direction of its site carries its colour (kernelVoronoi.h:133-191).
+__device__ __forceinline__ bool isolated(const int *colour, const short2 *gpix, int T, int logT, int x, int y)
+{
+    int c = colour[((size_t)y << logT) + x];
+    if (c < 0) return false;
+    short2 s = gpix[c];
+    int dx = (s.x > x) - (s.x < x), dy = (s.y > y) - (s.y < y);
+    if (dx == 0 && dy == 0) return false;
+    if (dx != 0 && colour[((size_t)y << logT) + x + dx] == c) return false;
+    if (dy != 0) {
+        if (colour[((size_t)(y + dy) << logT) + x] == c) return false;
+        if (dx != 0 && colour[((size_t)(y + dy) << logT) + x + dx] == c) return false;
+    }
+    return true;
+}
+
+struct IslandDetectAll {
+    const int *colour;
+    const short2 *gpix;
+    int *list;
+    Counters *ct;
+    int T, logT, cap;
+    __device__ void operator()(long long i) const
+    {
+        int x = (int)(i & (T - 1)), y = (int)(i >> logT);
+        if (isolated(colour, gpix, T, logT, x, y)) {
+            int k = atomicAdd(&ct->nlist, 1);
+            if (k < cap) list[k] = (int)i;
+            else set_err(ct, GPUDT_ERR_NOMEM, 1);
+        }
+    }
+};
+
+struct IslandMark {
+    int *colour;
+    const int *list;
+    int from;
+    __device__ void operator()(long long i) const { colour[list[from + i]] = -1; }
+};
+
+// Neighbours of newly marked pixels may now be isolated.
+struct IslandDetectNear {
+    const int *colour;
+    const short2 *gpix;
+    int *list;
+    Counters *ct;
+    int T, logT, from, cap;
+    __device__ void operator()(long long i) const
+    {
+        int p = list[from + i];
+        int x = p & (T - 1), y = p >> logT;
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                int xx = x + dx, yy = y + dy;
+                if ((dx == 0 && dy == 0) || xx < 0 || yy < 0 || xx >= T || yy >= T) continue;
+                if (isolated(colour, gpix, T, logT, xx, yy)) {
+                    // a pixel next to several new islands is listed once per
+                    // neighbour; the set (not the multiplicity) is what matters
+                    int q = (yy << logT) + xx;
+                    int k = atomicAdd(&ct->nlist, 1);
+                    if (k < cap) list[k] = q;
+                    else set_err(ct, GPUDT_ERR_NOMEM, 2);
+                }
+            }
+    }
+};
+
+// Recolour: an unassigned pixel takes, among its assigned 8-neighbours, the
+// colour whose site is nearest to it (ties: lower id).  Jacobi rounds.
+struct IslandPropose {
+    const int *colour;
+    const short2 *gpix;
+    const int *list;
+    int *cand;
+    Counters *ct;
+    int T, logT;
+    __device__ void operator()(long long i) const
+    {
+        int p = list[i];
+        if (colour[p] >= 0) {
+            cand[i] = colour[p];
+            return;
+        }
+        int x = p & (T - 1), y = p >> logT;
+        long long best = -1;
+        int bestc = -1;
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                int xx = x + dx, yy = y + dy;
+                if ((dx == 0 && dy == 0) || xx < 0 || yy < 0 || xx >= T || yy >= T) continue;
+                int c = colour[((size_t)yy << logT) + xx];
+                if (c < 0) continue;
+                short2 s = gpix[c];
+                long long d = (long long)(s.x - x) * (s.x - x) + (long long)(s.y - y) * (s.y - y);
+                if (bestc < 0 || d < best || (d == best && c < bestc)) {
+                    best = d;
+                    bestc = c;
+                }
+            }
+        cand[i] = bestc;
+        if (bestc < 0) atomicAdd(&ct->changed, 1);
+    }
+};
+
+struct IslandApply {
+    int *colour;
+    const int *list;
+    const int *cand;
+    __device__ void operator()(long long i) const { colour[list[i]] = cand[i]; }
+};
+
+// ------------------------------------------------- degenerate input check
+// An input with fewer than 3 distinct points, or with all points collinear,
+// has no triangle; the pipeline is skipped for it.
+struct FirstDistinct {
+    const double *xy;
+    int *out;
+    __device__ void operator()(long long i) const
+    {
+        if (xy[2 * i] != xy[0] || xy[2 * i + 1] != xy[1]) atomicMin(out, (int)i);
+    }
+};
+
+struct CountOffLine {
+    const double *xy;
+    const int *b;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        int j = *b;
+        int s = orient2d_filter(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
+        if (s == 2) s = orient2d_exact(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
+        if (s != 0) atomicAdd(&ct->changed, 1);
+    }
+};
+
+// Returns 1 when the input has at least one triangle.
+int has_triangles(Ctx &c, const double *d_xy, int n)
+{
+    if (n < 3) return 0;
+    int *first = c.aux;
+    int big = 0x7fffffff;
+    GALPHA_CUDA(cudaMemcpyAsync(first, &big, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+    launch_n(c, FirstDistinct{d_xy, first}, n);
+    int hfirst = 0;
+    GALPHA_CUDA(cudaMemcpyAsync(&hfirst, first, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    if (hfirst == 0x7fffffff) return 0;
+    launch_n(c, CountOffLine{d_xy, first, c.ctr}, n);
+    int r = read_counters(c);
+    if (r) return r;
+    return c.hctr->changed > 0 ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ stages
+int stage_setup(Ctx &c, const double *d_xy, int n, double minX, double minY, double maxX, double maxY, int T)
+{
+    c.N = n;
+    c.T = T;
+    c.logT = 0;
+    while ((1 << c.logT) < T) c.logT++;
+    int nside = (T - 1 + kFakeSpacing - 1) / kFakeSpacing;
+    c.F = 4 * nside;
+    c.V = c.N + c.F;
+    grid_scaling(minX, minY, maxX, maxY, T, c.scale, c.shiftX, c.shiftY);
+    int W2 = ((T >> 6) + 31) / 32;
+    GALPHA_CUDA(cudaMemsetAsync(c.occ, 0, sizeof(uint32_t) * (size_t)T * (T >> 5), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.bandocc, 0, sizeof(uint32_t) * (size_t)T * W2, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.ctr, 0, sizeof(Counters), c.stream));
+    SetupSites s;
+    s.xy = d_xy;
+    s.opos = c.opos;
+    s.pos = c.pos;
+    s.gpix = c.gpix;
+    s.idmap = c.idmap;
+    s.occ = c.occ;
+    s.bandocc = c.bandocc;
+    s.vstate = c.vstate;
+    s.vtri = c.vtri;
+    s.vround = c.vround;
+    s.anchor = c.anchor;
+    s.N = c.N;
+    s.T = T;
+    s.logT = c.logT;
+    s.W2 = W2;
+    s.scale = c.scale;
+    s.sx = c.shiftX;
+    s.sy = c.shiftY;
+    s.minX = minX;
+    s.minY = minY;
+    s.maxX = maxX;
+    s.maxY = maxY;
+    s.ring = RingPix{T, nside};
+    s.ct = c.ctr;
+    launch_n(c, s, c.V);
+    launch_n(c, MinId{c.gpix, c.idmap, c.logT}, c.N);
+    launch_n(c, ClassifySites{c.gpix, c.idmap, c.vstate, c.anchor, c.logT}, c.N);
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
+int stage_voronoi(Ctx &c)
+{
+    const int T = c.T;
+    int W2 = ((T >> 6) + 31) / 32;
+    int r0 = launch_column_pass(c, W2);
+    if (r0) return r0;
+    r0 = launch_row_pass(c);
+    if (r0) return r0;
+    GALPHA_CUDA(cudaGetLastError());
+    // islands
+    long long npix = (long long)T * T;
+    int cap = (int)std::min<long long>(npix, (long long)c.cap_tris * 3);
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    launch_n(c, IslandDetectAll{c.colour, c.gpix, c.list, c.ctr, T, c.logT, cap}, npix);
+    int r = read_counters(c);
+    if (r) return r;
+    int total = c.hctr->nlist;
+    c.st.nIslandPixels = total;
+    if (total == 0) return GPUDT_OK;
+    // iterate detection around newly marked pixels
+    int from = 0, to = total, guard = 0;
+    while (from < to) {
+        if (to > cap) return GPUDT_ERR_NOMEM;
+        launch_n(c, IslandMark{c.colour, c.list, from}, to - from);
+        launch_n(c, IslandDetectNear{c.colour, c.gpix, c.list, c.ctr, T, c.logT, from, cap},
+                 to - from);
+        r = read_counters(c);
+        if (r) return r;
+        from = to;
+        to = c.hctr->nlist;
+        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    total = to;
+    c.st.nIslandPixels = total;
+    // recolour
+    guard = 0;
+    while (true) {
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+        launch_n(c, IslandPropose{c.colour, c.gpix, c.list, c.list2, c.ctr, T, c.logT}, total);
+        launch_n(c, IslandApply{c.colour, c.list, c.list2}, total);
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->changed == 0) break;
+        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    return GPUDT_OK;
+}
+
+int stage_triangles(Ctx &c)
+{
+    const int T = c.T;
+    long long nwin = (long long)(T - 1) * (T - 1);
+    int ntiles = (int)((nwin + kEmitTile - 1) / kEmitTile);
+    int r0 = launch_emit(c, ntiles, nwin, false);
+    if (r0) return r0;
+    int r = exclusive_scan_int(c, c.tilecount, c.tilecount, ntiles, &c.ctr->ntris);
+    if (r) return r;
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->err) return c.hctr->err;
+    if (c.hctr->ntris > c.cap_tris) return GPUDT_ERR_NOMEM;
+    r = launch_emit(c, ntiles, nwin, true);
+    if (r) return r;
+    return GPUDT_OK;
+}
+
+}  // namespace galpha

@@ -1,0 +1,1387 @@
+// dt_mesh.cu -- mesh stages of the Delaunay pipeline, all on the device.
+//
+// Stage map (reference -> here):
+//   cpuVertexArray + kernelFindNextTriangles      stage_links: per-vertex incidence lists
+//   (cudaReconstruction.cu:348-436; a host pass)   (count / scan / fill) and a matching
+//                                                  kernel; validates the mesh (one
+//                                                  triangle per directed edge, the hull is
+//                                                  exactly the fake ring)
+//   kernelDetectShifting / kernelShiftable         stage_shift: a site moves from its grid
+//   (cudaReconstruction.cu:241-341,                 position to its true position when its
+//    cudaShifting.cu:117-170)                       whole fan stays counterclockwise; rounds
+//                                                  of local priority minima (hashed ids)
+//   kernelDetectBadCases / DeleteTriangles /       stage_shift (second half): unshiftable
+//   FixVertexArray / PatchHoles /                   sites are removed; one thread clips the
+//   UpdateTriangleLinks (cudaShifting.cu:175-488)   star hole around the site's kernel point
+//   kernelLocateTriangleContainer ... kernel       stage_missing: straight-line walk with
+//   UpdateMissingTriangleLinks (cudaMissing.cu:     exact orientation, 1->3 / 2->4 splits,
+//   166-527)                                        exact duplicates dropped (lowest id kept)
+//   cudaFixBoundary (cudaBoundary.cu:106-608)      stage_boundary: fake ring sites removed
+//                                                  in priority rounds, pockets patched with
+//                                                  the ccw>0 stack rule, then reflex hull
+//                                                  vertices filled so the hull is convex
+//   cudaFlipping (cudaFlipping.cu:227-685) +       stage_flip: Lawson flips with exact
+//   host gpudtRecursiveFlip (gpudt.cpp:191-304,     in-circle on device, min-id voting, an
+//   879-914)                                        active work list; no host fix-up
+//   kernelMarkValidTriangles1 ... FixIndices1      stage_compact: scan-compaction of live
+//   (cudaMissing.cu:529-617, cudaBoundary.cu)       slots, links remapped, AoS output
+//
+// Concurrent local operations in one round (hole patches, splits, flips) use a
+// two-phase relink: phase 1 writes each operation's own new triangles, records
+// where every outer edge went (fwd[] of the consumed slot, epoch[] = round) and
+// appends (new location, old outer link) records; phase 2 resolves each record
+// against the forwarding of the neighbour if that neighbour was consumed in the
+// same round, else writes the neighbour's back-link.  No operation ever writes
+// a triangle owned by another operation of the same round.
+#include <cstdio>
+#include <algorithm>
+#include "internal.cuh"
+#include "exact.cuh"
+
+namespace galpha {
+
+// ------------------------------------------------------------ small helpers
+__device__ __forceinline__ int orientv(const double2 *P, int a, int b, int c, Counters *ct)
+{
+    double2 A = P[a], B = P[b], C = P[c];
+    int s = orient2d_filter(A.x, A.y, B.x, B.y, C.x, C.y);
+    if (s != 2) return s;
+    atomicAdd(&ct->exact_orient, 1ull);
+    s = orient2d_exact(A.x, A.y, B.x, B.y, C.x, C.y);
+    if (s == EXACT_OVERFLOW) {
+        set_err(ct, GPUDT_ERR_EXACT, 1);
+        return 0;
+    }
+    return s;
+}
+
+__device__ __forceinline__ int orientp(double2 A, double2 B, double2 C, Counters *ct)
+{
+    int s = orient2d_filter(A.x, A.y, B.x, B.y, C.x, C.y);
+    if (s != 2) return s;
+    atomicAdd(&ct->exact_orient, 1ull);
+    s = orient2d_exact(A.x, A.y, B.x, B.y, C.x, C.y);
+    if (s == EXACT_OVERFLOW) {
+        set_err(ct, GPUDT_ERR_EXACT, 2);
+        return 0;
+    }
+    return s;
+}
+
+__device__ __forceinline__ int4 ldv(const int4 *tv, int t) { return tv[t]; }
+
+__device__ __forceinline__ void set_link(int4 *tn, int loc, int val)
+{
+    int *p = (int *)&tn[dtri(loc)];
+    p[dori(loc)] = val;
+}
+
+__device__ __forceinline__ int get_link(const int4 *tn, int loc)
+{
+    const int *p = (const int *)&tn[dtri(loc)];
+    return p[dori(loc)];
+}
+
+__device__ __forceinline__ void push_rec(Relink *rec, Counters *ct, int loc, int old)
+{
+    int k = atomicAdd(&ct->nrec, 1);
+    rec[k] = Relink{loc, old};
+}
+
+__device__ __forceinline__ void set_fwd(int4 *fwd, int t, int i, int loc)
+{
+    int *p = (int *)&fwd[t];
+    p[i] = loc;
+}
+
+__device__ __forceinline__ int alloc_slot(int *freelist, Counters *ct)
+{
+    int k = atomicSub(&ct->nfree, 1) - 1;
+    if (k >= 0) return freelist[k];
+    return atomicAdd(&ct->ntris, 1);
+}
+
+__device__ __forceinline__ void free_slot(int4 *tv, int *freelist, Counters *ct, int t)
+{
+    tv[t] = make_int4(-1, -1, -1, 0);
+    int k = atomicAdd(&ct->nfree, 1);
+    freelist[k] = t;
+}
+
+// ------------------------------------------------------------------- links
+struct CountDeg {
+    const int4 *tv;
+    int *deg;
+    __device__ void operator()(long long i) const
+    {
+        int4 v = tv[i];
+        atomicAdd(&deg[v.x], 1);
+        atomicAdd(&deg[v.y], 1);
+        atomicAdd(&deg[v.z], 1);
+    }
+};
+
+struct FillInc {
+    const int4 *tv;
+    const int *start;
+    int *cursor, *inc;
+    __device__ void operator()(long long i) const
+    {
+        int t = (int)i;
+        int4 v = tv[t];
+        int a[3] = {v.x, v.y, v.z};
+        for (int k = 0; k < 3; k++) {
+            int s = start[a[k]] + atomicAdd(&cursor[a[k]], 1);
+            inc[s] = enc(t, k);
+        }
+    }
+};
+
+struct MatchLinks {
+    const int4 *tv;
+    int4 *tn;
+    const int *start, *inc;
+    int *vtri;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        int t = (int)i;
+        int4 v = tv[t];
+        int n[3];
+        for (int k = 0; k < 3; k++) {
+            int a = geti(v, p1(k)), b = geti(v, m1(k));  // edge a -> b, opposite vtx[k]
+            int found = -1, cnt = 0, same = 0;
+            for (int s = start[b]; s < start[b + 1]; s++) {
+                int e = inc[s], u = dtri(e), j = dori(e);
+                int4 w = tv[u];
+                if (geti(w, p1(j)) == a) {  // u has b -> a
+                    found = enc(u, m1(j));
+                    cnt++;
+                }
+            }
+            for (int s = start[a]; s < start[a + 1]; s++) {
+                int e = inc[s], u = dtri(e), j = dori(e);
+                if (geti(tv[u], p1(j)) == b) same++;  // triangles with a -> b
+            }
+            if (cnt > 1 || same != 1) set_err(ct, GPUDT_ERR_TOPOLOGY, 20);
+            if (found < 0) atomicAdd(&ct->changed, 1);  // hull edge
+            n[k] = found;
+            if (k == 0) vtri[v.x] = enc(t, 0);
+        }
+        tn[t] = make_int4(n[0], n[1], n[2], 0);
+    }
+};
+
+struct SetVtri {
+    const int4 *tv;
+    int *vtri;
+    __device__ void operator()(long long i) const
+    {
+        int t = (int)i;
+        int4 v = tv[t];
+        vtri[v.x] = enc(t, 0);
+        vtri[v.y] = enc(t, 1);
+        vtri[v.z] = enc(t, 2);
+    }
+};
+
+int stage_links(Ctx &c)
+{
+    int r = read_counters(c);
+    if (r) return r;
+    int nt = c.hctr->ntris;
+    int *deg = c.deg;       // [V+1]
+    int *start = c.aux2;    // [V+1]
+    GALPHA_CUDA(cudaMemsetAsync(deg, 0, sizeof(int) * (size_t)(c.V + 1), c.stream));
+    launch_n(c, CountDeg{c.tv, deg}, nt);
+    r = exclusive_scan_int(c, deg, start, c.V + 1, nullptr);
+    if (r) return r;
+    GALPHA_CUDA(cudaMemsetAsync(deg, 0, sizeof(int) * (size_t)(c.V + 1), c.stream));
+    launch_n(c, FillInc{c.tv, start, deg, c.inc}, nt);
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+    launch_n(c, MatchLinks{c.tv, c.tn, start, c.inc, c.vtri, c.ctr}, nt);
+    launch_n(c, SetVtri{c.tv, c.vtri}, nt);
+    GALPHA_CUDA(cudaGetLastError());
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->err) return c.hctr->err;
+    // the only hull edges are the F edges of the fake ring
+    if (c.hctr->changed != c.F) {
+        c.hctr->errinfo = c.hctr->changed;
+        return GPUDT_ERR_TOPOLOGY;
+    }
+    return GPUDT_OK;
+}
+
+// ------------------------------------------------------------------- relink
+struct Relinker {
+    int4 *tn;
+    const int4 *fwd;
+    const int *epoch;
+    const Relink *rec;
+    const int4 *tv;
+    int *vtri;
+    int round;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        Relink r = rec[i];
+        if (r.old < 0) {
+            if (r.loc >= 0) set_link(tn, r.loc, -1);
+            return;
+        }
+        int u = dtri(r.old), b = dori(r.old);
+        if (epoch[u] == round) {
+            const int *f = (const int *)&fwd[u];
+            int there = f[b];
+            if (r.loc >= 0) set_link(tn, r.loc, there);
+            else if (there < 0) set_err(ct, GPUDT_ERR_TOPOLOGY, 30);  // both sides became hull
+        } else {
+            if (r.loc >= 0) set_link(tn, r.loc, r.old);
+            int *p = (int *)&tn[u];
+            p[b] = r.loc;  // -1 when the edge became a hull edge
+            if (r.loc < 0) {
+                int4 w = tv[u];
+                vtri[geti(w, p1(b))] = enc(u, p1(b));
+                vtri[geti(w, m1(b))] = enc(u, m1(b));
+            }
+        }
+    }
+};
+
+static int run_relink(Ctx &c, int round, int nrec)
+{
+    launch_n(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, nrec);
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
+// Host-side epoch counter: every operation round gets a fresh id.
+static int next_round(Ctx &c)
+{
+    static thread_local int counter = 1;
+    return ++counter;
+}
+
+// ------------------------------------------------------------------- shift
+// A fan walk around interior vertex v: calls f(t, i, a, b) for every
+// triangle (v, a, b) counterclockwise; returns false on a fan over kMaxFan*4.
+template <class Fn>
+__device__ __forceinline__ bool walk_fan(const int4 *tv, const int4 *tn, int start, Fn f)
+{
+    int e = start;
+    for (int guard = 0; guard < 4 * kMaxFan; guard++) {
+        int t = dtri(e), i = dori(e);
+        int4 w = tv[t];
+        if (!f(t, i, geti(w, p1(i)), geti(w, m1(i)))) return true;
+        int nx = geti(tn[t], p1(i));  // across (b, v)
+        if (nx < 0) return true;
+        e = enc(dtri(nx), p1(dori(nx)));
+        if (e == start) return true;
+    }
+    return false;
+}
+
+struct ShiftRound {
+    const int4 *tv, *tn;
+    double2 *pos;
+    const double2 *opos;
+    int8_t *vstate;
+    int *vround;
+    const int *vtri;
+    int round;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int v = (int)ii;
+        if (vstate[v] != VS_UNDECIDED) return;
+        uint32_t pv = prio((uint32_t)v);
+        bool wait = false, ok = true;
+        double2 q = opos[v];
+        bool fine = walk_fan(tv, tn, vtri[v], [&](int t, int i, int a, int b) {
+            int ra = vround[a];
+            if ((ra == 0 || ra == round) && prio((uint32_t)a) < pv) {
+                wait = true;
+                return false;
+            }
+            if (ok && orientp(q, pos[a], pos[b], ct) <= 0) ok = false;
+            return true;
+        });
+        if (!fine) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 40);
+            return;
+        }
+        if (wait) {
+            atomicAdd(&ct->nlist, 1);
+            return;
+        }
+        vround[v] = round;
+        if (ok) {
+            pos[v] = q;
+            vstate[v] = VS_SHIFTED;
+        } else {
+            vstate[v] = VS_BAD;
+            atomicAdd(&ct->changed, 1);
+        }
+    }
+};
+
+// Select BAD vertices that are the priority minimum among their BAD neighbours.
+struct BadSelect {
+    const int4 *tv, *tn;
+    const int8_t *vstate;
+    const int *vtri;
+    int *list;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int v = (int)ii;
+        if (vstate[v] != VS_BAD) return;
+        uint32_t pv = prio((uint32_t)v);
+        bool wait = false;
+        walk_fan(tv, tn, vtri[v], [&](int t, int i, int a, int b) {
+            if (vstate[a] == VS_BAD && prio((uint32_t)a) < pv) {
+                wait = true;
+                return false;
+            }
+            return true;
+        });
+        if (wait) return;
+        int k = atomicAdd(&ct->nlist, 1);
+        list[k] = v;
+    }
+};
+
+// Remove vertex v (interior) and triangulate its star hole by ear clipping
+// with the kernel point K = pos[v] (cudaShifting.cu:350-450 semantics: an ear
+// (A,B,C) is cut when ccw(A,B,C) > 0 and K is strictly left of A->C).
+struct BadRemove {
+    int4 *tv, *tn, *fwd;
+    int *epoch, *freelist, *vtri, *anchor;
+    const int *list;
+    double2 *pos;
+    int8_t *vstate;
+    Relink *rec;
+    int round, nreal;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int v = list[ii];
+        int U[kMaxFan], Fs[kMaxFan], Fi[kMaxFan], O[kMaxFan];
+        int d = 0;
+        bool over = false;
+        bool fine = walk_fan(tv, tn, vtri[v], [&](int t, int i, int a, int b) {
+            if (d >= kMaxFan) {
+                over = true;
+                return false;
+            }
+            U[d] = a;
+            Fs[d] = t;
+            Fi[d] = i;
+            O[d] = geti(tn[t], i);
+            d++;
+            return true;
+        });
+        if (!fine || over || d < 3) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 50);
+            return;
+        }
+        double2 K = pos[v];
+        // polygon ring with owners of each current edge (U[k] -> U[next])
+        int nxt[kMaxFan], prv[kMaxFan], own[kMaxFan];  // own: -2-k original edge k, else loc
+        for (int k = 0; k < d; k++) {
+            nxt[k] = (k + 1) % d;
+            prv[k] = (k + d - 1) % d;
+            own[k] = -2 - k;
+        }
+        int used = 0, remaining = d, cur = 0, stall = 0;
+        auto owner_link = [&](int ownv, int loc) {
+            if (ownv <= -2) {
+                int k = -2 - ownv;
+                set_fwd(fwd, Fs[k], Fi[k], loc);
+                push_rec(rec, ct, loc, O[k]);
+            } else {
+                set_link(tn, loc, ownv);
+                set_link(tn, ownv, loc);
+            }
+        };
+        for (int k = 0; k < d; k++) epoch[Fs[k]] = round;
+        // strict pass first (K strictly inside what remains); when a full
+        // cycle finds no such ear, K lies on a candidate diagonal and the
+        // closed test is used (the rest stays star-shaped from K)
+        bool strict = true;
+        while (remaining > 3) {
+            int A = prv[cur], B = cur, C = nxt[cur];
+            bool ear = orientp(pos[U[A]], pos[U[B]], pos[U[C]], ct) > 0;
+            if (ear && remaining > 4) {
+                int k = orientp(pos[U[A]], pos[U[C]], K, ct);
+                ear = strict ? k > 0 : k >= 0;
+            } else if (ear) {
+                // last quad: any diagonal giving two counterclockwise triangles
+                int D = nxt[C];
+                ear = orientp(pos[U[A]], pos[U[C]], pos[U[D]], ct) > 0;
+            }
+            if (ear) {
+                int s = Fs[used++];
+                tv[s] = make_int4(U[A], U[B], U[C], 0);
+                tn[s] = make_int4(-1, -1, -1, 0);
+                // edges: opp A (0) = B->C owned by own[B]; opp C (2) = A->B owned by own[A];
+                // opp B (1) = C->A: the new diagonal, owner of ring edge A->C
+                owner_link(own[B], enc(s, 0));
+                owner_link(own[A], enc(s, 2));
+                own[A] = enc(s, 1);
+                vtri[U[A]] = enc(s, 0);
+                vtri[U[B]] = enc(s, 1);
+                vtri[U[C]] = enc(s, 2);
+                nxt[A] = C;
+                prv[C] = A;
+                remaining--;
+                cur = C;
+                stall = 0;
+                strict = true;
+            } else {
+                cur = nxt[cur];
+                if (++stall > remaining + 1) {
+                    if (strict) {
+                        strict = false;
+                        stall = 0;
+                        continue;
+                    }
+                    set_err(ct, GPUDT_ERR_TOPOLOGY, 51);
+                    return;
+                }
+            }
+        }
+        {
+            int A = cur, B = nxt[cur], C = nxt[nxt[cur]];
+            if (orientp(pos[U[A]], pos[U[B]], pos[U[C]], ct) <= 0) {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 52);
+                return;
+            }
+            int s = Fs[used++];
+            tv[s] = make_int4(U[A], U[B], U[C], 0);
+            tn[s] = make_int4(-1, -1, -1, 0);
+            owner_link(own[B], enc(s, 0));
+            owner_link(own[C], enc(s, 1));
+            owner_link(own[A], enc(s, 2));
+            vtri[U[A]] = enc(s, 0);
+            vtri[U[B]] = enc(s, 1);
+            vtri[U[C]] = enc(s, 2);
+        }
+        for (int k = used; k < d; k++) free_slot(tv, freelist, ct, Fs[k]);
+        int an = U[0];
+        for (int k = 0; k < d; k++)
+            if (U[k] < nreal) {
+                an = U[k];
+                break;
+            }
+        vtri[v] = -1;
+        vstate[v] = VS_MISSING;
+        anchor[v] = an;
+    }
+};
+
+struct CountState {
+    const int8_t *vstate;
+    int8_t s;
+    int *list;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        if (vstate[i] == s) {
+            int k = atomicAdd(&ct->nlist, 1);
+            if (list) list[k] = (int)i;
+        }
+    }
+};
+
+static int run_counts(Ctx &c) { return read_counters(c); }
+
+int stage_shift(Ctx &c)
+{
+    int r;
+    // vertices fixed from the start (fake ring) count as decided in round 1
+    int shiftRounds = 0, badCount = 0;
+    for (int round = 2;; round++) {
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int) + 0, c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+        launch_n(c, ShiftRound{c.tv, c.tn, c.pos, c.opos, c.vstate, c.vround, c.vtri, round, c.ctr}, c.N);
+        r = run_counts(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        shiftRounds++;
+        badCount += c.hctr->changed;
+        if (c.hctr->nlist == 0) break;
+        if (shiftRounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    c.st.shiftRounds = shiftRounds;
+    c.st.nBadShift = badCount;
+    // remove the unshiftable sites in independent rounds
+    int guard = 0;
+    while (badCount > 0) {
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+        launch_n(c, BadSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.ctr}, c.N);
+        r = run_counts(c);
+        if (r) return r;
+        int nsel = c.hctr->nlist;
+        if (nsel == 0) break;
+        int round = next_round(c);
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
+        launch_n(c, BadRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.anchor, c.list, c.pos, c.vstate,
+                              c.rec, round, c.N, c.ctr},
+                 nsel);
+        r = run_counts(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        r = run_relink(c, round, c.hctr->nrec);
+        if (r) return r;
+        badCount -= nsel;
+        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    return GPUDT_OK;
+}
+
+// ----------------------------------------------------------------- missing
+// Straight-line walk from vertex a to point q.  Returns the triangle and the
+// location kind: 0 inside, 1 on the edge opposite vtx[k] (k in *edge),
+// 2 on vertex vtx[k] (coincident), -1 failure.
+__device__ int locate(const int4 *tv, const int4 *tn, const double2 *P, const int *vtri, int a, double2 q,
+                      int *tri, int *edge, Counters *ct)
+{
+    int budget = 1 << 22;  // total walk steps over all restarts
+    for (int restart = 0; restart < 4096; restart++) {
+        double2 A = P[a];
+        if (A.x == q.x && A.y == q.y) {
+            int e = vtri[a];
+            *tri = dtri(e);
+            *edge = dori(e);
+            return 2;
+        }
+        // 1. wedge of a containing q: counterclockwise from vtri[a]; a hull
+        //    vertex's fan is open, so the clockwise side is searched after
+        int e = vtri[a], t = -1, ia = 0;
+        for (int dir = 0; dir < 2 && t < 0; dir++) {
+            e = vtri[a];
+            for (int guard = 0; guard < 4 * kMaxFan; guard++) {
+                int tt = dtri(e), i = dori(e);
+                int4 w = tv[tt];
+                int b = geti(w, p1(i)), c = geti(w, m1(i));
+                if (orientp(A, P[b], q, ct) >= 0 && orientp(A, P[c], q, ct) <= 0) {
+                    t = tt;
+                    ia = i;
+                    break;
+                }
+                int nx = dir == 0 ? geti(tn[tt], p1(i)) : geti(tn[tt], m1(i));
+                if (nx < 0) break;
+                e = dir == 0 ? enc(dtri(nx), p1(dori(nx))) : enc(dtri(nx), m1(dori(nx)));
+                if (e == vtri[a]) break;
+            }
+        }
+        if (t < 0) return -1;
+        // 2. walk along a -> q
+        int4 w = tv[t];
+        int b = geti(w, p1(ia)), c = geti(w, m1(ia));
+        int cross = ia;  // index (in t) of the vertex opposite the edge to cross
+        if (orientp(P[b], P[c], q, ct) >= 0) {
+            goto classify_t;
+        }
+        for (; budget > 0; budget--) {
+            // cross edge (b, c) of t (opposite vtx[cross]); b right of a->q, c left
+            int nx = geti(tn[t], cross);
+            if (nx < 0) return -1;
+            t = dtri(nx);
+            int j = dori(nx);
+            w = tv[t];
+            int d = geti(w, j);  // new triangle (d, c, b)
+            int o1 = orientp(P[b], P[d], q, ct), o2 = orientp(P[d], P[c], q, ct);
+            if (o1 >= 0 && o2 >= 0) goto classify_t;
+            int od = orientp(A, q, P[d], ct);
+            if (od > 0) {
+                // exit through (b, d): opposite c = vtx[p1(j)]
+                c = d;
+                cross = p1(j);
+            } else if (od < 0) {
+                // exit through (d, c): opposite b = vtx[m1(j)]
+                b = d;
+                cross = m1(j);
+            } else {
+                a = d;  // the walk runs through vertex d: restart there
+                goto next_restart;
+            }
+        }
+        return -1;
+    classify_t: {
+        int4 v = tv[t];
+        int x[3] = {v.x, v.y, v.z};
+        int o[3], zeros = 0, zk = -1, nzk = -1;
+        for (int k = 0; k < 3; k++) {
+            o[k] = orientp(P[x[p1(k)]], P[x[m1(k)]], q, ct);
+            if (o[k] < 0) return -1;
+            if (o[k] == 0) {
+                zeros++;
+                zk = k;
+            } else {
+                nzk = k;
+            }
+        }
+        *tri = t;
+        if (zeros == 0) {
+            *edge = 0;
+            return 0;
+        }
+        if (zeros == 1) {
+            *edge = zk;
+            return 1;
+        }
+        *edge = nzk;
+        return 2;
+    }
+    next_restart:;
+    }
+    return -1;
+}
+
+struct MissingLocate {
+    const int4 *tv, *tn;
+    const double2 *pos, *opos;
+    const int *vtri, *anchor;
+    int8_t *vstate;
+    const int *list;
+    int *loc;  // [nlist] encoded (t<<2)|edge, kind in bit 30..31 via separate array
+    int *kind;
+    int *vote;
+    int fallback;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int m = list[ii];
+        if (vstate[m] != VS_MISSING) {
+            kind[ii] = -1;
+            return;
+        }
+        int a = anchor[m];
+        for (int g = 0; g < 64 && a >= 0 && vtri[a] < 0; g++) a = anchor[a];
+        if (a < 0 || vtri[a] < 0) a = fallback;
+        int t, e;
+        int k = locate(tv, tn, pos, vtri, a, opos[m], &t, &e, ct);
+        kind[ii] = k;
+        if (k < 0) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 60);
+            return;
+        }
+        loc[ii] = enc(t, e);
+        if (k == 2) return;
+        atomicMin(&vote[t], m);
+        if (k == 1) {
+            int nb = geti(tn[t], e);
+            if (nb < 0) {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 61);
+                return;
+            }
+            atomicMin(&vote[dtri(nb)], m);
+        }
+    }
+};
+
+struct MissingInsert {
+    int4 *tv, *tn, *fwd;
+    int *epoch, *freelist, *vtri, *vote;
+    double2 *pos;
+    const double2 *opos;
+    int8_t *vstate;
+    const int *list, *loc, *kind;
+    Relink *rec;
+    int round;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int k = kind[ii];
+        if (k < 0) return;
+        int p = list[ii];
+        int t = dtri(loc[ii]), i = dori(loc[ii]);
+        if (k == 2) {
+            vstate[p] = VS_DUP;
+            atomicAdd(&ct->changed, 1);
+            return;
+        }
+        if (vote[t] != p) return;
+        int4 v = tv[t], n = tn[t];
+        if (k == 0) {
+            int v0 = v.x, v1 = v.y, v2 = v.z;
+            int s1 = alloc_slot(freelist, ct), s2 = alloc_slot(freelist, ct);
+            epoch[t] = round;
+            tv[t] = make_int4(p, v1, v2, 0);
+            tv[s1] = make_int4(p, v2, v0, 0);
+            tv[s2] = make_int4(p, v0, v1, 0);
+            tn[t] = make_int4(-1, enc(s1, 2), enc(s2, 1), 0);
+            tn[s1] = make_int4(-1, enc(s2, 2), enc(t, 1), 0);
+            tn[s2] = make_int4(-1, enc(t, 2), enc(s1, 1), 0);
+            fwd[t] = make_int4(enc(t, 0), enc(s1, 0), enc(s2, 0), 0);
+            push_rec(rec, ct, enc(t, 0), n.x);
+            push_rec(rec, ct, enc(s1, 0), n.y);
+            push_rec(rec, ct, enc(s2, 0), n.z);
+            vtri[p] = enc(t, 0);
+            vtri[v1] = enc(t, 1);
+            vtri[v2] = enc(t, 2);
+            vtri[v0] = enc(s1, 2);
+        } else {
+            int o0 = geti(n, i);
+            int u = dtri(o0), j = dori(o0);
+            if (vote[u] != p) return;
+            int v0 = geti(v, i), v1 = geti(v, p1(i)), v2 = geti(v, m1(i));
+            int o1 = geti(n, p1(i)), o2 = geti(n, m1(i));
+            int4 wv = tv[u], wn = tn[u];
+            int w = geti(wv, j);
+            int ou1 = geti(wn, p1(j)), ou2 = geti(wn, m1(j));
+            int s1 = alloc_slot(freelist, ct), s2 = alloc_slot(freelist, ct);
+            epoch[t] = round;
+            epoch[u] = round;
+            // A = t (p,v2,v0), B = s1 (p,v0,v1), C = u (p,v1,w), D = s2 (p,w,v2)
+            tv[t] = make_int4(p, v2, v0, 0);
+            tv[s1] = make_int4(p, v0, v1, 0);
+            tv[u] = make_int4(p, v1, w, 0);
+            tv[s2] = make_int4(p, w, v2, 0);
+            tn[t] = make_int4(-1, enc(s1, 2), enc(s2, 1), 0);
+            tn[s1] = make_int4(-1, enc(u, 2), enc(t, 1), 0);
+            tn[u] = make_int4(-1, enc(s2, 2), enc(s1, 1), 0);
+            tn[s2] = make_int4(-1, enc(t, 2), enc(u, 1), 0);
+            int4 ft = make_int4(0, 0, 0, 0), fu = make_int4(0, 0, 0, 0);
+            seti(ft, i, -1);
+            seti(ft, p1(i), enc(t, 0));
+            seti(ft, m1(i), enc(s1, 0));
+            seti(fu, j, -1);
+            seti(fu, p1(j), enc(u, 0));
+            seti(fu, m1(j), enc(s2, 0));
+            fwd[t] = ft;
+            fwd[u] = fu;
+            push_rec(rec, ct, enc(t, 0), o1);
+            push_rec(rec, ct, enc(s1, 0), o2);
+            push_rec(rec, ct, enc(u, 0), ou1);
+            push_rec(rec, ct, enc(s2, 0), ou2);
+            vtri[p] = enc(t, 0);
+            vtri[v2] = enc(t, 1);
+            vtri[v0] = enc(t, 2);
+            vtri[v1] = enc(u, 1);
+            vtri[w] = enc(u, 2);
+        }
+        pos[p] = opos[p];
+        vstate[p] = VS_SHIFTED;
+        atomicAdd(&ct->changed, 1);
+    }
+};
+
+struct ResetVotes {
+    int *vote;
+    const int4 *tn;
+    const int *loc, *kind;
+    __device__ void operator()(long long ii) const
+    {
+        int k = kind[ii];
+        if (k < 0 || k == 2) return;
+        int t = dtri(loc[ii]);
+        vote[t] = 0x7fffffff;
+    }
+};
+
+struct ResetVotesEdge {
+    int *vote;
+    const int *list2;  // neighbour slots tagged for edge insertions
+    __device__ void operator()(long long ii) const { vote[list2[ii]] = 0x7fffffff; }
+};
+
+// Record the neighbour slot of every on-edge insertion (before the mesh changes).
+struct EdgeTags {
+    const int4 *tn;
+    const int *loc, *kind;
+    int *list2;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        if (kind[ii] != 1) return;
+        int t = dtri(loc[ii]), e = dori(loc[ii]);
+        int nb = geti(tn[t], e);
+        if (nb < 0) return;
+        int k = atomicAdd(&ct->nlist2, 1);
+        list2[k] = dtri(nb);
+    }
+};
+
+int stage_missing(Ctx &c)
+{
+    int r;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    launch_n(c, CountState{c.vstate, VS_MISSING, c.list, c.ctr}, c.N);
+    r = read_counters(c);
+    if (r) return r;
+    int nmiss = c.hctr->nlist;
+    c.st.nMissing = nmiss;
+    if (nmiss == 0) return GPUDT_OK;
+    int *loc = c.aux, *kind = c.aux2 + 0;
+    // aux2 holds kind at [0, nmiss) ; edge tags in list2
+    int rounds = 0, remaining = nmiss, dups = 0;
+    while (remaining > 0) {
+        int round = next_round(c);
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+        launch_n(c, MissingLocate{c.tv, c.tn, c.pos, c.opos, c.vtri, c.anchor, c.vstate, c.list, loc, kind, c.vote,
+                                  c.N, c.ctr},
+                 nmiss);
+        launch_n(c, EdgeTags{c.tn, loc, kind, c.list2, c.ctr}, nmiss);
+        launch_n(c, MissingInsert{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.vote, c.pos, c.opos, c.vstate,
+                                  c.list, loc, kind, c.rec, round, c.ctr},
+                 nmiss);
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        if (c.hctr->nfree < 0) {
+            int z = 0;
+            GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->nfree, &z, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        }
+        if (c.hctr->ntris > c.cap_tris) return GPUDT_ERR_NOMEM;
+        r = run_relink(c, round, c.hctr->nrec);
+        if (r) return r;
+        launch_n(c, ResetVotes{c.vote, c.tn, loc, kind}, nmiss);
+        launch_n(c, ResetVotesEdge{c.vote, c.list2}, c.hctr->nlist2);
+        int done = c.hctr->changed;
+        remaining -= done;
+        rounds++;
+        if (done == 0 || rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    // count drops
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    launch_n(c, CountState{c.vstate, VS_DUP, nullptr, c.ctr}, c.N);
+    r = read_counters(c);
+    if (r) return r;
+    dups = c.hctr->nlist;
+    c.st.nDuplicates = dups;
+    c.st.missingRounds = rounds;
+    return GPUDT_OK;
+}
+
+// ---------------------------------------------------------------- boundary
+// Fan of a hull vertex f: from the clockwise-most triangle (whose edge f->u0 is
+// a hull edge) counterclockwise to the triangle whose edge ud->f is a hull edge.
+struct FakeSelect {
+    const int4 *tv, *tn;
+    const int8_t *vstate;
+    const int *vtri;
+    int *list;
+    int N, F;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int f = N + (int)ii;
+        if (vstate[f] != VS_FAKE) return;
+        uint32_t pf = prio((uint32_t)f);
+        // rotate clockwise to the hull, checking neighbours on the way
+        int e = vtri[f];
+        for (int guard = 0; guard < 8 * kMaxFan; guard++) {
+            int t = dtri(e), i = dori(e);
+            int4 w = tv[t];
+            int a = geti(w, p1(i)), b = geti(w, m1(i));
+            if ((vstate[a] == VS_FAKE && prio((uint32_t)a) < pf) || (vstate[b] == VS_FAKE && prio((uint32_t)b) < pf))
+                return;
+            int nx = geti(tn[t], m1(i));  // across (f, a)
+            if (nx < 0) break;
+            e = enc(dtri(nx), m1(dori(nx)));
+            if (e == vtri[f]) {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 70);
+                return;
+            }
+        }
+        // the counterclockwise side
+        e = vtri[f];
+        for (int guard = 0; guard < 8 * kMaxFan; guard++) {
+            int t = dtri(e), i = dori(e);
+            int4 w = tv[t];
+            int b = geti(w, m1(i));
+            if (vstate[b] == VS_FAKE && prio((uint32_t)b) < pf) return;
+            int nx = geti(tn[t], p1(i));  // across (b, f)
+            if (nx < 0) break;
+            e = enc(dtri(nx), p1(dori(nx)));
+        }
+        int k = atomicAdd(&ct->nlist, 1);
+        list[k] = f;
+    }
+};
+
+constexpr int kMaxChain = 256;
+
+struct FakeRemove {
+    int4 *tv, *tn, *fwd;
+    int *epoch, *freelist, *vtri;
+    const int *list;
+    const double2 *pos;
+    int8_t *vstate;
+    Relink *rec;
+    int *cand;  // boundary-candidate vertices
+    int round;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int f = list[ii];
+        // clockwise-most triangle
+        int e = vtri[f];
+        for (int guard = 0;; guard++) {
+            if (guard > 8 * kMaxFan) {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 71);
+                return;
+            }
+            int t = dtri(e), i = dori(e);
+            int nx = geti(tn[t], m1(i));
+            if (nx < 0) break;
+            e = enc(dtri(nx), m1(dori(nx)));
+        }
+        int U[kMaxChain + 1], Fs[kMaxChain], Fi[kMaxChain], O[kMaxChain];
+        int d = 0;
+        for (;;) {
+            if (d >= kMaxChain) {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 72);
+                return;
+            }
+            int t = dtri(e), i = dori(e);
+            int4 w = tv[t];
+            U[d] = geti(w, p1(i));
+            Fs[d] = t;
+            Fi[d] = i;
+            O[d] = geti(tn[t], i);
+            d++;
+            U[d] = geti(w, m1(i));
+            int nx = geti(tn[t], p1(i));
+            if (nx < 0) break;
+            e = enc(dtri(nx), p1(dori(nx)));
+        }
+        for (int k = 0; k < d; k++) epoch[Fs[k]] = round;
+        // stack rule over the chain U[0..d]
+        int S[kMaxChain + 1], SO[kMaxChain + 1];  // SO[k]: owner of chain edge S[k-1] -> S[k]
+        int top = 0, used = 0;
+        auto owner_link = [&](int ownv, int loc) {
+            if (ownv <= -2) {
+                int k = -2 - ownv;
+                set_fwd(fwd, Fs[k], Fi[k], loc);
+                push_rec(rec, ct, loc, O[k]);
+            } else {
+                set_link(tn, loc, ownv);
+                set_link(tn, ownv, loc);
+            }
+        };
+        for (int k = 0; k <= d; k++) {
+            int wv = U[k];
+            int wown = k > 0 ? -2 - (k - 1) : -1;
+            while (top >= 2 && orientp(pos[S[top - 2]], pos[S[top - 1]], pos[wv], ct) > 0) {
+                int s = Fs[used++];
+                int A = S[top - 2], B = S[top - 1];
+                tv[s] = make_int4(A, B, wv, 0);
+                tn[s] = make_int4(-1, -1, -1, 0);
+                // opp wv (2): A->B owned by SO[top-1]; opp A (0): B->wv owned by wown;
+                // opp B (1): wv->A, the new chain edge A->wv
+                owner_link(SO[top - 1], enc(s, 2));
+                owner_link(wown, enc(s, 0));
+                wown = enc(s, 1);
+                vtri[A] = enc(s, 0);
+                vtri[B] = enc(s, 1);
+                vtri[wv] = enc(s, 2);
+                top--;
+            }
+            S[top] = wv;
+            SO[top] = wown;
+            top++;
+        }
+        // remaining chain edges are hull edges now
+        for (int k = 1; k < top; k++) {
+            int ownv = SO[k];
+            if (ownv <= -2) {
+                int q = -2 - ownv;
+                set_fwd(fwd, Fs[q], Fi[q], -1);
+                push_rec(rec, ct, -1, O[q]);
+            } else {
+                set_link(tn, ownv, -1);
+            }
+        }
+        for (int k = 0; k < top; k++) {
+            int c = atomicAdd(&ct->nlist2, 1);
+            cand[c] = S[k];
+        }
+        for (int k = used; k < d; k++) free_slot(tv, freelist, ct, Fs[k]);
+        vtri[f] = -1;
+        vstate[f] = VS_GONE;
+    }
+};
+
+// Convexity check of a boundary candidate: finds its hull edges (u->v, v->w)
+// and reports reflex vertices (orient(u,v,w) < 0).
+__device__ bool hull_neighbours(const int4 *tv, const int4 *tn, int v, int start, int *u, int *w, int *tin,
+                                int *tout)
+{
+    // clockwise to the outgoing hull edge v->w (edge opposite b of (v,a,b) ... )
+    int e = start;
+    for (int guard = 0; guard < 8 * kMaxFan; guard++) {
+        int t = dtri(e), i = dori(e);
+        int nx = geti(tn[t], m1(i));  // across (v, a)
+        if (nx < 0) {
+            *w = geti(tv[t], p1(i));
+            *tout = enc(t, m1(i));
+            break;
+        }
+        e = enc(dtri(nx), m1(dori(nx)));
+        if (e == start) return false;  // interior vertex
+    }
+    e = start;
+    for (int guard = 0; guard < 8 * kMaxFan; guard++) {
+        int t = dtri(e), i = dori(e);
+        int nx = geti(tn[t], p1(i));  // across (b, v)
+        if (nx < 0) {
+            *u = geti(tv[t], m1(i));
+            *tin = enc(t, p1(i));
+            return true;
+        }
+        e = enc(dtri(nx), p1(dori(nx)));
+    }
+    return false;
+}
+
+struct ReflexCheck {
+    const int4 *tv, *tn;
+    const double2 *pos;
+    const int *vtri, *cand;
+    const int8_t *vstate;
+    int *list;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int v = cand[ii];
+        if (vtri[v] < 0) return;
+        int u, w, tin, tout;
+        if (!hull_neighbours(tv, tn, v, vtri[v], &u, &w, &tin, &tout)) return;
+        if (orientp(pos[u], pos[v], pos[w], ct) < 0) {
+            int k = atomicAdd(&ct->nlist, 1);
+            list[k] = v;
+        }
+    }
+};
+
+// Sequential fill of reflex hull vertices (rare): adds triangle (u, w, v) for a
+// reflex v between hull neighbours u and w, then re-examines u and w.
+struct Convexify {
+    int4 *tv, *tn;
+    const double2 *pos;
+    int *vtri, *freelist;
+    const int *list;
+    int nlist;
+    Counters *ct;
+    __device__ void operator()(long long) const;
+};
+
+__device__ void Convexify::operator()(long long) const
+{
+    int stack[1024];
+    int sp = 0;
+    for (int k = 0; k < nlist && sp < 1024; k++) stack[sp++] = list[k];
+    for (int guard = 0; sp > 0; guard++) {
+        if (guard > (1 << 22)) {
+            set_err(ct, GPUDT_ERR_NOCONVERGE, 80);
+            return;
+        }
+        int v = stack[--sp];
+        if (vtri[v] < 0) continue;
+        int u, w, tin, tout;
+        if (!hull_neighbours(tv, tn, v, vtri[v], &u, &w, &tin, &tout)) continue;
+        if (orientp(pos[u], pos[v], pos[w], ct) >= 0) continue;
+        int s = alloc_slot(freelist, ct);
+        // (u, w, v): opp u (0) = w->v, the reverse of hull edge v->w (tout);
+        //            opp w (1) = v->u, the reverse of hull edge u->v (tin); opp v (2) = new hull u->w
+        tv[s] = make_int4(u, w, v, 0);
+        tn[s] = make_int4(tout, tin, -1, 0);
+        set_link(tn, tout, enc(s, 0));
+        set_link(tn, tin, enc(s, 1));
+        vtri[u] = enc(s, 0);
+        vtri[w] = enc(s, 1);
+        vtri[v] = enc(s, 2);
+        if (sp + 2 <= 1024) {
+            stack[sp++] = u;
+            stack[sp++] = w;
+        } else {
+            set_err(ct, GPUDT_ERR_NOMEM, 81);
+            return;
+        }
+    }
+}
+
+int stage_boundary(Ctx &c)
+{
+    int r, guard = 0;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+    int *cand = c.aux;  // boundary candidates
+    int removed = 0;
+    while (removed < c.F) {
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+        launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.N, c.F, c.ctr}, c.F);
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        int nsel = c.hctr->nlist;
+        if (nsel == 0) return GPUDT_ERR_NOCONVERGE;
+        int round = next_round(c);
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
+        launch_n(c, FakeRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, c.pos, c.vstate, c.rec, cand,
+                               round, c.ctr},
+                 nsel);
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        r = run_relink(c, round, c.hctr->nrec);
+        if (r) return r;
+        removed += nsel;
+        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    r = read_counters(c);
+    if (r) return r;
+    int ncand = c.hctr->nlist2;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    launch_n(c, ReflexCheck{c.tv, c.tn, c.pos, c.vtri, cand, c.vstate, c.list, c.ctr}, ncand);
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->nlist > 0) {
+        launch_n(c, Convexify{c.tv, c.tn, c.pos, c.vtri, c.freelist, c.list, c.hctr->nlist, c.ctr}, 1);
+        GALPHA_CUDA(cudaGetLastError());
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        if (c.hctr->nfree < 0) {
+            int z = 0;
+            GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->nfree, &z, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        }
+    }
+    return GPUDT_OK;
+}
+
+// -------------------------------------------------------------------- flip
+struct FlipCheck {
+    const int4 *tv, *tn;
+    const double2 *pos;
+    const int *act;
+    int *vote, *prop, *target, *cands;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int t = act[ii];
+        int4 v = tv[t];
+        if (v.x < 0) return;
+        int4 n = tn[t];
+        int x[3] = {v.x, v.y, v.z}, nb[3] = {n.x, n.y, n.z};
+        for (int i = 0; i < 3; i++) {
+            int e = nb[i];
+            if (e < 0) continue;
+            int u = dtri(e);
+            int d = geti(tv[u], dori(e));
+            double2 A = pos[x[p1(i)]], B = pos[x[m1(i)]], C = pos[x[i]], D = pos[d];
+            double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
+            int s = incircle_filter(pa, pb, pc, pd);
+            if (s == 2) {
+                atomicAdd(&ct->exact_incircle, 1ull);
+                s = incircle_exact(pa, pb, pc, pd);
+                if (s == EXACT_OVERFLOW) {
+                    set_err(ct, GPUDT_ERR_EXACT, 90);
+                    return;
+                }
+            } else {
+                atomicAdd(&ct->filt_incircle, 1ull);
+            }
+            if (s > 0) {
+                prop[t] = i;
+                target[t] = u;
+                atomicMin(&vote[t], t);
+                atomicMin(&vote[u], t);
+                int k = atomicAdd(&ct->nlist, 1);
+                cands[k] = t;
+                return;
+            }
+        }
+    }
+};
+
+struct FlipApply {
+    int4 *tv, *tn, *fwd;
+    int *epoch, *vtri, *vote, *stamp, *next;
+    const int *prop, *target, *cands;
+    Relink *rec;
+    int round;
+    Counters *ct;
+    __device__ void add_next(int x) const
+    {
+        if (x < 0) return;
+        if (atomicExch(&stamp[x], round) != round) {
+            int k = atomicAdd(&ct->nlist2, 1);
+            next[k] = x;
+        }
+    }
+    __device__ void operator()(long long ii) const
+    {
+        int t = cands[ii];
+        int u = target[t];
+        if (vote[t] != t || vote[u] != t) {
+            add_next(t);
+            return;
+        }
+        int i = prop[t];
+        int4 tvv = tv[t], tnn = tn[t];
+        int e = geti(tnn, i);
+        int j = dori(e);
+        int4 uvv = tv[u], unn = tn[u];
+        int a = geti(tvv, i), b = geti(tvv, p1(i)), cc = geti(tvv, m1(i)), d = geti(uvv, j);
+        int ot1 = geti(tnn, p1(i)), ot2 = geti(tnn, m1(i));
+        int ou1 = geti(unn, p1(j)), ou2 = geti(unn, m1(j));
+        epoch[t] = round;
+        epoch[u] = round;
+        tv[t] = make_int4(a, b, d, 0);
+        tv[u] = make_int4(d, cc, a, 0);
+        tn[t] = make_int4(-1, enc(u, 1), -1, 0);
+        tn[u] = make_int4(-1, enc(t, 1), -1, 0);
+        int4 ft = make_int4(0, 0, 0, 0), fu = make_int4(0, 0, 0, 0);
+        seti(ft, i, -1);
+        seti(ft, p1(i), enc(u, 0));
+        seti(ft, m1(i), enc(t, 2));
+        seti(fu, j, -1);
+        seti(fu, p1(j), enc(t, 0));
+        seti(fu, m1(j), enc(u, 2));
+        fwd[t] = ft;
+        fwd[u] = fu;
+        push_rec(rec, ct, enc(t, 0), ou1);
+        push_rec(rec, ct, enc(t, 2), ot2);
+        push_rec(rec, ct, enc(u, 0), ot1);
+        push_rec(rec, ct, enc(u, 2), ou2);
+        vtri[a] = enc(t, 0);
+        vtri[b] = enc(t, 1);
+        vtri[d] = enc(t, 2);
+        vtri[cc] = enc(u, 1);
+        atomicAdd(&ct->nflips, 1);
+        add_next(t);
+        add_next(u);
+        if (ou1 >= 0) add_next(dtri(ou1));
+        if (ot2 >= 0) add_next(dtri(ot2));
+        if (ot1 >= 0) add_next(dtri(ot1));
+        if (ou2 >= 0) add_next(dtri(ou2));
+    }
+};
+
+struct FlipReset {
+    int *vote;
+    const int *target, *cands;
+    __device__ void operator()(long long ii) const
+    {
+        int t = cands[ii];
+        vote[t] = 0x7fffffff;
+        vote[target[t]] = 0x7fffffff;
+    }
+};
+
+struct AllAlive {
+    const int4 *tv;
+    int *list;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        if (tv[i].x >= 0) {
+            int k = atomicAdd(&ct->nlist, 1);
+            list[k] = (int)i;
+        }
+    }
+};
+
+int stage_flip(Ctx &c)
+{
+    int r = read_counters(c);
+    if (r) return r;
+    int nt = c.hctr->ntris;
+    int *act = c.list, *nxt = c.list2;
+    int *prop = c.aux, *target = c.aux2, *cands = c.inc, *stamp = c.stamp;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    launch_n(c, AllAlive{c.tv, act, c.ctr}, nt);
+    r = read_counters(c);
+    if (r) return r;
+    int nact = c.hctr->nlist;
+    GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
+    int rounds = 0;
+    long long flips = 0;
+    while (nact > 0) {
+        int round = next_round(c);
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 3 * sizeof(int), c.stream));  // nlist, nlist2, nrec
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nflips, 0, sizeof(int), c.stream));
+        launch_n(c, FlipCheck{c.tv, c.tn, c.pos, act, c.vote, prop, target, cands, c.ctr}, nact);
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        int ncand = c.hctr->nlist;
+        if (ncand == 0) break;
+        launch_n(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nxt, prop, target, cands, c.rec,
+                              round, c.ctr},
+                 ncand);
+        r = read_counters(c);
+        if (r) return r;
+        r = run_relink(c, round, c.hctr->nrec);
+        if (r) return r;
+        launch_n(c, FlipReset{c.vote, target, cands}, ncand);
+        flips += c.hctr->nflips;
+        nact = c.hctr->nlist2;
+        std::swap(act, nxt);
+        if (++rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+    }
+    c.st.nFlips = (int)flips;
+    c.st.flipRounds = rounds;
+    return GPUDT_OK;
+}
+
+// ----------------------------------------------------------------- compact
+struct MarkAlive {
+    const int4 *tv;
+    int *flag;
+    __device__ void operator()(long long i) const { flag[i] = tv[i].x >= 0 ? 1 : 0; }
+};
+
+struct CompactWrite {
+    const int4 *tv, *tn;
+    const int *newidx;
+    int4 *cv, *cn;
+    gpudtTriangle *out;
+    __device__ void operator()(long long ii) const
+    {
+        int t = (int)ii;
+        int4 v = tv[t];
+        if (v.x < 0) return;
+        int4 n = tn[t];
+        int k = newidx[t];
+        int nn[3] = {n.x, n.y, n.z};
+        for (int q = 0; q < 3; q++)
+            if (nn[q] >= 0) nn[q] = enc(newidx[dtri(nn[q])], dori(nn[q]));
+        cv[k] = make_int4(v.x, v.y, v.z, 0);
+        cn[k] = make_int4(nn[0], nn[1], nn[2], 0);
+        gpudtTriangle g;
+        g.tri[0] = nn[0];
+        g.tri[1] = nn[1];
+        g.tri[2] = nn[2];
+        g.vtx[0] = v.x;
+        g.vtx[1] = v.y;
+        g.vtx[2] = v.z;
+        g.tmp[0] = g.tmp[1] = g.tmp[2] = 0;
+        out[k] = g;
+    }
+};
+
+int stage_compact(Ctx &c)
+{
+    int r = read_counters(c);
+    if (r) return r;
+    int nt = c.hctr->ntris;
+    launch_n(c, MarkAlive{c.tv, c.aux}, nt);
+    r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->nlist);
+    if (r) return r;
+    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, c.outtri}, nt);
+    GALPHA_CUDA(cudaGetLastError());
+    r = read_counters(c);
+    if (r) return r;
+    c.nT_out = c.hctr->nlist;
+    return GPUDT_OK;
+}
+
+}  // namespace galpha

@@ -1,0 +1,242 @@
+// internal.cuh -- device context, buffers and launch helpers of galpha-b200.
+//
+// One handle owns one CUDA stream and one set of device buffers, grown on
+// demand and reused across calls, so repeated calls allocate nothing.  All
+// kernels of the pipeline are launched on that stream; the few host decisions
+// between stages read a small pinned counter block.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include "../../include/gpudt.h"
+#include "../../include/galpha.h"
+
+#ifndef GALPHA_HD
+#define GALPHA_HD __host__ __device__ __forceinline__
+#endif
+
+namespace galpha {
+
+// ------------------------------------------------------------- constants
+constexpr int kFakeSpacing = 32;                 // fake ring site every <= 32 pixels
+constexpr int kMargin = kFakeSpacing / 2 + 1;    // real sites stay >= 17 pixels from the border
+constexpr int kMaxFan = 64;                      // star holes / fans handled per thread
+constexpr int kMaxRounds = 100000;               // cap of every iterative stage
+
+// vertex states
+enum : int8_t {
+    VS_UNDECIDED = 0,  // present in the texture, not yet shifted
+    VS_SHIFTED = 1,    // in the mesh at its true coordinates
+    VS_BAD = 2,        // cannot be shifted: to be removed and re-inserted
+    VS_MISSING = 3,    // not in the mesh, to be inserted by point location
+    VS_FAKE = 4,       // fake ring site in the mesh
+    VS_DUP = 5,        // exact duplicate of a lower index: dropped
+    VS_GONE = 6,       // fake ring site removed
+};
+
+// Device counter block (one per handle, mapped to host through a pinned copy).
+struct Counters {
+    int ntris;      // triangle slots in use (tail of the slot array)
+    int nfree;      // entries of the free-slot stack
+    int nlist;      // generic work-list length
+    int nlist2;     // second work list
+    int nrec;       // relink records this round
+    int changed;    // generic progress flag / count
+    int err;        // first error code (GPUDT_ERR_*), 0 if none
+    int errinfo;    // stage-specific detail of the first error
+    int nisland;    // island pixels
+    int nflips;     // flips this round
+    int nties;      // exact spectrum ties merged
+    int pad[5];
+    unsigned long long exact_compares;
+    unsigned long long exact_orient;
+    unsigned long long exact_incircle;
+    unsigned long long filt_incircle;
+    unsigned long long exact_attached;
+};
+
+// Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
+// when the edge became a hull edge) and the encoded outer neighbour it had
+// before the round (old = (u<<2)|j, or -1).
+struct Relink {
+    int loc;
+    int old;
+};
+
+// A grown-on-demand device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    long long budget = 0;
+    long long reserved = 0;
+    int sm_count = 148;
+
+    // problem
+    int N = 0, F = 0, V = 0, T = 0, logT = 0;
+    double scale = 1, shiftX = 0, shiftY = 0;
+    int cap_tris = 0;
+
+    // device arrays (pointers into bufs)
+    double2 *opos = nullptr;   // [V] true coordinates
+    double2 *pos = nullptr;    // [V] current coordinates
+    short2 *gpix = nullptr;    // [V] texture pixel of each site
+    int *idmap = nullptr;      // [T*T] site id of each occupied pixel (lowest index)
+    uint32_t *occ = nullptr;   // [T * T/32] column-major occupancy bits
+    uint32_t *bandocc = nullptr;  // [T * W2] per-column 64-row band occupancy
+    int16_t *ycol = nullptr;   // [T*T] row of the nearest site in the pixel's column
+    int *colour = nullptr;     // [T*T] discrete Voronoi diagram (site id per pixel)
+    int *list = nullptr;       // [max(T*T/?, V, cap)] work list
+    int *list2 = nullptr;
+    int *aux = nullptr;        // [cap] generic int scratch
+    int *aux2 = nullptr;
+    int4 *tv = nullptr;        // [cap] triangle vertices (x,y,z; w = flags)
+    int4 *tn = nullptr;        // [cap] triangle neighbours (x,y,z; w unused)
+    int4 *fwd = nullptr;       // [cap] forwarding of consumed triangles' edges
+    int *epoch = nullptr;      // [cap] round that consumed the slot
+    int *vote = nullptr;       // [cap]
+    int *stamp = nullptr;      // [cap]
+    int4 *cv = nullptr;        // [cap] compacted triangle vertices
+    int4 *cn = nullptr;        // [cap] compacted triangle neighbours
+    int *freelist = nullptr;   // [cap]
+    Relink *rec = nullptr;     // [3*cap]
+    int *vtri = nullptr;       // [V] one incident oriented triangle
+    int8_t *vstate = nullptr;  // [V]
+    int *vround = nullptr;     // [V]
+    int *anchor = nullptr;     // [V]
+    int *deg = nullptr;        // [V+1]
+    int *inc = nullptr;        // [3*cap]
+    int *tilecount = nullptr;  // [ntiles + 1]
+    Counters *ctr = nullptr;   // device counters
+    Counters *hctr = nullptr;  // pinned host mirror
+
+    // alpha arrays
+    int nT_out = 0, nE = 0, nSpecIn = 0, nSpec = 0;
+    int *e_off = nullptr;      // [nT+1] first edge of each triangle
+    int4 *edges = nullptr;     // [nE] p1, p2, tIndex | vOpp<<30? (see alpha.cu)
+    int *edge_ro = nullptr;    // [nE]
+    int2 *edge_nu = nullptr;   // [nE]
+    int *tri_ro = nullptr;     // [nT]
+    int2 *pt_nu = nullptr;     // [N]
+    unsigned long long *keys = nullptr, *keys2 = nullptr;  // [nSpecIn]
+    int *vals = nullptr, *vals2 = nullptr;                 // [nSpecIn]
+    int *rank = nullptr;       // [nSpecIn]
+    double *spectrum = nullptr;  // [nSpecIn + 1]
+    int *hist = nullptr;       // scan scratch
+    int *rhist = nullptr;      // radix sort histograms
+    gpudtTriangle *outtri = nullptr;  // [cap] AoS output staging
+
+    DevBuf bufs[64];
+    int nbufs = 0;
+
+    // events for stage timing
+    cudaEvent_t ev[GALPHA_STAGE_TOTAL + 2];
+    cudaEvent_t kev[8];  // [2k, 2k+1] bracket single kernel k (see gpudtStatus.kernelMs)
+    bool events = false;
+    gpudtStatus st;
+    bool have_mesh = false, have_alpha = false;
+};
+
+// ------------------------------------------------------------- error helpers
+#define GALPHA_CUDA(call)                                               \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) return galpha::cuda_fail(e_, #call);     \
+    } while (0)
+
+int cuda_fail(cudaError_t e, const char *what);
+const char *last_error_text();
+
+// Reserve device buffers for V vertices, T texture, cap triangles.
+int reserve(Ctx &c, int V, int T, int cap_tris, bool alpha);
+int read_counters(Ctx &c);
+
+// Kernel launches issued by this library (all handles, all threads).
+extern unsigned long long g_launches;
+inline void count_launch(unsigned long long k = 1) { __atomic_fetch_add(&g_launches, k, __ATOMIC_RELAXED); }
+
+#ifdef __CUDACC__
+// Grid-stride launch of a device functor over [0, n).
+template <class F>
+__global__ void __launch_bounds__(256) k_for_each(F f, long long n)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) f(i);
+}
+
+template <class F>
+inline void launch_n(const Ctx &c, F f, long long n)
+{
+    if (n <= 0) return;
+    long long blocks = (n + 255) / 256;
+    long long maxb = (long long)c.sm_count * 8;
+    if (blocks > maxb) blocks = maxb;
+    k_for_each<<<(unsigned)blocks, 256, 0, c.stream>>>(f, n);
+    count_launch();
+}
+#endif
+
+// Report the first error from device code.
+__device__ __forceinline__ void set_err(Counters *ct, int code, int info)
+{
+    if (atomicCAS(&ct->err, 0, code) == 0) ct->errinfo = info;
+}
+
+// 32-bit invertible mix (murmur3 finaliser): a random-looking priority per id.
+GALPHA_HD uint32_t prio(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+GALPHA_HD int enc(int t, int i) { return (t << 2) | i; }
+GALPHA_HD int dtri(int e) { return e >> 2; }
+GALPHA_HD int dori(int e) { return e & 3; }
+GALPHA_HD int p1(int i) { return i == 2 ? 0 : i + 1; }
+GALPHA_HD int m1(int i) { return i == 0 ? 2 : i - 1; }
+GALPHA_HD int geti(const int4 &v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+GALPHA_HD void seti(int4 &v, int i, int x)
+{
+    if (i == 0) v.x = x;
+    else if (i == 1) v.y = x;
+    else v.z = x;
+}
+
+// Stage entry points (dt_grid.cu, dt_mesh.cu, alpha.cu)
+int has_triangles(Ctx &c, const double *d_xy, int n);
+int stage_setup(Ctx &c, const double *d_xy, int n, double minX, double minY, double maxX, double maxY, int T);
+int stage_voronoi(Ctx &c);
+int stage_triangles(Ctx &c);
+int stage_links(Ctx &c);
+int stage_shift(Ctx &c);
+int stage_missing(Ctx &c);
+int stage_boundary(Ctx &c);
+int stage_flip(Ctx &c);
+int stage_compact(Ctx &c);
+int stage_alpha(Ctx &c);
+int alpha_from_host_mesh(Ctx &c, const double *h_xy, int n, const gpudtTriangle *tris, int nt);
+
+// Block-level kernels of the Voronoi stage (voronoi_kernels.cu)
+constexpr int kEmitThreads = 256;
+constexpr int kEmitTile = kEmitThreads;
+int launch_column_pass(Ctx &c, int W2);
+int launch_row_pass(Ctx &c);
+int launch_emit(Ctx &c, int ntiles, long long nwin, bool write);
+// LSD radix sort of (keys, vals) ascending (sort.cu)
+int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n);
+
+// Prefix sums (scan.cu)
+int exclusive_scan_int(Ctx &c, const int *in, int *out, int n, int *total_dev);
+size_t scan_scratch_bytes(int n);
+
+}  // namespace galpha

@@ -1,0 +1,373 @@
+// voronoi_kernels.cu -- block-level kernels of the discrete Voronoi stage:
+// the column pass, the per-row lower envelope + colouring, and the 2x2-window
+// triangle emission.  Launchers are called from dt_grid.cu.
+#include "internal.cuh"
+
+namespace galpha {
+
+// ------------------------------------------------------------ column pass
+// Thread (x, band): ycol[y][x] = row of the nearest occupied pixel of column x
+// (ties: the upper one, i.e. smaller y), -1 for an empty column.
+__global__ void __launch_bounds__(256) k_column_pass(const uint32_t *__restrict__ occ,
+                                                     const uint32_t *__restrict__ bandocc,
+                                                     int16_t *__restrict__ ycol, int T, int W2)
+{
+    int x = blockIdx.x * 32 + threadIdx.x;
+    int b = blockIdx.y * blockDim.y + threadIdx.y;
+    int nb = T >> 6;
+    if (x >= T || b >= nb) return;
+    const uint32_t *col = occ + (size_t)x * (T >> 5);
+    const uint32_t *bo = bandocc + (size_t)x * W2;
+    unsigned long long m = (unsigned long long)col[2 * b] | ((unsigned long long)col[2 * b + 1] << 32);
+    // previous non-empty band
+    int yabove = -1, ybelow = -1;
+    {
+        int w = b >> 5;
+        uint32_t bits = bo[w] & ((b & 31) ? (0xffffffffu >> (32 - (b & 31))) : 0u);
+        while (true) {
+            if (bits) {
+                int pb = w * 32 + 31 - __clz(bits);
+                unsigned long long pm =
+                    (unsigned long long)col[2 * pb] | ((unsigned long long)col[2 * pb + 1] << 32);
+                yabove = pb * 64 + 63 - __clzll(pm);
+                break;
+            }
+            if (--w < 0) break;
+            bits = bo[w];
+        }
+    }
+    {
+        int w = b >> 5;
+        int sh = (b & 31) + 1;
+        uint32_t bits = sh >= 32 ? 0u : (bo[w] & (0xffffffffu << sh));
+        while (true) {
+            if (bits) {
+                int nb2 = w * 32 + __ffs(bits) - 1;
+                unsigned long long nm =
+                    (unsigned long long)col[2 * nb2] | ((unsigned long long)col[2 * nb2 + 1] << 32);
+                ybelow = nb2 * 64 + __ffsll((long long)nm) - 1;
+                break;
+            }
+            if (++w >= W2) break;
+            bits = bo[w];
+        }
+    }
+    int y0 = b * 64;
+    int16_t *out = ycol + (size_t)y0 * T + x;
+    for (int r = 0; r < 64; r++) {
+        unsigned long long lowmask = (r == 63) ? ~0ull : ((2ull << r) - 1ull);
+        unsigned long long lo = m & lowmask;
+        unsigned long long hi = m & ~((1ull << r) - 1ull);
+        int y = y0 + r;
+        int yp = lo ? (y0 + 63 - __clzll(lo)) : yabove;
+        int yn = hi ? (y0 + __ffsll((long long)hi) - 1) : ybelow;
+        int best;
+        if (yp < 0) best = yn;
+        else if (yn < 0) best = yp;
+        else best = (y - yp <= yn - y) ? yp : yn;
+        out[(size_t)r * T] = (int16_t)best;
+    }
+}
+
+// --------------------------------------------------------------- row pass
+// Exact-integer lower envelope of the parabolas f_x(p) = (p - x)^2 + (y - yc[x])^2.
+struct Par {
+    int x;
+    int c;  // x^2 + h
+};
+
+__device__ __forceinline__ int par_c(int x, int yc, int y)
+{
+    int h = y - yc;
+    return x * x + h * h;
+}
+
+// true if b is hidden between a and c: s(a,b) >= s(b,c) with s(a,b) = (cb - ca) / (2 (xb - xa)).
+__device__ __forceinline__ bool dominated(Par a, Par b, Par c)
+{
+    long long n1 = (long long)(b.c - a.c), d1 = 2LL * (b.x - a.x);
+    long long n2 = (long long)(c.c - b.c), d2 = 2LL * (c.x - b.x);
+    return n1 * d2 >= n2 * d1;
+}
+
+// last integer pixel owned by a (a left of b, ties go left): floor((cb - ca) / (2 (xb - xa)))
+__device__ __forceinline__ int boundary(Par a, Par b)
+{
+    int num = b.c - a.c, den = 2 * (b.x - a.x);
+    int q = num / den;
+    if ((num % den != 0) && ((num < 0) != (den < 0))) q--;
+    return q;
+}
+
+constexpr int kRowThreads = 256;
+constexpr int16_t kDead = -2;  // nxt[] marker of an element popped from the envelope
+
+__global__ void __launch_bounds__(kRowThreads) k_row_pass(const int16_t *__restrict__ ycol,
+                                                          const int *__restrict__ idmap,
+                                                          int *__restrict__ colour, int T, int logT)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    int16_t *ys = (int16_t *)smem;       // [T]
+    int16_t *nxt = ys + T;               // [T]
+    int16_t *prv = nxt + T;              // [T]
+    int *row = (int *)(prv + T + (T & 1));  // [T] colour staging
+    __shared__ int16_t segHead[kRowThreads], segTail[kRowThreads];
+
+    const int y = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int S = T / kRowThreads;
+    // 1. load the row of column candidates (16-byte vectors)
+    {
+        const int4 *src = (const int4 *)(ycol + (size_t)y * T);
+        int4 *dst = (int4 *)ys;
+        for (int k = tid; k < T / 8; k += kRowThreads) dst[k] = src[k];
+    }
+    __syncthreads();
+    // 2. local envelope of each thread's segment
+    {
+        int head = -1, tail = -1;
+        int x0 = tid * S;
+        for (int x = x0; x < x0 + S; x++) {
+            int yc = ys[x];
+            if (yc < 0) continue;
+            Par cur{x, par_c(x, yc, y)};
+            while (tail >= 0 && prv[tail] >= 0) {
+                int pt = prv[tail];
+                Par a{pt, par_c(pt, ys[pt], y)}, b{tail, par_c(tail, ys[tail], y)};
+                if (!dominated(a, b, cur)) break;
+                nxt[tail] = kDead;
+                tail = pt;
+            }
+            prv[x] = (int16_t)tail;
+            nxt[x] = -1;
+            if (tail >= 0) nxt[tail] = (int16_t)x;
+            else head = x;
+            tail = x;
+        }
+        segHead[tid] = (int16_t)head;
+        segTail[tid] = (int16_t)tail;
+    }
+    __syncthreads();
+    // 3. pairwise merges
+    for (int w = 1; w < kRowThreads; w <<= 1) {
+        if ((tid & (2 * w - 1)) == 0) {
+            int lh = segHead[tid], lt = segTail[tid];
+            int rh = segHead[tid + w], rt = segTail[tid + w];
+            if (lh < 0) {
+                lh = rh;
+                lt = rt;
+            } else if (rh >= 0) {
+                while (true) {
+                    int plt = prv[lt];
+                    if (plt >= 0) {
+                        Par a{plt, par_c(plt, ys[plt], y)}, b{lt, par_c(lt, ys[lt], y)},
+                            c{rh, par_c(rh, ys[rh], y)};
+                        if (dominated(a, b, c)) {
+                            nxt[lt] = kDead;
+                            lt = plt;
+                            continue;
+                        }
+                    }
+                    int nrh = nxt[rh];
+                    if (nrh >= 0) {
+                        Par a{lt, par_c(lt, ys[lt], y)}, b{rh, par_c(rh, ys[rh], y)},
+                            c{nrh, par_c(nrh, ys[nrh], y)};
+                        if (dominated(a, b, c)) {
+                            nxt[rh] = kDead;
+                            prv[nrh] = -1;
+                            rh = nrh;
+                            continue;
+                        }
+                    }
+                    break;
+                }
+                nxt[lt] = (int16_t)rh;
+                prv[rh] = (int16_t)lt;
+                lt = rt;
+            }
+            segHead[tid] = (int16_t)lh;
+            segTail[tid] = (int16_t)lt;
+        }
+        __syncthreads();
+    }
+    // 4. colour: every live element paints its own interval
+    {
+        int x0 = tid * S;
+        for (int x = x0; x < x0 + S; x++) {
+            int yc = ys[x];
+            if (yc < 0) continue;
+            int nx = nxt[x];
+            if (nx == kDead) continue;  // popped from the envelope
+            int pv = prv[x];
+            Par me{x, par_c(x, yc, y)};
+            int lo = 0, hi = T - 1;
+            if (pv >= 0) {
+                Par a{pv, par_c(pv, ys[pv], y)};
+                lo = boundary(a, me) + 1;
+            }
+            if (nx >= 0) {
+                Par b{nx, par_c(nx, ys[nx], y)};
+                hi = boundary(me, b);
+            }
+            if (lo < 0) lo = 0;
+            if (hi > T - 1) hi = T - 1;
+            if (lo > hi) continue;
+            int id = idmap[((size_t)yc << logT) + x];
+            for (int p = lo; p <= hi; p++) row[p] = id;
+        }
+    }
+    __syncthreads();
+    {
+        const int4 *src = (const int4 *)row;
+        int4 *dst = (int4 *)(colour + (size_t)y * T);
+        for (int k = tid; k < T / 4; k += kRowThreads) dst[k] = src[k];
+    }
+}
+
+// ------------------------------------------------------ dual triangles
+// 2x2 window at (x, y): corners c0 (x,y), c1 (x+1,y), c2 (x+1,y+1), c3 (x,y+1),
+// counterclockwise.  Returns the triangle count and the triangles.
+__device__ __forceinline__ long long orient_pix(short2 a, short2 b, short2 c)
+{
+    return (long long)(a.x - c.x) * (b.y - c.y) - (long long)(a.y - c.y) * (b.x - c.x);
+}
+
+__device__ __forceinline__ int window_tris(const int *colour, const short2 *gpix, int logT, int x, int y,
+                                           int3 *t, int *bad)
+{
+    size_t r0 = ((size_t)y << logT) + x, r1 = r0 + ((size_t)1 << logT);
+    int c[4] = {colour[r0], colour[r0 + 1], colour[r1 + 1], colour[r1]};
+    if (c[0] == c[2] || c[1] == c[3]) return 0;
+    int L[4], n = 0;
+    for (int k = 0; k < 4; k++)
+        if (c[k] != c[(k + 3) & 3]) L[n++] = c[k];
+    if (n == 3) {
+        t[0] = make_int3(L[0], L[1], L[2]);
+        if (orient_pix(gpix[L[0]], gpix[L[1]], gpix[L[2]]) <= 0) *bad = 1;
+        return 1;
+    }
+    if (n == 4) {
+        short2 g0 = gpix[L[0]], g1 = gpix[L[1]], g2 = gpix[L[2]], g3 = gpix[L[3]];
+        if (orient_pix(g0, g1, g2) > 0 && orient_pix(g0, g2, g3) > 0) {
+            t[0] = make_int3(L[0], L[1], L[2]);
+            t[1] = make_int3(L[0], L[2], L[3]);
+        } else {
+            t[0] = make_int3(L[1], L[2], L[3]);
+            t[1] = make_int3(L[1], L[3], L[0]);
+            if (orient_pix(g1, g2, g3) <= 0 || orient_pix(g1, g3, g0) <= 0) *bad = 1;
+        }
+        return 2;
+    }
+    return 0;
+}
+
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *total)
+{
+    __shared__ int warpsum[kEmitThreads / 32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warpsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < kEmitThreads / 32 ? warpsum[lane] : 0;
+        int si = s;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += t;
+        }
+        if (lane < kEmitThreads / 32) warpsum[lane] = si - s;
+    }
+    __syncthreads();
+    int excl = incl - v + warpsum[w];
+    if (total) {
+        __shared__ int tot;
+        if (threadIdx.x == kEmitThreads - 1) tot = excl + v;
+        __syncthreads();
+        *total = tot;
+    }
+    return excl;
+}
+
+__global__ void __launch_bounds__(kEmitThreads) k_emit_count(const int *__restrict__ colour,
+                                                             const short2 *__restrict__ gpix, int *tilecount,
+                                                             int T, int logT, long long nwin, Counters *ct)
+{
+    long long w = (long long)blockIdx.x * kEmitThreads + threadIdx.x;
+    int n = 0, bad = 0;
+    if (w < nwin) {
+        int x = (int)(w % (T - 1)), y = (int)(w / (T - 1));
+        int3 t[2];
+        n = window_tris(colour, gpix, logT, x, y, t, &bad);
+        if (bad) set_err(ct, GPUDT_ERR_TOPOLOGY, 10);
+    }
+    int total;
+    block_exclusive_scan(n, &total);
+    if (threadIdx.x == 0) tilecount[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kEmitThreads) k_emit_write(const int *__restrict__ colour,
+                                                             const short2 *__restrict__ gpix,
+                                                             const int *__restrict__ tileoff, int4 *tv, int T,
+                                                             int logT, long long nwin)
+{
+    long long w = (long long)blockIdx.x * kEmitThreads + threadIdx.x;
+    int n = 0, bad = 0;
+    int3 t[2];
+    if (w < nwin) {
+        int x = (int)(w % (T - 1)), y = (int)(w / (T - 1));
+        n = window_tris(colour, gpix, logT, x, y, t, &bad);
+    }
+    int off = block_exclusive_scan(n, nullptr) + tileoff[blockIdx.x];
+    for (int k = 0; k < n; k++) tv[off + k] = make_int4(t[k].x, t[k].y, t[k].z, 0);
+}
+
+
+// ---------------------------------------------------------------- launchers
+int launch_column_pass(Ctx &c, int W2)
+{
+    const int T = c.T;
+    dim3 block(32, 8), grid(T / 32, ((T >> 6) + 7) / 8);
+    if (c.events) cudaEventRecord(c.kev[2], c.stream);
+    k_column_pass<<<grid, block, 0, c.stream>>>(c.occ, c.bandocc, c.ycol, T, W2);
+    if (c.events) cudaEventRecord(c.kev[3], c.stream);
+    count_launch();
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
+int launch_row_pass(Ctx &c)
+{
+    const int T = c.T;
+    size_t sm = sizeof(int16_t) * (3 * (size_t)T + (T & 1)) + sizeof(int) * (size_t)T;
+    static int configured = 0;
+    if (configured < (int)sm) {
+        GALPHA_CUDA(cudaFuncSetAttribute(k_row_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        configured = (int)sm;
+    }
+    if (c.events) cudaEventRecord(c.kev[0], c.stream);
+    k_row_pass<<<T, kRowThreads, sm, c.stream>>>(c.ycol, c.idmap, c.colour, T, c.logT);
+    if (c.events) cudaEventRecord(c.kev[1], c.stream);
+    count_launch();
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
+int launch_emit(Ctx &c, int ntiles, long long nwin, bool write)
+{
+    if (c.events) cudaEventRecord(c.kev[write ? 6 : 4], c.stream);
+    if (!write)
+        k_emit_count<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.T, c.logT, nwin, c.ctr);
+    else
+        k_emit_write<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.tv, c.T, c.logT, nwin);
+    count_launch();
+    if (c.events) cudaEventRecord(c.kev[write ? 7 : 5], c.stream);
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
+}  // namespace galpha

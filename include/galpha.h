@@ -1,0 +1,116 @@
+/*
+ * galpha.h -- alpha-shape (GAlpha) boundary of the galpha-b200 engine, plus the
+ * re-entrant handle API used by the DT + alpha-spectrum hot path.
+ *
+ *   reference interface                                  replaced by
+ *   ---------------------------------------------------  -------------------------------
+ *   Alpha_Shapes_2D(PGPUDTPARAMS, PGPUDTOUTPUT)          galphaCompute(h, params, dt, out)
+ *     + computeAlphaShapes()                              (alpha of a host triangulation)
+ *     gpudt/AlphaShape/Alpha_Shapes_2D.h:43-121,
+ *     Alpha_Shapes_2D.cu:206-727
+ *   public members spectrum / private point_list,        GAlphaOutput arrays (same element
+ *     edge_list, tri_list (Alpha_Shapes_2D.h:100-117,      layouts as headers.h:48-90)
+ *     headers.h:48-64)
+ *   gpudtComputeDT then Alpha_Shapes_2D (main.cu:392-395) galphaTriangulate +
+ *                                                         galphaComputeResident (mesh stays in
+ *                                                         device memory between the two)
+ *
+ * Interval semantics (kernel.cu:219-624): the spectrum holds squared radii in
+ * increasing order, spectrum[0] = 0 is the sentinel "attached / not applicable";
+ * exactly equal values share one rank; every *_rank indexes the spectrum;
+ * nu_max_rank 0 on a hull edge means "infinity".  Edges are numbered as the
+ * reference numbers them: triangle t owns its edge i (opposite vtx[i]) when
+ * vtx[i+1] < vtx[i+2] or tri[i] == -1, edges ordered by t then i.
+ */
+#ifndef GALPHA_GALPHA_H
+#define GALPHA_GALPHA_H
+
+#include "gpudt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* headers.h:48-64 element layouts */
+typedef struct { int nu_min_rank, nu_max_rank; } galphaPointInterval;
+typedef struct {
+    int ro_rank, nu_min_rank, nu_max_rank;
+    int sc; /* simplex_category: 0 ATTACHED, 1 UNATTACHED */
+    int tIndex, vOpp;
+} galphaEdgeInterval;
+typedef struct { int ro_rank; } galphaTriangleInterval;
+
+typedef struct {
+    int nSpectrum;                    /* distinct values incl. the 0 sentinel */
+    double *spectrum;                 /* [nSpectrum] */
+    int nPoints;
+    galphaPointInterval *point_list;  /* [nPoints] */
+    int nEdges;
+    galphaEdgeInterval *edge_list;    /* [nEdges] */
+    int nTris;
+    galphaTriangleInterval *tri_list; /* [nTris] */
+    long long exactCompares;          /* spectrum comparisons resolved exactly */
+    long long exactTies;              /* exactly equal neighbours merged */
+    long long exactAttached;          /* attached tests resolved exactly */
+} GAlphaOutput;
+
+typedef struct galpha_ctx *galphaHandle;
+
+/* Stage indices of gpudtStatus.ms */
+#define GALPHA_STAGE_UPLOAD    0
+#define GALPHA_STAGE_VORONOI   1  /* scatter + column pass + row pass + islands */
+#define GALPHA_STAGE_TRIANGLES 2  /* Voronoi vertices -> triangles + links */
+#define GALPHA_STAGE_SHIFT     3  /* shifting + bad-case removal */
+#define GALPHA_STAGE_MISSING   4  /* missing-site insertion */
+#define GALPHA_STAGE_BOUNDARY  5  /* fake ring removal + hull */
+#define GALPHA_STAGE_FLIP      6  /* Lawson flipping */
+#define GALPHA_STAGE_COMPACT   7  /* compaction / output layout */
+#define GALPHA_STAGE_ALPHA     8  /* birth times + attached + sort + ranks + intervals */
+#define GALPHA_STAGE_DOWNLOAD  9
+#define GALPHA_STAGE_TOTAL     10
+
+/* Create a handle on CUDA device `device` (-1: current device).  Device memory
+ * is reserved lazily and grown on demand; budgetBytes (0: no limit) caps it. */
+int galphaCreate(int device, long long budgetBytes, galphaHandle *out);
+int galphaDestroy(galphaHandle h);
+/* Work on a caller stream (a cudaStream_t passed as void*; NULL: the handle's own). */
+int galphaSetStream(galphaHandle h, void *stream);
+
+/* Delaunay triangulation.  If out != NULL the triangles are copied to host
+ * (out->triangles allocated with new[], capacity 2 * nVerts, as gpudtComputeDT);
+ * the mesh also stays resident on the device for galphaComputeResident. */
+int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *out, gpudtStatus *st);
+
+/* Alpha spectrum + intervals of the handle's resident mesh. */
+int galphaComputeResident(galphaHandle h, GAlphaOutput *out);
+
+/* Alpha spectrum + intervals of a host triangulation (Alpha_Shapes_2D(pInput, pDT)). */
+int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *dt, GAlphaOutput *out);
+
+/* Device-resident hot path: points already in device memory (d_xy: 2*n doubles).
+ * Runs DT (+ alpha when withAlpha) and leaves every result on the device.
+ * Returns the status; counts through galphaGetCounts. */
+int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY,
+                    double maxX, double maxY, int fboSize, int withAlpha, gpudtStatus *st);
+
+/* Sizes of the last result: nTris, nEdges, nSpectrum (any pointer may be NULL). */
+int galphaGetCounts(galphaHandle h, int *nTris, int *nEdges, int *nSpectrum);
+
+/* Copy the resident triangles (gpudtTriangle layout) to host memory. */
+int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap);
+
+void galphaReleaseOutput(GAlphaOutput *out);
+
+/* Text of the last error on the calling thread. */
+const char *galphaLastError(void);
+
+/* Number of CUDA kernels this library has launched since it was loaded. */
+unsigned long long galphaLaunchCount(void);
+
+/* Version / build information string. */
+const char *galphaVersion(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

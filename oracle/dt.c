@@ -251,3 +251,62 @@ done:
     if (status < 0) return status;
     return c->nt;
 }
+
+/*
+ * Mesh validator: the invariants of the reference's checkResult (main.cu:163-343)
+ * with exact predicates, plus link symmetry and the convex-hull boundary.
+ * out[0] link errors, out[1] non-counterclockwise triangles, out[2] interior
+ * edges failing the exact empty-circle test (incircle > 0), out[3] hull edges,
+ * out[4] hull edges with some point strictly outside (non-convex hull),
+ * out[5] vertex indices out of range.
+ */
+int oracle_check_mesh(int npts, const double *xy, int ntri, const int *vtx, const int *nbr, long long *out)
+{
+    int t, i;
+    for (i = 0; i < 6; i++) out[i] = 0;
+    for (t = 0; t < ntri; t++)
+        for (i = 0; i < 3; i++)
+            if (vtx[3 * t + i] < 0 || vtx[3 * t + i] >= npts) out[5]++;
+    if (out[5]) return -1;
+    for (t = 0; t < ntri; t++) {
+        const int *v = vtx + 3 * t;
+        if (orx_orient2d(xy + 2 * v[0], xy + 2 * v[1], xy + 2 * v[2]) <= 0) out[1]++;
+        for (i = 0; i < 3; i++) {
+            int e = nbr[3 * t + i];
+            int a = v[(i + 1) % 3], b = v[(i + 2) % 3];
+            if (e < 0) {
+                out[3]++;
+                continue;
+            }
+            int u = e >> 2, j = e & 3;
+            if (u < 0 || u >= ntri || j > 2 || nbr[3 * u + j] != ((t << 2) | i) || vtx[3 * u + (j + 1) % 3] != b ||
+                vtx[3 * u + (j + 2) % 3] != a) {
+                out[0]++;
+                continue;
+            }
+            if (orx_incircle(xy + 2 * a, xy + 2 * b, xy + 2 * v[i], xy + 2 * vtx[3 * u + j]) > 0) out[2]++;
+        }
+    }
+    /* hull edges: no input point strictly to the right of a -> b */
+    {
+        int *ha = (int *)malloc(sizeof(int) * (size_t)(out[3] + 1)), *hb = (int *)malloc(sizeof(int) * (size_t)(out[3] + 1));
+        int nh = 0, k;
+        for (t = 0; t < ntri; t++)
+            for (i = 0; i < 3; i++)
+                if (nbr[3 * t + i] < 0) {
+                    ha[nh] = vtx[3 * t + (i + 1) % 3];
+                    hb[nh] = vtx[3 * t + (i + 2) % 3];
+                    nh++;
+                }
+        if (nh <= 4096)
+            for (k = 0; k < nh; k++)
+                for (i = 0; i < npts; i++)
+                    if (orx_orient2d(xy + 2 * ha[k], xy + 2 * hb[k], xy + 2 * i) < 0) {
+                        out[4]++;
+                        break;
+                    }
+        free(ha);
+        free(hb);
+    }
+    return 0;
+}

@@ -23,6 +23,10 @@ extern "C" {
  * Returns the triangle count or a negative ORACLE_ERR_*. */
 int oracle_dt(int npts, const double *xy, int cap, int *out_vtx, int *out_nbr, int *out_nkept);
 
+/* Validates a mesh; out[6]: link errors, non-CCW, non-Delaunay edges, hull
+ * edges, non-convex hull edges, bad indices. */
+int oracle_check_mesh(int npts, const double *xy, int ntri, const int *vtx, const int *nbr, long long *out);
+
 /* Exact sign predicates (for cross-checks of the product's predicates). */
 int oracle_orient2d(const double *a, const double *b, const double *c);
 int oracle_incircle(const double *a, const double *b, const double *c, const double *d);

@@ -54,6 +54,7 @@ def lib():
         L.oracle_incircle.argtypes = [_dp, _dp, _dp, _dp]
         L.oracle_exact_counts.argtypes = [ctypes.c_int]
         L.oracle_exact_counts.restype = ctypes.c_longlong
+        L.oracle_check_mesh.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, ctypes.POINTER(ctypes.c_longlong)]
         L.oracle_alpha_count_edges.argtypes = [ctypes.c_int, _ip, _ip]
         L.oracle_alpha.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, ctypes.POINTER(_AlphaOut)]
         L.oracle_compare_rho.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp]
@@ -84,6 +85,19 @@ def dt(points):
     if nt < 0:
         raise RuntimeError("oracle_dt failed with status %d" % nt)
     return vtx[:nt].copy(), nbr[:nt].copy(), int(kept[0])
+
+
+def check_mesh(points, vtx, nbr):
+    """Exact validation of a triangle mesh (checkResult invariants, main.cu:163-343).
+
+    Returns dict: links, ccw, delaunay, hull_edges, nonconvex, bad_index."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    vtx = np.ascontiguousarray(vtx, dtype=np.int32).reshape(-1, 3)
+    nbr = np.ascontiguousarray(nbr, dtype=np.int32).reshape(-1, 3)
+    out = (ctypes.c_longlong * 6)()
+    lib().oracle_check_mesh(pts.shape[0], _d(pts), vtx.shape[0], _i(vtx), _i(nbr), out)
+    keys = ["links", "ccw", "delaunay", "hull_edges", "nonconvex", "bad_index"]
+    return {k: int(out[i]) for i, k in enumerate(keys)}
 
 
 def alpha(points, vtx, nbr):

@@ -1,0 +1,39 @@
+"""Parity helpers for the alpha stage: compare engine output with oracle.alpha
+on the same triangle array (edge numbering follows triangle order,
+kernel.cu:138-217, so both sides must see identical triangles)."""
+import numpy as np
+
+from oracle import oracle as O
+
+
+def ulp_diff(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    ia = a.view(np.int64)
+    ib = b.view(np.int64)
+    return np.abs(ia - ib)
+
+
+def compare_alpha(points, vtx, nbr, res, ulp_tol=4):
+    """res: dict from Engine.alpha_*().  Returns (ok, report)."""
+    ref = O.alpha(points, vtx, nbr)
+    rep = {}
+    spec, rspec = res["spectrum"], ref["spectrum"]
+    rep["nspec"] = (len(spec), len(rspec))
+    same_len = len(spec) == len(rspec)
+    maxulp = int(ulp_diff(spec, rspec).max()) if same_len and len(spec) else -1
+    rep["spectrum_max_ulp"] = maxulp
+    rep["ref_formula_max_ulp"] = int(ulp_diff(ref["spectrum_ref"], rspec).max()) if len(rspec) else 0
+    tri_ok = np.array_equal(res["tri_list"]["ro_rank"], ref["tri_ro"])
+    e = res["edge_list"]
+    E = ref["edge"]
+    edge_ok = (len(e) == len(E) and np.array_equal(e["ro_rank"], E[:, 2]) and np.array_equal(e["nu_min_rank"], E[:, 3])
+               and np.array_equal(e["nu_max_rank"], E[:, 4]) and np.array_equal(e["tIndex"], E[:, 5])
+               and np.array_equal(e["vOpp"], E[:, 6]))
+    p = res["point_list"]
+    pt_ok = np.array_equal(p["nu_min_rank"], ref["point"][:, 0]) and np.array_equal(p["nu_max_rank"], ref["point"][:, 1])
+    rep.update(tri_ok=tri_ok, edge_ok=edge_ok, point_ok=pt_ok)
+    ok = same_len and 0 <= maxulp <= ulp_tol and tri_ok and edge_ok and pt_ok
+    if len(spec) == 1 and same_len:
+        ok = tri_ok and edge_ok and pt_ok
+    return ok, rep

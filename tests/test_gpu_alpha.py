@@ -1,0 +1,84 @@
+"""GPU parity tests of the alpha spectrum and intervals (Alpha_Shapes_2D).
+
+The CUDA result is compared with the CPU oracle on the same triangle array
+(edge numbering follows triangle order, kernel.cu:138-217): ranks and
+intervals identical, spectrum values within 4 ulp of the exact-then-rounded
+FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import galpha_b200 as G
+from galpha_b200 import datasets as D
+from alphacheck import compare_alpha
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+ULP_TOL = 4
+
+
+def both(engine, pts, fbo):
+    p = G.GPUDTParams(pts, fboSize=fbo)
+    dt = engine.triangulate(p)
+    return p, dt, engine.alpha_resident()
+
+
+def test_c1_alpha(engine):
+    pts, fbo = D.make("c1")
+    p, dt, a = both(engine, pts, fbo)
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+    assert ok, rep
+    g = np.load(os.path.join(GOLD, "golden_c1.npz"))
+    assert np.array_equal(a["spectrum"], g["spectrum"])
+
+
+@pytest.mark.parametrize("name,fbo", [("bird", 512), ("alpha", 512), ("1000_1", 2048), ("10000_1", 2048)])
+def test_reference_fixtures_alpha(engine, name, fbo):
+    pts = np.load(os.path.join(GOLD, "golden_ref_%s.npz" % name))["points"]
+    p, dt, a = both(engine, pts, fbo)
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+    assert ok, rep
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_alpha(engine, seed):
+    rng = np.random.default_rng(300 + seed)
+    for pts in (rng.random((8000, 2)), D.degenerate_mix(8000, seed), np.floor(rng.random((4000, 2)) * 32) / 32):
+        p, dt, a = both(engine, pts, 1024)
+        ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+        assert ok, rep
+
+
+def test_alpha_of_host_mesh_matches_resident(engine):
+    pts = np.random.default_rng(11).random((5000, 2))
+    p, dt, a = both(engine, pts, 1024)
+    b = engine.alpha_of(p, dt)
+    for k in ("spectrum", "point_list", "edge_list", "tri_list"):
+        assert np.array_equal(a[k], b[k]), k
+    shapes = G.AlphaShapes2D(p, dt, engine=engine).compute_alpha_shapes()
+    assert np.array_equal(shapes.spectrum, a["spectrum"])
+
+
+def test_alpha_empty_and_tiny(engine):
+    p, dt, a = both(engine, np.array([[0, 0], [1, 1.0]]), 256)
+    assert dt.nTris == 0 and list(a["spectrum"]) == [0.0]
+    assert (a["point_list"]["nu_min_rank"] == -1).all()
+    pts = np.array([[0, 0], [1, 0], [0, 1.0]])
+    p, dt, a = both(engine, pts, 256)
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+    assert ok, rep
+    assert list(a["spectrum"]) == [0.0, 0.25, 0.5]
+
+
+def test_large_alpha_properties(engine):
+    """c2 size: the spectrum is strictly increasing and every rank is in range."""
+    pts, fbo = D.make("c2")
+    p, dt, a = both(engine, pts, fbo)
+    s = a["spectrum"]
+    assert s[0] == 0.0 and np.all(np.diff(s[1:]) >= 0)
+    ro = a["tri_list"]["ro_rank"]
+    assert ro.min() >= 1 and ro.max() < len(s)
+    e = a["edge_list"]
+    assert e["ro_rank"].max() < len(s) and (e["nu_min_rank"] <= np.where(e["nu_max_rank"] == 0, 1 << 30, e["nu_max_rank"])).all()

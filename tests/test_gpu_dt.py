@@ -1,0 +1,158 @@
+"""GPU parity tests of the Delaunay triangulation (gpudtComputeDT contract).
+
+Every case runs the CUDA library through its C ABI and compares with the CPU
+oracle on the same seeded inputs: identical canonical triangle sets where the
+DT is unique, the exact checkResult invariants (main.cu:163-343) plus the same
+triangle count, vertex set and hull where it is not (cocircular input).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import galpha_b200 as G
+from galpha_b200 import datasets as D
+from dtcheck import compare_dt
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def run(engine, pts, fbo, **kw):
+    return engine.triangulate(G.GPUDTParams(pts, fboSize=fbo, **kw))
+
+
+def assert_parity(pts, dt, must_be_identical):
+    ok, rep = compare_dt(pts, dt.vtx, dt.tri)
+    assert ok, rep
+    if must_be_identical:
+        assert rep["identical"], rep
+
+
+def test_config_c1_identical(engine):
+    pts, fbo = D.make("c1")
+    dt = run(engine, pts, fbo)
+    assert_parity(pts, dt, True)
+    g = np.load(os.path.join(GOLD, "golden_c1.npz"))
+    assert dt.nTris == len(g["triangles"])
+
+
+@pytest.mark.parametrize("name,fbo", [("bird", 512), ("alpha", 512), ("1000_1", 2048), ("10000_1", 2048)])
+def test_reference_fixtures(engine, name, fbo):
+    g = np.load(os.path.join(GOLD, "golden_ref_%s.npz" % name))
+    pts = g["points"]
+    dt = run(engine, pts, fbo)
+    # the reference's integer-coordinate fixtures have cocircular quads
+    assert_parity(pts, dt, False)
+    assert dt.nTris == len(g["triangles"])
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("fbo", [256, 1024])
+def test_uniform_random(engine, seed, fbo):
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(10, 20000))
+    pts = rng.random((n, 2))
+    assert_parity(pts, run(engine, pts, fbo), True)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_gaussian_and_clusters(engine, seed):
+    rng = np.random.default_rng(200 + seed)
+    n = 5000
+    g = rng.normal(0, 1, (n, 2))
+    assert_parity(g, run(engine, g, 512), True)
+    c = rng.random((8, 2))
+    cl = c[rng.integers(0, 8, n)] + rng.normal(0, 0.002, (n, 2))
+    assert_parity(cl, run(engine, cl, 1024), True)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_degenerate_mix(engine, seed):
+    pts = D.degenerate_mix(20000, 50 + seed)
+    dt = run(engine, pts, 2048)
+    assert_parity(pts, dt, False)
+    assert dt.status.nDuplicates > 0
+
+
+def test_duplicates_keep_lowest_index(engine):
+    rng = np.random.default_rng(5)
+    base = rng.random((500, 2))
+    pts = np.concatenate([base, base[::-1]])  # index i and 999-i coincide
+    dt = run(engine, pts, 512)
+    assert_parity(pts, dt, True)
+    used = np.unique(dt.vtx)
+    assert used.max() < 500
+
+
+def test_lattice_cocircular(engine):
+    g = np.stack(np.meshgrid(np.arange(64), np.arange(64)), -1).reshape(-1, 2) / 64.0
+    dt = run(engine, g, 1024)
+    assert_parity(g, dt, False)
+    assert dt.nTris == 2 * 63 * 63
+
+
+@pytest.mark.parametrize("pts,ntri", [
+    ([[0, 0], [1, 0], [0, 1]], 1),
+    ([[0, 0], [1, 0], [0, 1], [1, 1.2]], 2),
+    ([[0, 0], [1, 1]], 0),
+    ([[0, 0], [1, 1], [2, 2], [3, 3]], 0),
+    ([[0.5, 0.5]] * 6, 0),
+])
+def test_tiny_and_degenerate(engine, pts, ntri):
+    pts = np.asarray(pts, dtype=np.float64)
+    dt = run(engine, pts, 256)
+    assert dt.nTris == ntri
+    if ntri:
+        assert_parity(pts, dt, True)
+
+
+def test_deterministic_and_reusable(engine):
+    rng = np.random.default_rng(9)
+    a = rng.random((30000, 2))
+    b = rng.random((700, 2))
+    d1 = run(engine, a, 2048)
+    d2 = run(engine, b, 256)
+    d3 = run(engine, a, 2048)
+    assert np.array_equal(d1.triangles, d3.triangles)
+    assert_parity(b, d2, True)
+
+
+def test_errors(engine):
+    pts = np.random.default_rng(1).random((100, 2))
+    with pytest.raises(G.GpudtError) as e:
+        run(engine, pts, 300)          # not a power of two
+    assert e.value.code == -1
+    bad = pts.copy()
+    bad[3, 0] = np.nan
+    with pytest.raises(G.GpudtError) as e:
+        run(engine, bad, 512)
+    assert e.value.code == -1
+    with pytest.raises(G.GpudtError) as e:  # caller bounds that do not hold the points
+        run(engine, pts, 512, minX=0.2)
+    assert e.value.code == -1
+    with pytest.raises(G.GpudtError) as e:
+        G.Engine(budget_bytes=1 << 20).triangulate(G.GPUDTParams(pts, fboSize=512))
+    assert e.value.code == -3
+    # the engine stays usable after errors
+    assert_parity(pts, run(engine, pts, 512), True)
+
+
+def test_reference_entry_point_symbols():
+    L = G.load()
+    for sym in ["_Z14gpudtComputeDTP11GPUDTPARAMS", "_Z20gpudtReleaseDTOutputP11GPUDTOUTPUT", "gpudtComputeDTEx"]:
+        assert hasattr(L, sym)
+    out = G.gpudt_compute_dt(G.GPUDTParams(np.random.default_rng(2).random((300, 2)), fboSize=512))
+    assert out.nTris > 0
+
+
+def test_large_uniform_properties(engine):
+    """c2 size (4M points, texture 8192): exact validity of the full mesh."""
+    pts, fbo = D.make("c2")
+    dt = run(engine, pts, fbo)
+    chk = O.check_mesh(pts, dt.vtx, dt.tri)
+    assert chk["links"] == 0 and chk["ccw"] == 0 and chk["delaunay"] == 0 and chk["bad_index"] == 0, chk
+    n = len(np.unique(dt.vtx))
+    assert n == len(pts)
+    assert dt.nTris == 2 * n - 2 - chk["hull_edges"]
