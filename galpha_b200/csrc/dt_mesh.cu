@@ -326,6 +326,69 @@ struct ShiftRound {
     }
 };
 
+// Optimistic shifting: every undecided site is a candidate for its true
+// position; a triangle that would not stay counterclockwise with its candidate
+// vertices moved drops those candidates; repeated until no triangle drops
+// anything.  At the fixed point every triangle is counterclockwise with all
+// remaining candidates moved together, so they are committed at once and only
+// the dropped sites go through the priority rounds (ShiftRound).
+struct ShiftCandidates {
+    const int8_t *vstate;
+    int8_t *cand;
+    __device__ void operator()(long long i) const { cand[i] = vstate[i] == VS_UNDECIDED ? 1 : 0; }
+};
+
+struct ShiftCheckTris {
+    const int4 *tv;
+    const double2 *pos, *opos;
+    int8_t *cand, *drop;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int4 v = tv[ii];
+        if (v.x < 0) return;
+        int8_t c0 = cand[v.x], c1 = cand[v.y], c2 = cand[v.z];
+        if (!(c0 | c1 | c2)) return;
+        double2 a = c0 ? opos[v.x] : pos[v.x];
+        double2 b = c1 ? opos[v.y] : pos[v.y];
+        double2 c = c2 ? opos[v.z] : pos[v.z];
+        if (orientp(a, b, c, ct) > 0) return;
+        if (c0) drop[v.x] = 1;
+        if (c1) drop[v.y] = 1;
+        if (c2) drop[v.z] = 1;
+    }
+};
+
+struct ShiftDrop {
+    int8_t *cand, *drop;
+    Counters *ct;
+    __device__ void operator()(long long i) const
+    {
+        if (drop[i]) {
+            drop[i] = 0;
+            if (cand[i]) {
+                cand[i] = 0;
+                atomicAdd(&ct->changed, 1);
+            }
+        }
+    }
+};
+
+struct ShiftCommit {
+    const int8_t *cand;
+    double2 *pos;
+    const double2 *opos;
+    int8_t *vstate;
+    int *vround;
+    __device__ void operator()(long long i) const
+    {
+        if (!cand[i]) return;
+        pos[i] = opos[i];
+        vstate[i] = VS_SHIFTED;
+        vround[i] = 1;  // decided before the priority rounds start
+    }
+};
+
 // Select BAD vertices that are the priority minimum among their BAD neighbours.
 struct BadSelect {
     const int4 *tv, *tn;
@@ -500,8 +563,27 @@ static int run_counts(Ctx &c) { return read_counters(c); }
 int stage_shift(Ctx &c)
 {
     int r;
-    // vertices fixed from the start (fake ring) count as decided in round 1
     int shiftRounds = 0, badCount = 0;
+    {
+        r = read_counters(c);
+        if (r) return r;
+        int nt = c.hctr->ntris;
+        int8_t *cand = (int8_t *)c.list2, *drop = (int8_t *)c.list2 + ((c.V + 255) & ~255);
+        launch_n(c, ShiftCandidates{c.vstate, cand}, c.V);
+        GALPHA_CUDA(cudaMemsetAsync(drop, 0, (size_t)c.V, c.stream));
+        for (int it = 0; it < kMaxRounds; it++) {
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+            launch_n(c, ShiftCheckTris{c.tv, c.pos, c.opos, cand, drop, c.ctr}, nt);
+            launch_n(c, ShiftDrop{cand, drop, c.ctr}, c.V);
+            r = read_counters(c);
+            if (r) return r;
+            shiftRounds++;
+            if (c.hctr->changed == 0) break;
+        }
+        launch_n(c, ShiftCommit{cand, c.pos, c.opos, c.vstate, c.vround}, c.V);
+    }
+    // vertices fixed from the start (fake ring) and the optimistic set count
+    // as decided in round 1; the rest go through priority rounds
     for (int round = 2;; round++) {
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int) + 0, c.stream));
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));

@@ -12,7 +12,7 @@ import pytest
 
 import galpha_b200 as G
 from galpha_b200 import datasets as D
-from dtcheck import compare_dt
+from dtcheck import canon_set, compare_dt
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -115,7 +115,9 @@ def test_deterministic_and_reusable(engine):
     d1 = run(engine, a, 2048)
     d2 = run(engine, b, 256)
     d3 = run(engine, a, 2048)
-    assert np.array_equal(d1.triangles, d3.triangles)
+    # the triangle set is deterministic; the slot order, like the reference's,
+    # depends on the order of concurrent work-list appends
+    assert canon_set(d1.vtx) == canon_set(d3.vtx)
     assert_parity(b, d2, True)
 
 
