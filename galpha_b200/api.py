@@ -194,6 +194,35 @@ class DTOutput:
         return self.triangles["tri"]
 
 
+class _HostPool:
+    """Reused host output buffers, pinned when torch is available (one DMA copy
+    per result instead of a pageable copy)."""
+
+    def __init__(self):
+        self._bufs = {}
+        self._keep = {}
+        try:
+            import torch
+
+            self._torch = torch if torch.cuda.is_available() else None
+        except Exception:
+            self._torch = None
+
+    def get(self, name, n, dtype):
+        dtype = np.dtype(dtype)
+        a = self._bufs.get(name)
+        if a is None or len(a) < n or a.dtype != dtype:
+            nbytes = max(1, int(n) * dtype.itemsize)
+            if self._torch is not None:
+                t = self._torch.empty(nbytes, dtype=self._torch.uint8, pin_memory=True)
+                self._keep[name] = t
+                a = t.numpy().view(dtype)[: max(1, int(n))]
+            else:
+                a = np.empty(max(1, int(n)), dtype=dtype)
+            self._bufs[name] = a
+        return a
+
+
 class Engine:
     """A libgalpha handle: one CUDA stream and one device arena, reused across calls."""
 
@@ -202,6 +231,8 @@ class Engine:
         h = ctypes.c_void_p()
         _check(self._L.galphaCreate(device, budget_bytes, ctypes.byref(h)), "galphaCreate")
         self._h = h
+        self._pool = _HostPool()
+        self._npoints = 0
 
     def close(self):
         if getattr(self, "_h", None):
@@ -214,37 +245,66 @@ class Engine:
         except Exception:
             pass
 
-    def triangulate(self, params):
-        """Delaunay triangulation of params (gpudtComputeDT semantics)."""
+    def triangulate(self, params, copy=True):
+        """Delaunay triangulation of params (gpudtComputeDT semantics).
+
+        With copy=False the triangle array is a view of a reused pinned buffer,
+        valid until the next call on this engine."""
         cp = params._c()
+        cap = 2 * params.nPoints + 64
+        buf = self._pool.get("tri", cap, TRIANGLE_DTYPE)
         out = _Output()
+        out.triangles = buf.ctypes.data
+        out.nTris = len(buf)
         st = Status()
         _check(self._L.galphaTriangulate(self._h, ctypes.byref(cp), ctypes.byref(out), ctypes.byref(st)),
                "galphaTriangulate")
-        n = out.nTris
-        arr = np.empty(n, dtype=TRIANGLE_DTYPE)
-        if n:
-            ctypes.memmove(arr.ctypes.data, out.triangles, n * TRIANGLE_DTYPE.itemsize)
-        self._L.gpudt_release_dt_output(ctypes.byref(out))
-        return DTOutput(arr, st)
+        self._npoints = params.nPoints
+        arr = buf[: out.nTris]
+        return DTOutput(arr.copy() if copy else arr, st)
 
-    def alpha_resident(self):
-        """Alpha spectrum + intervals of the mesh left on the device by triangulate()."""
+    def _alpha_bufs(self, n, nt):
+        ne = 3 * max(n, 1) + 8
         out = _AlphaOut()
-        _check(self._L.galphaComputeResident(self._h, ctypes.byref(out)), "galphaComputeResident")
-        return _alpha_arrays(self._L, out)
+        sp = self._pool.get("spec", 1 + nt + ne, np.float64)
+        pt = self._pool.get("pt", max(n, 1), POINT_INTERVAL_DTYPE)
+        ed = self._pool.get("edge", ne, EDGE_INTERVAL_DTYPE)
+        tr = self._pool.get("trilist", max(nt, 1), TRIANGLE_INTERVAL_DTYPE)
+        out.spectrum, out.nSpectrum = sp.ctypes.data, len(sp)
+        out.point_list, out.nPoints = pt.ctypes.data, len(pt)
+        out.edge_list, out.nEdges = ed.ctypes.data, len(ed)
+        out.tri_list, out.nTris = tr.ctypes.data, len(tr)
+        return out, (sp, pt, ed, tr)
 
-    def alpha_of(self, params, dt):
+    def _alpha_result(self, out, bufs, copy):
+        sp, pt, ed, tr = bufs
+        res = {
+            "spectrum": sp[: out.nSpectrum], "point_list": pt[: out.nPoints],
+            "edge_list": ed[: out.nEdges], "tri_list": tr[: out.nTris],
+        }
+        if copy:
+            res = {k: v.copy() for k, v in res.items()}
+        res.update(exactCompares=out.exactCompares, exactTies=out.exactTies, exactAttached=out.exactAttached)
+        return res
+
+    def alpha_resident(self, copy=True):
+        """Alpha spectrum + intervals of the mesh left on the device by triangulate()."""
+        nt = self.counts()[0]
+        out, bufs = self._alpha_bufs(self._npoints, nt)
+        _check(self._L.galphaComputeResident(self._h, ctypes.byref(out)), "galphaComputeResident")
+        return self._alpha_result(out, bufs, copy)
+
+    def alpha_of(self, params, dt, copy=True):
         """Alpha spectrum + intervals of a given triangulation (Alpha_Shapes_2D(pInput, pDT))."""
         cp = params._c()
         tri = np.ascontiguousarray(dt.triangles)
         o = _Output()
         o.triangles = tri.ctypes.data if len(tri) else None
         o.nTris = len(tri)
-        out = _AlphaOut()
+        out, bufs = self._alpha_bufs(params.nPoints, len(tri))
         _check(self._L.galphaCompute(self._h, ctypes.byref(cp), ctypes.byref(o), ctypes.byref(out)),
                "galphaCompute")
-        return _alpha_arrays(self._L, out)
+        return self._alpha_result(out, bufs, copy)
 
     def run_device(self, d_xy_ptr, n, bounds, fbo_size, with_alpha=True):
         """Hot path on device-resident points (d_xy_ptr: device address of 2n doubles)."""
@@ -252,6 +312,7 @@ class Engine:
         _check(self._L.galphaRunDevice(self._h, ctypes.c_void_p(d_xy_ptr), n, bounds[0], bounds[1], bounds[2],
                                        bounds[3], fbo_size, 1 if with_alpha else 0, ctypes.byref(st)),
                "galphaRunDevice")
+        self._npoints = n
         return st
 
     def counts(self):
@@ -261,26 +322,6 @@ class Engine:
 
     def set_stream(self, stream_ptr):
         _check(self._L.galphaSetStream(self._h, ctypes.c_void_p(stream_ptr)), "galphaSetStream")
-
-
-def _alpha_arrays(L, out):
-    def take(ptr, n, dtype):
-        a = np.empty(n, dtype=dtype)
-        if n:
-            ctypes.memmove(a.ctypes.data, ptr, n * np.dtype(dtype).itemsize)
-        return a
-
-    res = {
-        "spectrum": take(out.spectrum, out.nSpectrum, np.float64),
-        "point_list": take(out.point_list, out.nPoints, POINT_INTERVAL_DTYPE),
-        "edge_list": take(out.edge_list, out.nEdges, EDGE_INTERVAL_DTYPE),
-        "tri_list": take(out.tri_list, out.nTris, TRIANGLE_INTERVAL_DTYPE),
-        "exactCompares": out.exactCompares,
-        "exactTies": out.exactTies,
-        "exactAttached": out.exactAttached,
-    }
-    L.galphaReleaseOutput(ctypes.byref(out))
-    return res
 
 
 _default_engine = None

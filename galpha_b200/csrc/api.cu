@@ -111,6 +111,7 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(rank, int, 3 * cap);
     TAKE(spectrum, double, 3 * cap);
     TAKE(outtri, gpudtTriangle, cap);
+    TAKE(edge_aos, galphaEdgeInterval, 2 * cap);
     TAKE(ctr, Counters, 1);
 #undef TAKE
     return total + 4096;
@@ -416,11 +417,22 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
                    params->fboSize);
     if (!r && out) {
         int n = params->nPoints;
-        int nv = n + std::max(4, (int)(std::sqrt((double)n) / 10));
-        int capacity = std::max(2 * nv, c.nT_out);
-        gpudtTriangle *tris = new (std::nothrow) gpudtTriangle[capacity > 0 ? capacity : 1];
-        if (!tris) r = GPUDT_ERR_NOMEM;
-        else {
+        gpudtTriangle *tris = nullptr;
+        if (out->triangles) {
+            // caller buffer: out->nTris is its capacity
+            if (out->nTris < c.nT_out) {
+                g_err = "galphaTriangulate: output buffer too small";
+                r = GPUDT_ERR_NOMEM;
+            } else {
+                tris = out->triangles;
+            }
+        } else {
+            int nv = n + std::max(4, (int)(std::sqrt((double)n) / 10));
+            int capacity = std::max(2 * nv, c.nT_out);
+            tris = new (std::nothrow) gpudtTriangle[capacity > 0 ? capacity : 1];
+            if (!tris) r = GPUDT_ERR_NOMEM;
+        }
+        if (!r) {
             if (c.nT_out > 0) {
                 cudaError_t e = cudaMemcpyAsync(tris, c.outtri, sizeof(gpudtTriangle) * (size_t)c.nT_out,
                                                 cudaMemcpyDeviceToHost, c.stream);
@@ -461,54 +473,68 @@ int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap)
     return GPUDT_OK;
 }
 
+// Edge records in the reference's edge_interval layout, built on the device.
+struct EdgeAos {
+    const int4 *edges;
+    const int *ero;
+    const int2 *enu;
+    galphaEdgeInterval *out;
+    __device__ void operator()(long long e) const
+    {
+        galphaEdgeInterval E;
+        int4 q = edges[e];
+        E.ro_rank = ero[e];
+        E.nu_min_rank = enu[e].x;
+        E.nu_max_rank = enu[e].y;
+        E.sc = E.ro_rank == 0 ? 0 : 1;
+        E.tIndex = q.z;
+        E.vOpp = q.w;
+        out[e] = E;
+    }
+};
+
+// Copies the alpha result to host memory.  When the caller passes buffers
+// (non-NULL pointers, capacities in the count fields) they are filled in place
+// -- pinned buffers make these single DMA copies; otherwise the arrays are
+// allocated with malloc and released by galphaReleaseOutput.
 static int download_alpha(Ctx &c, GAlphaOutput *out)
 {
-    memset(out, 0, sizeof(*out));
+    bool caller = out->spectrum && out->point_list && out->edge_list && out->tri_list;
+    if (caller) {
+        if (out->nSpectrum < c.nSpec || out->nPoints < c.N || out->nEdges < c.nE || out->nTris < c.nT_out) {
+            g_err = "galphaComputeResident: output buffers too small (see galphaGetCounts)";
+            return GPUDT_ERR_NOMEM;
+        }
+    } else {
+        memset(out, 0, sizeof(*out));
+        out->spectrum = (double *)malloc(sizeof(double) * (size_t)std::max(1, c.nSpec));
+        out->point_list = (galphaPointInterval *)malloc(sizeof(galphaPointInterval) * (size_t)std::max(1, c.N));
+        out->edge_list = (galphaEdgeInterval *)malloc(sizeof(galphaEdgeInterval) * (size_t)std::max(1, c.nE));
+        out->tri_list = (galphaTriangleInterval *)malloc(sizeof(galphaTriangleInterval) * (size_t)std::max(1, c.nT_out));
+        if (!out->spectrum || !out->point_list || !out->edge_list || !out->tri_list) {
+            galphaReleaseOutput(out);
+            return GPUDT_ERR_NOMEM;
+        }
+    }
     out->nSpectrum = c.nSpec;
     out->nPoints = c.N;
     out->nEdges = c.nE;
     out->nTris = c.nT_out;
-    out->spectrum = (double *)malloc(sizeof(double) * (size_t)std::max(1, c.nSpec));
-    out->point_list = (galphaPointInterval *)malloc(sizeof(galphaPointInterval) * (size_t)std::max(1, c.N));
-    out->edge_list = (galphaEdgeInterval *)malloc(sizeof(galphaEdgeInterval) * (size_t)std::max(1, c.nE));
-    out->tri_list = (galphaTriangleInterval *)malloc(sizeof(galphaTriangleInterval) * (size_t)std::max(1, c.nT_out));
-    int4 *edges = (int4 *)malloc(sizeof(int4) * (size_t)std::max(1, c.nE));
-    int *ero = (int *)malloc(sizeof(int) * (size_t)std::max(1, c.nE));
-    int2 *enu = (int2 *)malloc(sizeof(int2) * (size_t)std::max(1, c.nE));
-    if (!out->spectrum || !out->point_list || !out->edge_list || !out->tri_list || !edges || !ero || !enu) {
-        free(edges);
-        free(ero);
-        free(enu);
-        galphaReleaseOutput(out);
-        return GPUDT_ERR_NOMEM;
-    }
     cudaStream_t s = c.stream;
+    galphaEdgeInterval *d_edges = (galphaEdgeInterval *)c.edge_aos;
+    launch_n(c, EdgeAos{c.edges, c.edge_ro, c.edge_nu, d_edges}, c.nE);
     GALPHA_CUDA(cudaMemcpyAsync(out->spectrum, c.spectrum, sizeof(double) * (size_t)c.nSpec, cudaMemcpyDeviceToHost, s));
     if (c.N > 0)
         GALPHA_CUDA(cudaMemcpyAsync(out->point_list, c.pt_nu, sizeof(int2) * (size_t)c.N, cudaMemcpyDeviceToHost, s));
     if (c.nT_out > 0)
         GALPHA_CUDA(cudaMemcpyAsync(out->tri_list, c.tri_ro, sizeof(int) * (size_t)c.nT_out, cudaMemcpyDeviceToHost, s));
-    if (c.nE > 0) {
-        GALPHA_CUDA(cudaMemcpyAsync(edges, c.edges, sizeof(int4) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
-        GALPHA_CUDA(cudaMemcpyAsync(ero, c.edge_ro, sizeof(int) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
-        GALPHA_CUDA(cudaMemcpyAsync(enu, c.edge_nu, sizeof(int2) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
-    }
+    if (c.nE > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(out->edge_list, d_edges, sizeof(galphaEdgeInterval) * (size_t)c.nE,
+                                    cudaMemcpyDeviceToHost, s));
     GALPHA_CUDA(cudaStreamSynchronize(s));
-    for (int e = 0; e < c.nE; e++) {
-        galphaEdgeInterval &E = out->edge_list[e];
-        E.ro_rank = ero[e];
-        E.nu_min_rank = enu[e].x;
-        E.nu_max_rank = enu[e].y;
-        E.sc = ero[e] == 0 ? 0 : 1;
-        E.tIndex = edges[e].z;
-        E.vOpp = edges[e].w;
-    }
     out->exactCompares = (long long)c.hctr->exact_compares;
     out->exactTies = c.hctr->nties;
     out->exactAttached = (long long)c.hctr->exact_attached;
-    free(edges);
-    free(ero);
-    free(enu);
     return GPUDT_OK;
 }
 

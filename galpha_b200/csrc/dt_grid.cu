@@ -356,6 +356,31 @@ int stage_voronoi(Ctx &c)
     int W2 = ((T >> 6) + 31) / 32;
     int r0 = launch_column_pass(c, W2);
     if (r0) return r0;
+    // Fused path: colours stay in shared memory and the dual triangles are
+    // emitted directly.  Sparse inputs (mean site spacing above 16 pixels)
+    // make the per-pixel window scan long, so they take the envelope path.
+    c.fused_done = false;
+    long long D = T - 2 * kMargin;
+    if ((long long)c.N * 256 >= D * D) {
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, sizeof(int), c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nisland, 0, sizeof(int), c.stream));
+        r0 = launch_vd_tri(c);
+        if (r0) return r0;
+        r0 = read_counters(c);
+        if (r0) return r0;
+        if (c.hctr->err) return c.hctr->err;
+        int nflag = c.hctr->nisland;
+        c.st.nIslandPixels = nflag;  // tiles with island pixels, repaired locally
+        if (nflag > 0) {
+            r0 = launch_vd_repair(c, nflag);
+            if (r0) return r0;
+            r0 = read_counters(c);
+            if (r0) return r0;
+            if (c.hctr->err) return c.hctr->err;
+        }
+        c.fused_done = true;
+        return GPUDT_OK;
+    }
     r0 = launch_row_pass(c);
     if (r0) return r0;
     GALPHA_CUDA(cudaGetLastError());
@@ -400,6 +425,7 @@ int stage_voronoi(Ctx &c)
 
 int stage_triangles(Ctx &c)
 {
+    if (c.fused_done) return GPUDT_OK;  // emitted by the fused kernel
     const int T = c.T;
     long long nwin = (long long)(T - 1) * (T - 1);
     int ntiles = (int)((nwin + kEmitTile - 1) / kEmitTile);

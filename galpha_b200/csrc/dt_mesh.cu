@@ -94,11 +94,18 @@ __device__ __forceinline__ void set_fwd(int4 *fwd, int t, int i, int loc)
     p[i] = loc;
 }
 
-__device__ __forceinline__ int alloc_slot(int *freelist, Counters *ct)
+// Pops a free slot, else takes one from the tail; -1 (and GPUDT_ERR_NOMEM)
+// when the slot array is full.
+__device__ __forceinline__ int alloc_slot(int *freelist, Counters *ct, int cap)
 {
     int k = atomicSub(&ct->nfree, 1) - 1;
     if (k >= 0) return freelist[k];
-    return atomicAdd(&ct->ntris, 1);
+    int s = atomicAdd(&ct->ntris, 1);
+    if (s >= cap) {
+        set_err(ct, GPUDT_ERR_NOMEM, 5);
+        return -1;
+    }
+    return s;
 }
 
 __device__ __forceinline__ void free_slot(int4 *tv, int *freelist, Counters *ct, int t)
@@ -115,24 +122,29 @@ struct CountDeg {
     __device__ void operator()(long long i) const
     {
         int4 v = tv[i];
+        if (v.x < 0) return;  // released slot
         atomicAdd(&deg[v.x], 1);
         atomicAdd(&deg[v.y], 1);
         atomicAdd(&deg[v.z], 1);
     }
 };
 
+// Incidence entry of vertex v in triangle t (v = vtx[k]): the oriented slot
+// and the next vertex counterclockwise, so matching reads only the list.
 struct FillInc {
     const int4 *tv;
     const int *start;
-    int *cursor, *inc;
+    int *cursor;
+    int2 *inc;
     __device__ void operator()(long long i) const
     {
         int t = (int)i;
         int4 v = tv[t];
+        if (v.x < 0) return;
         int a[3] = {v.x, v.y, v.z};
         for (int k = 0; k < 3; k++) {
             int s = start[a[k]] + atomicAdd(&cursor[a[k]], 1);
-            inc[s] = enc(t, k);
+            inc[s] = make_int2(enc(t, k), a[p1(k)]);
         }
     }
 };
@@ -140,33 +152,33 @@ struct FillInc {
 struct MatchLinks {
     const int4 *tv;
     int4 *tn;
-    const int *start, *inc;
+    const int *start;
+    const int2 *inc;
     int *vtri;
     Counters *ct;
     __device__ void operator()(long long i) const
     {
         int t = (int)i;
         int4 v = tv[t];
+        if (v.x < 0) {
+            tn[t] = make_int4(-1, -1, -1, 0);
+            return;
+        }
         int n[3];
         for (int k = 0; k < 3; k++) {
             int a = geti(v, p1(k)), b = geti(v, m1(k));  // edge a -> b, opposite vtx[k]
             int found = -1, cnt = 0, same = 0;
-            for (int s = start[b]; s < start[b + 1]; s++) {
-                int e = inc[s], u = dtri(e), j = dori(e);
-                int4 w = tv[u];
-                if (geti(w, p1(j)) == a) {  // u has b -> a
-                    found = enc(u, m1(j));
+            for (int s = start[b], e = start[b + 1]; s < e; s++) {
+                int2 x = inc[s];
+                if (x.y == a) {  // a triangle with b -> a
+                    found = enc(dtri(x.x), m1(dori(x.x)));
                     cnt++;
                 }
             }
-            for (int s = start[a]; s < start[a + 1]; s++) {
-                int e = inc[s], u = dtri(e), j = dori(e);
-                if (geti(tv[u], p1(j)) == b) same++;  // triangles with a -> b
-            }
+            for (int s = start[a], e = start[a + 1]; s < e; s++) same += inc[s].y == b;  // a -> b
             if (cnt > 1 || same != 1) set_err(ct, GPUDT_ERR_TOPOLOGY, 20);
             if (found < 0) atomicAdd(&ct->changed, 1);  // hull edge
             n[k] = found;
-            if (k == 0) vtri[v.x] = enc(t, 0);
         }
         tn[t] = make_int4(n[0], n[1], n[2], 0);
     }
@@ -179,6 +191,7 @@ struct SetVtri {
     {
         int t = (int)i;
         int4 v = tv[t];
+        if (v.x < 0) return;
         vtri[v.x] = enc(t, 0);
         vtri[v.y] = enc(t, 1);
         vtri[v.z] = enc(t, 2);
@@ -197,9 +210,10 @@ int stage_links(Ctx &c)
     r = exclusive_scan_int(c, deg, start, c.V + 1, nullptr);
     if (r) return r;
     GALPHA_CUDA(cudaMemsetAsync(deg, 0, sizeof(int) * (size_t)(c.V + 1), c.stream));
-    launch_n(c, FillInc{c.tv, start, deg, c.inc}, nt);
+    int2 *inc = (int2 *)c.rec;  // relink records are not in use yet: 3*cap int2
+    launch_n(c, FillInc{c.tv, start, deg, inc}, nt);
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-    launch_n(c, MatchLinks{c.tv, c.tn, start, c.inc, c.vtri, c.ctr}, nt);
+    launch_n(c, MatchLinks{c.tv, c.tn, start, inc, c.vtri, c.ctr}, nt);
     launch_n(c, SetVtri{c.tv, c.vtri}, nt);
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
@@ -773,7 +787,7 @@ struct MissingInsert {
     int8_t *vstate;
     const int *list, *loc, *kind;
     Relink *rec;
-    int round;
+    int round, cap;
     Counters *ct;
     __device__ void operator()(long long ii) const
     {
@@ -790,7 +804,8 @@ struct MissingInsert {
         int4 v = tv[t], n = tn[t];
         if (k == 0) {
             int v0 = v.x, v1 = v.y, v2 = v.z;
-            int s1 = alloc_slot(freelist, ct), s2 = alloc_slot(freelist, ct);
+            int s1 = alloc_slot(freelist, ct, cap), s2 = alloc_slot(freelist, ct, cap);
+            if (s1 < 0 || s2 < 0) return;
             epoch[t] = round;
             tv[t] = make_int4(p, v1, v2, 0);
             tv[s1] = make_int4(p, v2, v0, 0);
@@ -815,7 +830,8 @@ struct MissingInsert {
             int4 wv = tv[u], wn = tn[u];
             int w = geti(wv, j);
             int ou1 = geti(wn, p1(j)), ou2 = geti(wn, m1(j));
-            int s1 = alloc_slot(freelist, ct), s2 = alloc_slot(freelist, ct);
+            int s1 = alloc_slot(freelist, ct, cap), s2 = alloc_slot(freelist, ct, cap);
+            if (s1 < 0 || s2 < 0) return;
             epoch[t] = round;
             epoch[u] = round;
             // A = t (p,v2,v0), B = s1 (p,v0,v1), C = u (p,v1,w), D = s2 (p,w,v2)
@@ -911,7 +927,7 @@ int stage_missing(Ctx &c)
                  nmiss);
         launch_n(c, EdgeTags{c.tn, loc, kind, c.list2, c.ctr}, nmiss);
         launch_n(c, MissingInsert{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.vote, c.pos, c.opos, c.vstate,
-                                  c.list, loc, kind, c.rec, round, c.ctr},
+                                  c.list, loc, kind, c.rec, round, c.cap_tris, c.ctr},
                  nmiss);
         r = read_counters(c);
         if (r) return r;
@@ -944,15 +960,26 @@ int stage_missing(Ctx &c)
 // ---------------------------------------------------------------- boundary
 // Fan of a hull vertex f: from the clockwise-most triangle (whose edge f->u0 is
 // a hull edge) counterclockwise to the triangle whose edge ud->f is a hull edge.
+// Fake ring sites are removed class by class (ring index mod 4 in the order
+// 0, 2, 1, 3): sites of one class are separated along the border by sites of
+// other classes that are still present, so they are not adjacent and their
+// fans are disjoint; the priority test below only matters in the rare case of
+// an edge cutting a texture corner.
 struct FakeSelect {
     const int4 *tv, *tn;
     const int8_t *vstate;
     const int *vtri;
     int *list;
-    int N, F;
+    int *count;
+    int N, F, cls;
     Counters *ct;
+    __device__ bool conflicts(int f, int g, uint32_t pf) const
+    {
+        return g >= N && vstate[g] == VS_FAKE && ((g - N) & 3) == cls && prio((uint32_t)g) < pf;
+    }
     __device__ void operator()(long long ii) const
     {
+        if (((int)ii & 3) != cls) return;
         int f = N + (int)ii;
         if (vstate[f] != VS_FAKE) return;
         uint32_t pf = prio((uint32_t)f);
@@ -962,8 +989,7 @@ struct FakeSelect {
             int t = dtri(e), i = dori(e);
             int4 w = tv[t];
             int a = geti(w, p1(i)), b = geti(w, m1(i));
-            if ((vstate[a] == VS_FAKE && prio((uint32_t)a) < pf) || (vstate[b] == VS_FAKE && prio((uint32_t)b) < pf))
-                return;
+            if (conflicts(f, a, pf) || conflicts(f, b, pf)) return;
             int nx = geti(tn[t], m1(i));  // across (f, a)
             if (nx < 0) break;
             e = enc(dtri(nx), m1(dori(nx)));
@@ -977,14 +1003,23 @@ struct FakeSelect {
         for (int guard = 0; guard < 8 * kMaxFan; guard++) {
             int t = dtri(e), i = dori(e);
             int4 w = tv[t];
-            int b = geti(w, m1(i));
-            if (vstate[b] == VS_FAKE && prio((uint32_t)b) < pf) return;
+            if (conflicts(f, geti(w, m1(i)), pf)) return;
             int nx = geti(tn[t], p1(i));  // across (b, f)
             if (nx < 0) break;
             e = enc(dtri(nx), p1(dori(nx)));
         }
-        int k = atomicAdd(&ct->nlist, 1);
+        int k = atomicAdd(count, 1);
         list[k] = f;
+        atomicAdd(&ct->changed, 1);
+    }
+};
+
+struct ZeroInts {
+    int *a, *b;
+    __device__ void operator()(long long) const
+    {
+        *a = 0;
+        if (b) *b = 0;
     }
 };
 
@@ -1150,7 +1185,7 @@ struct Convexify {
     const double2 *pos;
     int *vtri, *freelist;
     const int *list;
-    int nlist;
+    int nlist, cap;
     Counters *ct;
     __device__ void operator()(long long) const;
 };
@@ -1170,7 +1205,8 @@ __device__ void Convexify::operator()(long long) const
         int u, w, tin, tout;
         if (!hull_neighbours(tv, tn, v, vtri[v], &u, &w, &tin, &tout)) continue;
         if (orientp(pos[u], pos[v], pos[w], ct) >= 0) continue;
-        int s = alloc_slot(freelist, ct);
+        int s = alloc_slot(freelist, ct, cap);
+        if (s < 0) return;
         // (u, w, v): opp u (0) = w->v, the reverse of hull edge v->w (tout);
         //            opp w (1) = v->u, the reverse of hull edge u->v (tin); opp v (2) = new hull u->w
         tv[s] = make_int4(u, w, v, 0);
@@ -1192,30 +1228,31 @@ __device__ void Convexify::operator()(long long) const
 
 int stage_boundary(Ctx &c)
 {
-    int r, guard = 0;
+    int r;
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
     int *cand = c.aux;  // boundary candidates
+    const int order[4] = {0, 2, 1, 3};
+    const long long recn = 4LL * c.cap_tris;
     int removed = 0;
-    while (removed < c.F) {
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-        launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.N, c.F, c.ctr}, c.F);
+    for (int pass = 0; removed < c.F; pass++) {
+        if (pass > kMaxRounds / 4) return GPUDT_ERR_NOCONVERGE;
+        for (int q = 0; q < 4; q++) {
+            int round = next_round(c);
+            launch_n(c, ZeroInts{&c.ctr->nlist, &c.ctr->nrec}, 1);
+            launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, &c.ctr->nlist, c.N, c.F, order[q], c.ctr},
+                     c.F);
+            launch_dev(c, FakeRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, c.pos, c.vstate, c.rec,
+                                     cand, round, c.ctr},
+                       &c.ctr->nlist, c.F);
+            launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
+        }
+        GALPHA_CUDA(cudaGetLastError());
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        int nsel = c.hctr->nlist;
-        if (nsel == 0) return GPUDT_ERR_NOCONVERGE;
-        int round = next_round(c);
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
-        launch_n(c, FakeRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, c.pos, c.vstate, c.rec, cand,
-                               round, c.ctr},
-                 nsel);
-        r = read_counters(c);
-        if (r) return r;
-        if (c.hctr->err) return c.hctr->err;
-        r = run_relink(c, round, c.hctr->nrec);
-        if (r) return r;
-        removed += nsel;
-        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (c.hctr->changed == removed) return GPUDT_ERR_NOCONVERGE;  // a full pass removed nothing
+        removed = c.hctr->changed;
     }
     r = read_counters(c);
     if (r) return r;
@@ -1225,7 +1262,7 @@ int stage_boundary(Ctx &c)
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->nlist > 0) {
-        launch_n(c, Convexify{c.tv, c.tn, c.pos, c.vtri, c.freelist, c.list, c.hctr->nlist, c.ctr}, 1);
+        launch_n(c, Convexify{c.tv, c.tn, c.pos, c.vtri, c.freelist, c.list, c.hctr->nlist, c.cap_tris, c.ctr}, 1);
         GALPHA_CUDA(cudaGetLastError());
         r = read_counters(c);
         if (r) return r;
@@ -1239,11 +1276,16 @@ int stage_boundary(Ctx &c)
 }
 
 // -------------------------------------------------------------------- flip
+// Rounds run back to back on device-side counts (ping-pong active lists);
+// the host looks at the counters only every kFlipSync rounds.
+constexpr int kFlipSync = 4;
+
 struct FlipCheck {
     const int4 *tv, *tn;
     const double2 *pos;
     const int *act;
     int *vote, *prop, *target, *cands;
+    int *cand_n;
     Counters *ct;
     __device__ void operator()(long long ii) const
     {
@@ -1268,14 +1310,14 @@ struct FlipCheck {
                     return;
                 }
             } else {
-                atomicAdd(&ct->filt_incircle, 1ull);
+                warp_count(&ct->filt_incircle);
             }
             if (s > 0) {
                 prop[t] = i;
                 target[t] = u;
                 atomicMin(&vote[t], t);
                 atomicMin(&vote[u], t);
-                int k = atomicAdd(&ct->nlist, 1);
+                int k = atomicAdd(cand_n, 1);
                 cands[k] = t;
                 return;
             }
@@ -1286,6 +1328,7 @@ struct FlipCheck {
 struct FlipApply {
     int4 *tv, *tn, *fwd;
     int *epoch, *vtri, *vote, *stamp, *next;
+    int *next_n;
     const int *prop, *target, *cands;
     Relink *rec;
     int round;
@@ -1294,7 +1337,7 @@ struct FlipApply {
     {
         if (x < 0) return;
         if (atomicExch(&stamp[x], round) != round) {
-            int k = atomicAdd(&ct->nlist2, 1);
+            int k = atomicAdd(next_n, 1);
             next[k] = x;
         }
     }
@@ -1358,14 +1401,29 @@ struct FlipReset {
     }
 };
 
+// Start of a flip round: the next list becomes current (counts stay in the
+// counter block; the host alternates the list buffers).
+struct FlipRoundStart {
+    int p;  // parity of the round: act[p] is current
+    Counters *ct;
+    __device__ void operator()(long long) const
+    {
+        ct->act[1 - p] = 0;
+        ct->flips_total += ct->nflips;
+        ct->nflips = 0;
+        ct->cand = 0;
+        ct->nrec = 0;
+    }
+};
+
 struct AllAlive {
     const int4 *tv;
     int *list;
-    Counters *ct;
+    int *count;
     __device__ void operator()(long long i) const
     {
         if (tv[i].x >= 0) {
-            int k = atomicAdd(&ct->nlist, 1);
+            int k = atomicAdd(count, 1);
             list[k] = (int)i;
         }
     }
@@ -1376,40 +1434,37 @@ int stage_flip(Ctx &c)
     int r = read_counters(c);
     if (r) return r;
     int nt = c.hctr->ntris;
-    int *act = c.list, *nxt = c.list2;
+    int *lists[2] = {c.list, c.list2};
     int *prop = c.aux, *target = c.aux2, *cands = c.inc, *stamp = c.stamp;
-    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-    launch_n(c, AllAlive{c.tv, act, c.ctr}, nt);
-    r = read_counters(c);
-    if (r) return r;
-    int nact = c.hctr->nlist;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->act[0], 0, 2 * sizeof(int), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->flips_total, 0, sizeof(int), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nflips, 0, sizeof(int), c.stream));
+    launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
-    int rounds = 0;
-    long long flips = 0;
-    while (nact > 0) {
-        int round = next_round(c);
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 3 * sizeof(int), c.stream));  // nlist, nlist2, nrec
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nflips, 0, sizeof(int), c.stream));
-        launch_n(c, FlipCheck{c.tv, c.tn, c.pos, act, c.vote, prop, target, cands, c.ctr}, nact);
+    const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
+    int rounds = 0, done = 0;
+    while (!done) {
+        for (int k = 0; k < kFlipSync; k++) {
+            int p = rounds & 1;
+            int round = next_round(c);
+            launch_n(c, FlipRoundStart{p, c.ctr}, 1);
+            launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand, c.ctr},
+                       &c.ctr->act[p], capn);
+            launch_dev(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, lists[1 - p],
+                                    &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr},
+                       &c.ctr->cand, capn);
+            launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
+            launch_dev(c, FlipReset{c.vote, target, cands}, &c.ctr->cand, capn);
+            rounds++;
+        }
+        GALPHA_CUDA(cudaGetLastError());
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        int ncand = c.hctr->nlist;
-        if (ncand == 0) break;
-        launch_n(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nxt, prop, target, cands, c.rec,
-                              round, c.ctr},
-                 ncand);
-        r = read_counters(c);
-        if (r) return r;
-        r = run_relink(c, round, c.hctr->nrec);
-        if (r) return r;
-        launch_n(c, FlipReset{c.vote, target, cands}, ncand);
-        flips += c.hctr->nflips;
-        nact = c.hctr->nlist2;
-        std::swap(act, nxt);
-        if (++rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        done = c.hctr->act[rounds & 1] == 0;
+        if (rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
     }
-    c.st.nFlips = (int)flips;
+    c.st.nFlips = c.hctr->flips_total + c.hctr->nflips;
     c.st.flipRounds = rounds;
     return GPUDT_OK;
 }

@@ -47,7 +47,10 @@ struct Counters {
     int nisland;    // island pixels
     int nflips;     // flips this round
     int nties;      // exact spectrum ties merged
-    int pad[5];
+    int act[2];     // flip: active-list lengths (ping-pong)
+    int cand;       // flip: candidates this round
+    int flips_total;
+    int pad[1];
     unsigned long long exact_compares;
     unsigned long long exact_orient;
     unsigned long long exact_incircle;
@@ -130,6 +133,7 @@ struct Ctx {
     int *hist = nullptr;       // scan scratch
     int *rhist = nullptr;      // radix sort histograms
     gpudtTriangle *outtri = nullptr;  // [cap] AoS output staging
+    galphaEdgeInterval *edge_aos = nullptr;  // [2*cap] edge records for download
 
     DevBuf bufs[64];
     int nbufs = 0;
@@ -140,6 +144,7 @@ struct Ctx {
     bool events = false;
     gpudtStatus st;
     bool have_mesh = false, have_alpha = false;
+    bool fused_done = false;  // triangles came from the fused colour + dual kernel
 };
 
 // ------------------------------------------------------------- error helpers
@@ -170,6 +175,28 @@ __global__ void __launch_bounds__(256) k_for_each(F f, long long n)
     for (; i < n; i += stride) f(i);
 }
 
+// Grid-stride launch over [0, *n) with the count read on the device, so a
+// round of kernels can run without the host learning its size.
+template <class F>
+__global__ void __launch_bounds__(256) k_for_each_dev(F f, const int *n)
+{
+    long long nn = *n;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < nn; i += stride) f(i);
+}
+
+template <class F>
+inline void launch_dev(const Ctx &c, F f, const int *n_dev, long long max_n)
+{
+    if (max_n <= 0) return;
+    long long blocks = (max_n + 255) / 256;
+    long long maxb = (long long)c.sm_count * 8;
+    if (blocks > maxb) blocks = maxb;
+    k_for_each_dev<<<(unsigned)blocks, 256, 0, c.stream>>>(f, n_dev);
+    count_launch();
+}
+
 template <class F>
 inline void launch_n(const Ctx &c, F f, long long n)
 {
@@ -186,6 +213,13 @@ inline void launch_n(const Ctx &c, F f, long long n)
 __device__ __forceinline__ void set_err(Counters *ct, int code, int info)
 {
     if (atomicCAS(&ct->err, 0, code) == 0) ct->errinfo = info;
+}
+
+// Counts one event per calling thread with one atomic per warp.
+__device__ __forceinline__ void warp_count(unsigned long long *c)
+{
+    unsigned m = __activemask();
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(c, (unsigned long long)__popc(m));
 }
 
 // 32-bit invertible mix (murmur3 finaliser): a random-looking priority per id.
@@ -232,6 +266,8 @@ constexpr int kEmitTile = kEmitThreads;
 int launch_column_pass(Ctx &c, int W2);
 int launch_row_pass(Ctx &c);
 int launch_emit(Ctx &c, int ntiles, long long nwin, bool write);
+int launch_vd_tri(Ctx &c);
+int launch_vd_repair(Ctx &c, int nflag);
 // LSD radix sort of (keys, vals) ascending (sort.cu)
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n);
 

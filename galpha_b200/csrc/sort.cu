@@ -93,15 +93,23 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long l
     }
 }
 
-struct OrXor {
-    const unsigned long long *keys;
-    unsigned long long *acc;  // [0] = first key, [1] = OR of xor
-    __device__ void operator()(long long i) const
-    {
-        unsigned long long x = keys[i] ^ acc[0];
+// OR over all keys of (key XOR first key): the bits on which keys differ.
+// Reduced per warp and per block; one 64-bit atomic per block.
+__global__ void __launch_bounds__(256) k_or_xor(const unsigned long long *__restrict__ keys, long long n,
+                                                unsigned long long *acc)
+{
+    __shared__ unsigned long long ws[8];
+    unsigned long long k0 = acc[0], x = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x |= keys[i] ^ k0;
+    for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; w++) x |= ws[w];
         if (x) atomicOr(&acc[1], x);
     }
-};
+}
 
 // Sorts (keys, vals)[0..n) ascending; result in keys/vals.  Uses keys2/vals2.
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
@@ -110,7 +118,11 @@ int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *
     unsigned long long *acc = (unsigned long long *)c.rhist;
     GALPHA_CUDA(cudaMemcpyAsync(acc, keys, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(acc + 1, 0, sizeof(unsigned long long), c.stream));
-    launch_n(c, OrXor{keys, acc}, n);
+    {
+        long long blocks = std::min<long long>((n + 255) / 256, (long long)c.sm_count * 4);
+        k_or_xor<<<(unsigned)blocks, 256, 0, c.stream>>>(keys, n, acc);
+        count_launch();
+    }
     unsigned long long hv[2];
     GALPHA_CUDA(cudaMemcpyAsync(hv, acc, sizeof(hv), cudaMemcpyDeviceToHost, c.stream));
     GALPHA_CUDA(cudaStreamSynchronize(c.stream));

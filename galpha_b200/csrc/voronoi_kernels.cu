@@ -327,6 +327,374 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit_write(const int *__restri
 }
 
 
+// ------------------------------------------------- fused colour + dual
+// One CTA owns a tile of KT_W x KT_H windows.  It colours the tile's pixels plus
+// a one-pixel halo (rows y0-1 .. y0+KT_H+1) by an exact window scan over the
+// column candidates, keeps the colours as packed site pixel coordinates in
+// shared memory, checks the island property on every pixel the windows use,
+// and emits the dual triangles of the tile -- the colour texture never goes
+// to HBM.  A tile with an island pixel emits nothing and raises a flag; the
+// host then runs the envelope path (k_row_pass + island repair + k_emit_*).
+//
+// Window scan: owner(x, y) = argmin over columns cx of (d, cx) with
+// d = (x - cx)^2 + (y - ycol[y][cx])^2 (ties: smaller column; within a column
+// the column pass already kept the upper site).  Columns are visited at
+// growing distance k from x; the scan stops once k^2 exceeds the best d, which
+// no further column can beat.  This is the same assignment k_row_pass makes.
+constexpr int KT_W = 128, KT_H = 8;
+constexpr int KT_CW = KT_W + 3, KT_CH = KT_H + 3;  // coloured pixels incl. halo
+constexpr int kFusedThreads = 256;
+
+__device__ __forceinline__ unsigned owner_scan(const int16_t *__restrict__ row, int x, int y, int T)
+{
+    long long bestd = 0x7fffffffffffffffLL;
+    int bx = -1;
+    int yc = row[x];
+    if (yc >= 0) {
+        bestd = (long long)(y - yc) * (y - yc);
+        bx = x;
+    }
+    for (int k = 1; (long long)k * k <= bestd || bx < 0; k++) {
+        if (k >= T) break;
+        long long kk = (long long)k * k;
+        int xl = x - k, xr = x + k;
+        if (xl >= 0) {
+            int c = row[xl];
+            if (c >= 0) {
+                long long d = kk + (long long)(y - c) * (y - c);
+                if (d < bestd || (d == bestd && xl < bx)) {
+                    bestd = d;
+                    bx = xl;
+                }
+            }
+        }
+        if (xr < T) {
+            int c = row[xr];
+            if (c >= 0) {
+                long long d = kk + (long long)(y - c) * (y - c);
+                if (d < bestd) {
+                    bestd = d;
+                    bx = xr;
+                }
+            }
+        }
+    }
+    int sy = row[bx];
+    return ((unsigned)sy << 16) | (unsigned)bx;
+}
+
+__device__ __forceinline__ long long orient_pk(unsigned a, unsigned b, unsigned c)
+{
+    int ax = a & 0xffff, ay = a >> 16, bx = b & 0xffff, by = b >> 16, cx = c & 0xffff, cy = c >> 16;
+    return (long long)(ax - cx) * (by - cy) - (long long)(ay - cy) * (bx - cx);
+}
+
+__global__ void __launch_bounds__(kFusedThreads) k_vd_tri(const int16_t *__restrict__ ycol,
+                                                          const int *__restrict__ idmap, int4 *__restrict__ tv,
+                                                          int2 *__restrict__ chunk, int *__restrict__ flagged,
+                                                          int T, int logT, int cap, Counters *ct)
+{
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    __shared__ unsigned col[KT_CH][KT_CW];
+    __shared__ int tile_island;
+    const int x0 = blockIdx.x * KT_W, y0 = blockIdx.y * KT_H;
+    if (threadIdx.x == 0) tile_island = 0;
+    // 1. colours of pixels (x0-1 .. x0+KT_W+1) x (y0-1 .. y0+KT_H+1), clamped
+    for (int k = threadIdx.x; k < KT_CH * KT_CW; k += kFusedThreads) {
+        int ly = k / KT_CW, lx = k - ly * KT_CW;
+        int x = x0 - 1 + lx, y = y0 - 1 + ly;
+        unsigned o = 0xffffffffu;
+        if (x >= 0 && y >= 0 && x < T && y < T) o = owner_scan(ycol + ((size_t)y << logT), x, y, T);
+        col[ly][lx] = o;
+    }
+    __syncthreads();
+    // 2. island test on every pixel a window of this tile uses
+    for (int k = threadIdx.x; k < (KT_H + 1) * (KT_W + 1); k += kFusedThreads) {
+        int ly = k / (KT_W + 1), lx = k - ly * (KT_W + 1);
+        int x = x0 + lx, y = y0 + ly;
+        if (x >= T || y >= T) continue;
+        unsigned c = col[ly + 1][lx + 1];
+        int sx = c & 0xffff, sy = c >> 16;
+        int dx = (sx > x) - (sx < x), dy = (sy > y) - (sy < y);
+        if (dx == 0 && dy == 0) continue;
+        bool ok = (dx != 0 && col[ly + 1][lx + 1 + dx] == c) || (dy != 0 && col[ly + 1 + dy][lx + 1] == c) ||
+                  (dx != 0 && dy != 0 && col[ly + 1 + dy][lx + 1 + dx] == c);
+        if (!ok) tile_island = 1;
+    }
+    __syncthreads();
+    if (tile_island) {
+        if (threadIdx.x == 0) {
+            chunk[tile] = make_int2(0, 0);
+            flagged[atomicAdd(&ct->nisland, 1)] = tile;
+        }
+        return;
+    }
+    // 3. dual triangles of the tile's windows (x, y) .. (x+1, y+1)
+    int n = 0;
+    unsigned tri[2 * (KT_H * KT_W / kFusedThreads)][3];
+    for (int k = threadIdx.x; k < KT_H * KT_W; k += kFusedThreads) {
+        int ly = k / KT_W, lx = k - ly * KT_W;
+        int x = x0 + lx, y = y0 + ly;
+        if (x >= T - 1 || y >= T - 1) continue;
+        unsigned c[4] = {col[ly + 1][lx + 1], col[ly + 1][lx + 2], col[ly + 2][lx + 2], col[ly + 2][lx + 1]};
+        if (c[0] == c[2] || c[1] == c[3]) continue;
+        unsigned L[4];
+        int m = 0;
+        for (int q = 0; q < 4; q++)
+            if (c[q] != c[(q + 3) & 3]) L[m++] = c[q];
+        if (m == 3) {
+            if (orient_pk(L[0], L[1], L[2]) <= 0) set_err(ct, GPUDT_ERR_TOPOLOGY, 11);
+            tri[n][0] = L[0];
+            tri[n][1] = L[1];
+            tri[n][2] = L[2];
+            n++;
+        } else if (m == 4) {
+            if (orient_pk(L[0], L[1], L[2]) > 0 && orient_pk(L[0], L[2], L[3]) > 0) {
+                tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
+                tri[n][0] = L[0]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
+            } else {
+                if (orient_pk(L[1], L[2], L[3]) <= 0 || orient_pk(L[1], L[3], L[0]) <= 0)
+                    set_err(ct, GPUDT_ERR_TOPOLOGY, 12);
+                tri[n][0] = L[1]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
+                tri[n][0] = L[1]; tri[n][1] = L[3]; tri[n][2] = L[0]; n++;
+            }
+        }
+    }
+    // block-wide offsets, one atomic per block
+    __shared__ int warpsum[kFusedThreads / 32];
+    __shared__ int base;
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int incl = n;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warpsum[w] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int q = 0; q < kFusedThreads / 32; q++) {
+            int v = warpsum[q];
+            warpsum[q] = s;
+            s += v;
+        }
+        base = s ? atomicAdd(&ct->ntris, s) : 0;
+        if (base + s > cap) set_err(ct, GPUDT_ERR_NOMEM, 13);
+        chunk[tile] = make_int2(base, s);
+    }
+    __syncthreads();
+    int off = base + warpsum[w] + incl - n;
+    if (off + n > cap) return;
+    for (int q = 0; q < n; q++) {
+        int a = idmap[((size_t)(tri[q][0] >> 16) << logT) + (tri[q][0] & 0xffff)];
+        int b = idmap[((size_t)(tri[q][1] >> 16) << logT) + (tri[q][1] & 0xffff)];
+        int c = idmap[((size_t)(tri[q][2] >> 16) << logT) + (tri[q][2] & 0xffff)];
+        tv[off + q] = make_int4(a, b, c, 0);
+    }
+}
+
+// Island repair for one tile: colours the tile with an 8-pixel margin, marks
+// island components (iterated isolation test, the repeat loop of
+// cudaIslandDetection, cudaVoronoi.cu:220-247), recolours them from their
+// non-island neighbours (each island pixel takes, among its 8 neighbours
+// already coloured, the site nearest to it; ties: smaller packed coordinate;
+// Jacobi rounds), and emits the tile's triangles.  Neighbouring tiles see the
+// same small components and make the same decisions.
+constexpr int KS_M = 8;
+constexpr int KS_W = KT_W + 1 + 2 * KS_M, KS_H = KT_H + 1 + 2 * KS_M;
+
+__global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *__restrict__ ycol,
+                                                                 const int *__restrict__ idmap,
+                                                                 int4 *__restrict__ tv, const int *__restrict__ tiles,
+                                                                 int tiles_x, int T, int logT, int cap, Counters *ct)
+{
+    __shared__ unsigned col[KS_H][KS_W];
+    __shared__ unsigned nxt[KS_H][KS_W];
+    __shared__ int changed, pending;
+    const int tile = tiles[blockIdx.x];
+    const int x0 = (tile % tiles_x) * KT_W, y0 = (tile / tiles_x) * KT_H;
+    const int gx = x0 - KS_M, gy = y0 - KS_M;  // pixel of col[0][0]
+    const unsigned NONE = 0xffffffffu, ISL = 0xfffffffeu;
+    for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+        int ly = k / KS_W, lx = k - ly * KS_W;
+        int x = gx + lx, y = gy + ly;
+        col[ly][lx] = (x >= 0 && y >= 0 && x < T && y < T) ? owner_scan(ycol + ((size_t)y << logT), x, y, T) : NONE;
+    }
+    __syncthreads();
+    // mark island components: a pixel whose toward-site neighbours (all inside
+    // the region) carry neither its colour is marked; repeat
+    for (int round = 0; round < KS_M; round++) {
+        if (threadIdx.x == 0) changed = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+            int ly = k / KS_W, lx = k - ly * KS_W;
+            unsigned c = col[ly][lx];
+            nxt[ly][lx] = c;
+            if (c >= ISL || ly == 0 || lx == 0 || ly == KS_H - 1 || lx == KS_W - 1) continue;
+            int x = gx + lx, y = gy + ly;
+            int sx = c & 0xffff, sy = c >> 16;
+            int dx = (sx > x) - (sx < x), dy = (sy > y) - (sy < y);
+            if (dx == 0 && dy == 0) continue;
+            bool ok = (dx != 0 && col[ly][lx + dx] == c) || (dy != 0 && col[ly + dy][lx] == c) ||
+                      (dx != 0 && dy != 0 && col[ly + dy][lx + dx] == c);
+            if (!ok) {
+                nxt[ly][lx] = ISL;
+                changed = 1;
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+            int ly = k / KS_W, lx = k - ly * KS_W;
+            col[ly][lx] = nxt[ly][lx];
+        }
+        __syncthreads();
+        if (!changed) break;
+    }
+    // recolour
+    for (int round = 0; round < 4 * KS_M; round++) {
+        if (threadIdx.x == 0) pending = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+            int ly = k / KS_W, lx = k - ly * KS_W;
+            unsigned c = col[ly][lx];
+            nxt[ly][lx] = c;
+            if (c != ISL) continue;
+            int x = gx + lx, y = gy + ly;
+            long long bd = -1;
+            unsigned bc = ISL;
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    int yy = ly + dy, xx = lx + dx;
+                    if ((!dx && !dy) || yy < 0 || xx < 0 || yy >= KS_H || xx >= KS_W) continue;
+                    unsigned q = col[yy][xx];
+                    if (q >= ISL) continue;
+                    int sx = q & 0xffff, sy = q >> 16;
+                    long long d = (long long)(sx - x) * (sx - x) + (long long)(sy - y) * (sy - y);
+                    if (bd < 0 || d < bd || (d == bd && q < bc)) {
+                        bd = d;
+                        bc = q;
+                    }
+                }
+            nxt[ly][lx] = bc;
+            if (bc == ISL) pending = 1;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+            int ly = k / KS_W, lx = k - ly * KS_W;
+            col[ly][lx] = nxt[ly][lx];
+        }
+        __syncthreads();
+        if (!pending) break;
+    }
+    // emit the tile's windows
+    int n = 0;
+    unsigned tri[2 * (KT_H * KT_W / kFusedThreads)][3];
+    for (int k = threadIdx.x; k < KT_H * KT_W; k += kFusedThreads) {
+        int ly = k / KT_W, lx = k - ly * KT_W;
+        int x = x0 + lx, y = y0 + ly;
+        if (x >= T - 1 || y >= T - 1) continue;
+        int py = ly + KS_M, px = lx + KS_M;
+        unsigned c[4] = {col[py][px], col[py][px + 1], col[py + 1][px + 1], col[py + 1][px]};
+        if (c[0] >= ISL || c[1] >= ISL || c[2] >= ISL || c[3] >= ISL) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 15);
+            continue;
+        }
+        if (c[0] == c[2] || c[1] == c[3]) continue;
+        unsigned L[4];
+        int m = 0;
+        for (int q = 0; q < 4; q++)
+            if (c[q] != c[(q + 3) & 3]) L[m++] = c[q];
+        if (m == 3) {
+            if (orient_pk(L[0], L[1], L[2]) <= 0) set_err(ct, GPUDT_ERR_TOPOLOGY, 16);
+            tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
+        } else if (m == 4) {
+            if (orient_pk(L[0], L[1], L[2]) > 0 && orient_pk(L[0], L[2], L[3]) > 0) {
+                tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
+                tri[n][0] = L[0]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
+            } else {
+                if (orient_pk(L[1], L[2], L[3]) <= 0 || orient_pk(L[1], L[3], L[0]) <= 0)
+                    set_err(ct, GPUDT_ERR_TOPOLOGY, 17);
+                tri[n][0] = L[1]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
+                tri[n][0] = L[1]; tri[n][1] = L[3]; tri[n][2] = L[0]; n++;
+            }
+        }
+    }
+    for (int q = 0; q < n; q++) {
+        int s = atomicAdd(&ct->ntris, 1);
+        if (s >= cap) {
+            set_err(ct, GPUDT_ERR_NOMEM, 18);
+            return;
+        }
+        int a = idmap[((size_t)(tri[q][0] >> 16) << logT) + (tri[q][0] & 0xffff)];
+        int b = idmap[((size_t)(tri[q][1] >> 16) << logT) + (tri[q][1] & 0xffff)];
+        int cc = idmap[((size_t)(tri[q][2] >> 16) << logT) + (tri[q][2] & 0xffff)];
+        tv[s] = make_int4(a, b, cc, 0);
+    }
+}
+
+// Redo set = flagged tiles and their 8 neighbours; their fast-path triangles
+// are released (dead slots: vertex 0 = -1, pushed on the free list).
+__global__ void k_redo_mark(const int *flagged, int nflag, unsigned char *redo, int tiles_x, int tiles_y)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nflag) return;
+    int t = flagged[i], tx = t % tiles_x, ty = t / tiles_x;
+    for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+            int x = tx + dx, y = ty + dy;
+            if (x >= 0 && y >= 0 && x < tiles_x && y < tiles_y) redo[y * tiles_x + x] = 1;
+        }
+}
+
+__global__ void k_redo_collect(const unsigned char *redo, int ntiles, const int2 *chunk, int4 *tv, int *list,
+                               int *freelist, Counters *ct)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles || !redo[t]) return;
+    list[atomicAdd(&ct->nlist, 1)] = t;
+    int2 ch = chunk[t];
+    for (int q = 0; q < ch.y; q++) {
+        tv[ch.x + q] = make_int4(-1, -1, -1, 0);
+        freelist[atomicAdd(&ct->nfree, 1)] = ch.x + q;
+    }
+}
+
+int launch_vd_repair(Ctx &c, int nflag)
+{
+    const int T = c.T;
+    int tiles_x = (T - 1 + KT_W - 1) / KT_W, tiles_y = (T - 1 + KT_H - 1) / KT_H;
+    int ntiles = tiles_x * tiles_y;
+    unsigned char *redo = (unsigned char *)c.aux;
+    GALPHA_CUDA(cudaMemsetAsync(redo, 0, (size_t)ntiles, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    k_redo_mark<<<(nflag + 127) / 128, 128, 0, c.stream>>>(c.list2, nflag, redo, tiles_x, tiles_y);
+    count_launch();
+    k_redo_collect<<<(ntiles + 255) / 256, 256, 0, c.stream>>>(redo, ntiles, (const int2 *)c.colour, c.tv, c.list,
+                                                                c.freelist, c.ctr);
+    count_launch();
+    int r = read_counters(c);
+    if (r) return r;
+    int nredo = c.hctr->nlist;
+    k_vd_tri_repair<<<nredo, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, c.list, tiles_x, T, c.logT,
+                                                           c.cap_tris, c.ctr);
+    count_launch();
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
+int launch_vd_tri(Ctx &c)
+{
+    const int T = c.T;
+    dim3 grid((T - 1 + KT_W - 1) / KT_W, (T - 1 + KT_H - 1) / KT_H);
+    if (c.events) cudaEventRecord(c.kev[0], c.stream);
+    k_vd_tri<<<grid, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, (int2 *)c.colour, c.list2, T, c.logT,
+                                                    c.cap_tris, c.ctr);
+    count_launch();
+    if (c.events) cudaEventRecord(c.kev[1], c.stream);
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
+
 // ---------------------------------------------------------------- launchers
 int launch_column_pass(Ctx &c, int W2)
 {

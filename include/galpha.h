@@ -76,12 +76,17 @@ int galphaDestroy(galphaHandle h);
 /* Work on a caller stream (a cudaStream_t passed as void*; NULL: the handle's own). */
 int galphaSetStream(galphaHandle h, void *stream);
 
-/* Delaunay triangulation.  If out != NULL the triangles are copied to host
- * (out->triangles allocated with new[], capacity 2 * nVerts, as gpudtComputeDT);
- * the mesh also stays resident on the device for galphaComputeResident. */
+/* Delaunay triangulation.  If out != NULL the triangles are copied to host:
+ * into out->triangles when the caller sets it (capacity in out->nTris; pinned
+ * memory makes it one DMA copy), else into a new[] array of capacity
+ * 2 * nVerts as gpudtComputeDT allocates it.  The mesh also stays resident on
+ * the device for galphaComputeResident. */
 int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *out, gpudtStatus *st);
 
-/* Alpha spectrum + intervals of the handle's resident mesh. */
+/* Alpha spectrum + intervals of the handle's resident mesh.  Output arrays:
+ * caller buffers when all four pointers are set (capacities in the count
+ * fields; GPUDT_ERR_NOMEM if too small), else malloc'd arrays released by
+ * galphaReleaseOutput. */
 int galphaComputeResident(galphaHandle h, GAlphaOutput *out);
 
 /* Alpha spectrum + intervals of a host triangulation (Alpha_Shapes_2D(pInput, pDT)). */
