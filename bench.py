@@ -201,7 +201,7 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    stages, kernels = [], []
+    stages, kernels, stats = [], [], None
     launches0 = L.galphaLaunchCount()
     torch.cuda.synchronize()
     for k in range(a.steps):
@@ -213,6 +213,9 @@ def main():
             ev[k][1].record(stream)
         stages.append(list(st.ms))
         kernels.append(list(st.kernelMs))
+        stats = {k: getattr(st, k) for k in ("nVerts", "nFake", "nDuplicates", "nMissing", "nBadShift", "nIslandPixels",
+                                             "nFlips", "flipRounds", "shiftRounds", "missingRounds", "exactOrient",
+                                             "exactIncircle", "filteredIncircle")}
     torch.cuda.synchronize()
     launches = L.galphaLaunchCount() - launches0
     clk = clocks.stop()
@@ -236,14 +239,16 @@ def main():
     peak = peaks.get("hbm_gbs", 6650.0)
     T = fbo
     row_ms = sum(k[0] for k in kernels) / len(kernels)
-    row_bytes = 6.0 * T * T  # per launch: read the int16 column-candidate texture, write the int32 colour texture
+    # k_vd_tri per launch: read the int16 column-candidate texture once (2 B/pixel)
+    # and write the dual triangles (16 B each)
+    row_bytes = 2.0 * T * T + 16.0 * nt
     col_ms = sum(k[1] for k in kernels) / len(kernels)
     stage_mean = [sum(s[i] for s in stages) / len(stages) for i in range(12)]
     # whole-pipeline algorithmic byte model (SURVEY-style compulsory traffic)
     n_spec = ns
     b_alg = 28.0 * T * T + 16.0 * n + 36.0 * nt + 8.0 * n_spec + 24.0 * n_spec + 12.0 * ne + 4.0 * nt + 8.0 * n
     roof = {
-        "bound": "hbm", "kernel": "k_row_pass (per-row lower envelope + colouring)",
+        "bound": "hbm", "kernel": "k_vd_tri (fused colouring + island test + dual triangles)",
         "achieved": row_bytes / (row_ms / 1e3) / 1e9 if row_ms > 0 else None, "peak": peak, "unit": "GB/s",
         "frac": (row_bytes / (row_ms / 1e3) / 1e9) / peak if row_ms > 0 else None,
         "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650",
@@ -298,9 +303,10 @@ def main():
             "stages_ms": {nm: stage_mean[i] for i, nm in enumerate(
                 ["upload", "voronoi", "triangles", "shift", "missing", "boundary", "flip", "compact", "alpha",
                  "download", "total"]) if i < 11},
-            "kernels_ms": {"row_pass": row_ms, "column_pass": col_ms,
+            "kernels_ms": {"vd_tri": row_ms, "column_pass": col_ms,
                            "emit": sum(k[2] for k in kernels) / len(kernels)},
             "counts": {"triangles": nt, "edges": ne, "spectrum": ns},
+            "pipeline_stats": stats,
         }
         print(json.dumps(line), flush=True)
     eng.close()

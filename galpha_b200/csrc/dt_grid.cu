@@ -371,15 +371,22 @@ int stage_voronoi(Ctx &c)
         if (c.hctr->err) return c.hctr->err;
         int nflag = c.hctr->nisland;
         c.st.nIslandPixels = nflag;  // tiles with island pixels, repaired locally
+        bool local_ok = true;
         if (nflag > 0) {
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->escalate, 0, sizeof(int), c.stream));
             r0 = launch_vd_repair(c, nflag);
             if (r0) return r0;
             r0 = read_counters(c);
             if (r0) return r0;
             if (c.hctr->err) return c.hctr->err;
+            local_ok = c.hctr->escalate == 0;
         }
-        c.fused_done = true;
-        return GPUDT_OK;
+        if (local_ok) {
+            c.fused_done = true;
+            return GPUDT_OK;
+        }
+        // an island component too large for a local repair: global path
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, 2 * sizeof(int), c.stream));  // ntris, nfree
     }
     r0 = launch_row_pass(c);
     if (r0) return r0;

@@ -50,7 +50,7 @@ struct Counters {
     int act[2];     // flip: active-list lengths (ping-pong)
     int cand;       // flip: candidates this round
     int flips_total;
-    int pad[1];
+    int escalate;   // island repair could not stay local: redo the Voronoi stage globally
     unsigned long long exact_compares;
     unsigned long long exact_orient;
     unsigned long long exact_incircle;

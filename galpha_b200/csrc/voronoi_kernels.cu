@@ -506,7 +506,8 @@ constexpr int KS_W = KT_W + 1 + 2 * KS_M, KS_H = KT_H + 1 + 2 * KS_M;
 __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *__restrict__ ycol,
                                                                  const int *__restrict__ idmap,
                                                                  int4 *__restrict__ tv, const int *__restrict__ tiles,
-                                                                 int tiles_x, int T, int logT, int cap, Counters *ct)
+                                                                 const int *__restrict__ freelist, int tiles_x, int T,
+                                                                 int logT, int cap, Counters *ct)
 {
     __shared__ unsigned col[KS_H][KS_W];
     __shared__ unsigned nxt[KS_H][KS_W];
@@ -549,6 +550,42 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         }
         __syncthreads();
         if (!changed) break;
+    }
+    // components that reach the region border may extend past the redo set:
+    // flood the island pixels from the border zone; if one of the tile's own
+    // pixels is reached, the repair cannot stay local
+    {
+        for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+            int ly = k / KS_W, lx = k - ly * KS_W;
+            bool border = ly <= 1 || lx <= 1 || ly >= KS_H - 2 || lx >= KS_W - 2;
+            nxt[ly][lx] = (col[ly][lx] == ISL && border) ? 1u : 0u;
+        }
+        __syncthreads();
+        for (int round = 0; round < KS_W + KS_H; round++) {
+            if (threadIdx.x == 0) changed = 0;
+            __syncthreads();
+            for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
+                int ly = k / KS_W, lx = k - ly * KS_W;
+                if (col[ly][lx] != ISL || nxt[ly][lx]) continue;
+                bool hit = false;
+                for (int dy = -1; dy <= 1 && !hit; dy++)
+                    for (int dx = -1; dx <= 1 && !hit; dx++) {
+                        int yy = ly + dy, xx = lx + dx;
+                        if (yy >= 0 && xx >= 0 && yy < KS_H && xx < KS_W && nxt[yy][xx] == 1u) hit = true;
+                    }
+                if (hit) {
+                    nxt[ly][lx] = 1u;
+                    changed = 1;
+                }
+            }
+            __syncthreads();
+            if (!changed) break;
+        }
+        for (int k = threadIdx.x; k < (KT_H + 1) * (KT_W + 1); k += kFusedThreads) {
+            int ly = k / (KT_W + 1) + KS_M, lx = k % (KT_W + 1) + KS_M;
+            if (nxt[ly][lx] == 1u) ct->escalate = 1;
+        }
+        __syncthreads();
     }
     // recolour
     for (int round = 0; round < 4 * KS_M; round++) {
@@ -620,7 +657,9 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         }
     }
     for (int q = 0; q < n; q++) {
-        int s = atomicAdd(&ct->ntris, 1);
+        // reuse the slots released by the redo set first, then the tail
+        int k = atomicSub(&ct->nfree, 1) - 1;
+        int s = k >= 0 ? freelist[k] : atomicAdd(&ct->ntris, 1);
         if (s >= cap) {
             set_err(ct, GPUDT_ERR_NOMEM, 18);
             return;
@@ -659,6 +698,11 @@ __global__ void k_redo_collect(const unsigned char *redo, int ntiles, const int2
     }
 }
 
+__global__ void k_clamp_free(Counters *ct)
+{
+    if (ct->nfree < 0) ct->nfree = 0;
+}
+
 int launch_vd_repair(Ctx &c, int nflag)
 {
     const int T = c.T;
@@ -675,8 +719,10 @@ int launch_vd_repair(Ctx &c, int nflag)
     int r = read_counters(c);
     if (r) return r;
     int nredo = c.hctr->nlist;
-    k_vd_tri_repair<<<nredo, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, c.list, tiles_x, T, c.logT,
-                                                           c.cap_tris, c.ctr);
+    k_vd_tri_repair<<<nredo, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, c.list, c.freelist, tiles_x, T,
+                                                           c.logT, c.cap_tris, c.ctr);
+    count_launch();
+    k_clamp_free<<<1, 1, 0, c.stream>>>(c.ctr);
     count_launch();
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;

@@ -85,7 +85,8 @@ typedef struct {
     long long filteredIncircle; /* in-circle tests decided by the FP64 filter */
     float ms[12];            /* stage times (CUDA events), see galpha.h GALPHA_STAGE_* */
     float kernelMs[4];       /* single-kernel times (CUDA events on the launch stream):
-                                [0] row pass (envelope + colouring), [1] column pass,
+                                [0] colour + dual-triangle kernel (k_vd_tri; k_row_pass on
+                                the envelope path), [1] column pass,
                                 [2] triangle emission (count + write), [3] unused */
 } gpudtStatus;
 
