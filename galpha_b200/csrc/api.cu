@@ -191,6 +191,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     r = ensure(H, V, T, 0);
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
+    for (int k = 0; k < 8; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = false;
     ev_record(c, 1);
     int nonempty = has_triangles(c, d_xy, n);
@@ -248,14 +249,17 @@ static void fill_times(Ctx &c, int last)
     }
     float tot = 0.f;
     if (cudaEventElapsedTime(&tot, c.ev[0], c.ev[last]) == cudaSuccess) c.st.ms[GALPHA_STAGE_TOTAL] = tot;
-    if (c.have_mesh && c.nT_out > 0) {
-        float a = 0.f, b = 0.f;
-        if (cudaEventElapsedTime(&a, c.kev[0], c.kev[1]) == cudaSuccess) c.st.kernelMs[0] = a;
-        if (cudaEventElapsedTime(&a, c.kev[2], c.kev[3]) == cudaSuccess) c.st.kernelMs[1] = a;
-        if (cudaEventElapsedTime(&a, c.kev[4], c.kev[5]) == cudaSuccess &&
-            cudaEventElapsedTime(&b, c.kev[6], c.kev[7]) == cudaSuccess)
-            c.st.kernelMs[2] = a + b;
-    }
+    auto kms = [&](int k) -> float {
+        float v = 0.f;
+        if (c.kev_rec[2 * k] && c.kev_rec[2 * k + 1]) {
+            if (cudaEventElapsedTime(&v, c.kev[2 * k], c.kev[2 * k + 1]) != cudaSuccess) v = 0.f;
+        }
+        return v;
+    };
+    c.st.kernelMs[0] = kms(0);
+    c.st.kernelMs[1] = kms(1);
+    c.st.kernelMs[2] = kms(2) + kms(3);
+    cudaGetLastError();  // a timing query never leaves an error behind
 }
 
 static int upload_points(HandleState &H, const gpudtVertex *pts, int n)
@@ -386,6 +390,7 @@ int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, doub
     std::lock_guard<std::mutex> lk(h->mu);
     Ctx &c = h->H.c;
     cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
     ev_record(c, 0);
     int r = run_dt(h->H, d_xy, n, minX, minY, maxX, maxY, fboSize);
     if (!r && withAlpha) {
@@ -410,6 +415,7 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
     std::lock_guard<std::mutex> lk(h->mu);
     Ctx &c = h->H.c;
     cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
     ev_record(c, 0);
     r = upload_points(h->H, params->points, params->nPoints);
     if (!r)
@@ -545,6 +551,7 @@ int galphaComputeResident(galphaHandle h, GAlphaOutput *out)
     Ctx &c = h->H.c;
     if (!c.have_mesh) return GPUDT_ERR_ARG;
     cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
     int r = GPUDT_OK;
     if (!c.have_alpha) {
         r = stage_alpha(c);
@@ -574,6 +581,7 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
     std::lock_guard<std::mutex> lk(h->mu);
     Ctx &c = h->H.c;
     cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
     int n = params->nPoints;
     int r = ensure(h->H, n + 4, 256, (long long)dt->nTris);
     if (r) return r;

@@ -141,6 +141,7 @@ struct Ctx {
     // events for stage timing
     cudaEvent_t ev[GALPHA_STAGE_TOTAL + 2];
     cudaEvent_t kev[8];  // [2k, 2k+1] bracket single kernel k (see gpudtStatus.kernelMs)
+    bool kev_rec[8];     // recorded during the current call
     bool events = false;
     gpudtStatus st;
     bool have_mesh = false, have_alpha = false;

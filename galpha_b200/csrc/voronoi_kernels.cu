@@ -5,6 +5,13 @@
 
 namespace galpha {
 
+static inline void kev_record(Ctx &c, int k)
+{
+    if (!c.events) return;
+    cudaEventRecord(c.kev[k], c.stream);
+    c.kev_rec[k] = true;
+}
+
 // ------------------------------------------------------------ column pass
 // Thread (x, band): ycol[y][x] = row of the nearest occupied pixel of column x
 // (ties: the upper one, i.e. smaller y), -1 for an empty column.
@@ -732,11 +739,11 @@ int launch_vd_tri(Ctx &c)
 {
     const int T = c.T;
     dim3 grid((T - 1 + KT_W - 1) / KT_W, (T - 1 + KT_H - 1) / KT_H);
-    if (c.events) cudaEventRecord(c.kev[0], c.stream);
+    kev_record(c, 0);
     k_vd_tri<<<grid, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, (int2 *)c.colour, c.list2, T, c.logT,
                                                     c.cap_tris, c.ctr);
     count_launch();
-    if (c.events) cudaEventRecord(c.kev[1], c.stream);
+    kev_record(c, 1);
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
 }
@@ -746,9 +753,9 @@ int launch_column_pass(Ctx &c, int W2)
 {
     const int T = c.T;
     dim3 block(32, 8), grid(T / 32, ((T >> 6) + 7) / 8);
-    if (c.events) cudaEventRecord(c.kev[2], c.stream);
+    kev_record(c, 2);
     k_column_pass<<<grid, block, 0, c.stream>>>(c.occ, c.bandocc, c.ycol, T, W2);
-    if (c.events) cudaEventRecord(c.kev[3], c.stream);
+    kev_record(c, 3);
     count_launch();
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
@@ -763,9 +770,9 @@ int launch_row_pass(Ctx &c)
         GALPHA_CUDA(cudaFuncSetAttribute(k_row_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         configured = (int)sm;
     }
-    if (c.events) cudaEventRecord(c.kev[0], c.stream);
+    kev_record(c, 0);
     k_row_pass<<<T, kRowThreads, sm, c.stream>>>(c.ycol, c.idmap, c.colour, T, c.logT);
-    if (c.events) cudaEventRecord(c.kev[1], c.stream);
+    kev_record(c, 1);
     count_launch();
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
@@ -773,13 +780,13 @@ int launch_row_pass(Ctx &c)
 
 int launch_emit(Ctx &c, int ntiles, long long nwin, bool write)
 {
-    if (c.events) cudaEventRecord(c.kev[write ? 6 : 4], c.stream);
+    kev_record(c, write ? 6 : 4);
     if (!write)
         k_emit_count<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.T, c.logT, nwin, c.ctr);
     else
         k_emit_write<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.tv, c.T, c.logT, nwin);
     count_launch();
-    if (c.events) cudaEventRecord(c.kev[write ? 7 : 5], c.stream);
+    kev_record(c, write ? 7 : 5);
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
 }

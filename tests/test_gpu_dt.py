@@ -158,3 +158,27 @@ def test_large_uniform_properties(engine):
     n = len(np.unique(dt.vtx))
     assert n == len(pts)
     assert dt.nTris == 2 * n - 2 - chk["hull_edges"]
+
+
+def test_voronoi_paths(engine):
+    """Each discrete-Voronoi path: fused (dense), fused + local island repair,
+    escalation to the global island path (sparse Gaussian tails), and the
+    envelope path for sparse input (mean spacing above 16 pixels)."""
+    rng = np.random.default_rng(5)
+    _ = rng.random((20000, 2))
+    cases = [
+        (rng.random((60000, 2)), 1024),         # dense: island tiles repaired locally
+        (rng.normal(0, 1, (1970, 2)), 512),     # large islands in the tails
+        (rng.random((300, 2)), 2048),           # sparse: envelope path
+        (D.degenerate_mix(200000, 7), 2048),    # duplicates, lattice ties, clusters
+    ]
+    for pts, fbo in cases:
+        dt = run(engine, pts, fbo)
+        assert_parity(pts, dt, False)
+
+
+def test_c1_through_reference_symbol_matches_handle(engine):
+    pts, fbo = D.make("c1")
+    a = G.gpudt_compute_dt(G.GPUDTParams(pts, fboSize=fbo))
+    b = run(engine, pts, fbo)
+    assert canon_set(a.vtx) == canon_set(b.vtx)
