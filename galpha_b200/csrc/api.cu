@@ -26,6 +26,7 @@ int cuda_fail(cudaError_t e, const char *what)
 }
 
 const char *last_error_text() { return g_err.c_str(); }
+void set_last_error(const char *text) { g_err = text; }
 
 int read_counters(Ctx &c)
 {

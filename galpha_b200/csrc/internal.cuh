@@ -157,6 +157,7 @@ struct Ctx {
 
 int cuda_fail(cudaError_t e, const char *what);
 const char *last_error_text();
+void set_last_error(const char *text);
 
 // Reserve device buffers for V vertices, T texture, cap triangles.
 int reserve(Ctx &c, int V, int T, int cap_tris, bool alpha);

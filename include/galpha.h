@@ -106,6 +106,31 @@ int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap);
 
 void galphaReleaseOutput(GAlphaOutput *out);
 
+/* Edge numbering of a triangle-neighbour mesh that is already in device
+ * memory, for callers that cannot allocate: a serving or rendering loop that
+ * has reserved its device memory up front and cannot give any to a library
+ * mid-stream, or code that must not call cudaMalloc/cudaFree because those
+ * can synchronise the whole device while other streams have work in flight.
+ * This call allocates nothing (no device or pinned memory, no handle, no
+ * events); it runs one kernel on `stream` and returns without waiting.
+ *
+ * In:  d_tris[0..nTris), gpudtTriangle layout, device memory.
+ * Out: d_edges[2*k], d_edges[2*k+1] = (tIndex, vOpp) of edge k, in the order
+ *      and with the owner rule of GAlphaOutput.edge_list (an edge belongs to
+ *      the triangle in which its first vertex has the smaller index, or that
+ *      has no neighbour across it); at most edgeCapacity pairs are written.
+ *      *d_nEdges = the number of edges (may exceed edgeCapacity), or a
+ *      negative GPUDT_ERR_* code written by the kernel.
+ * Limit: nTris <= 67,108,864; larger meshes are rejected with GPUDT_ERR_ARG
+ * (the kernel's scratch is a fixed 256 KB device array inside the library).
+ * Every call on a device shares that array: calls on one device must be
+ * ordered (one stream, or synchronised); two calls in flight at once race.
+ * The first call on each device looks up and zeroes the array on `stream`.
+ * No counterpart in the reference: there the edge list is built inside
+ * Alpha_Shapes_2D (Alpha_Shapes_2D.cu:170-199) in thrust-allocated memory. */
+int galphaEdgeListNoAlloc(const gpudtTriangle *d_tris, int nTris, int *d_edges, int edgeCapacity,
+                          int *d_nEdges, void *stream);
+
 /* Text of the last error on the calling thread. */
 const char *galphaLastError(void);
 
