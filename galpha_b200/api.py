@@ -103,6 +103,27 @@ EDGE_INTERVAL_DTYPE = np.dtype([
 ])
 TRIANGLE_INTERVAL_DTYPE = np.dtype([("ro_rank", np.int32)])
 
+ALPHA_DTYPE = np.dtype([("simplex_index", np.int32), ("st", np.int32), ("at", np.int32)])
+
+
+class _MasterOut(ctypes.Structure):
+    _fields_ = [("nMaster", ctypes.c_int), ("master_list", ctypes.c_void_p), ("nSpecPointers", ctypes.c_int),
+                ("spec_pointers", ctypes.c_void_p)]
+
+
+# alpha-complex classes (galpha.h GALPHA_*)
+EXTERIOR, SINGULAR, REGULAR, INTERIOR = 0, 1, 2, 3
+
+
+class QueryResult(ctypes.Structure):
+    """galphaQueryResult: counts per class (indexed by EXTERIOR..INTERIOR)."""
+    _fields_ = [("alpha", ctypes.c_double), ("rank", ctypes.c_int), ("nPoints", ctypes.c_int * 4),
+                ("nEdges", ctypes.c_int * 4), ("nTris", ctypes.c_int * 4)]
+
+    def as_dict(self):
+        return {"alpha": self.alpha, "rank": self.rank, "nPoints": list(self.nPoints),
+                "nEdges": list(self.nEdges), "nTris": list(self.nTris)}
+
 _lib = None
 _lib_path = None
 
@@ -128,6 +149,11 @@ def load(path=None):
     L.galphaGetCounts.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.galphaCopyTriangles.argtypes = [vp, vp, ip]
     L.galphaReleaseOutput.argtypes = [ctypes.POINTER(_AlphaOut)]
+    L.galphaQuery.argtypes = [vp, ctypes.c_double, ctypes.POINTER(QueryResult)]
+    L.galphaQueryQuantile.argtypes = [vp, ctypes.c_double, ctypes.POINTER(QueryResult)]
+    L.galphaCopyClasses.argtypes = [vp, vp, vp, vp]
+    L.galphaMasterList.argtypes = [vp, ctypes.POINTER(_MasterOut)]
+    L.galphaReleaseMasterList.argtypes = [ctypes.POINTER(_MasterOut)]
     L.galphaLastError.restype = ctypes.c_char_p
     L.galphaVersion.restype = ctypes.c_char_p
     L.galphaLaunchCount.restype = ctypes.c_ulonglong
@@ -302,6 +328,7 @@ class Engine:
         o.triangles = tri.ctypes.data if len(tri) else None
         o.nTris = len(tri)
         out, bufs = self._alpha_bufs(params.nPoints, len(tri))
+        self._npoints = params.nPoints
         _check(self._L.galphaCompute(self._h, ctypes.byref(cp), ctypes.byref(o), ctypes.byref(out)),
                "galphaCompute")
         return self._alpha_result(out, bufs, copy)
@@ -314,6 +341,43 @@ class Engine:
                "galphaRunDevice")
         self._npoints = n
         return st
+
+    def query(self, alpha=None, quantile=None):
+        """Alpha-complex query on the resident result: classify every simplex at
+        ``alpha`` (a squared radius) or at the spectrum quantile ``quantile``."""
+        res = QueryResult()
+        if quantile is not None:
+            _check(self._L.galphaQueryQuantile(self._h, float(quantile), ctypes.byref(res)), "galphaQueryQuantile")
+        else:
+            _check(self._L.galphaQuery(self._h, float(alpha), ctypes.byref(res)), "galphaQuery")
+        return res
+
+    def master_list(self):
+        """master_list (ALPHA_DTYPE array) and spec_pointers of the resident alpha
+        result (Alpha_Shapes_2D::compute_master_list)."""
+        out = _MasterOut()
+        _check(self._L.galphaMasterList(self._h, ctypes.byref(out)), "galphaMasterList")
+        try:
+            ml = np.empty(out.nMaster, ALPHA_DTYPE)
+            sp = np.empty(out.nSpecPointers, np.int32)
+            if out.nMaster:
+                ctypes.memmove(ml.ctypes.data, out.master_list, ml.nbytes)
+            if out.nSpecPointers:
+                ctypes.memmove(sp.ctypes.data, out.spec_pointers, sp.nbytes)
+        finally:
+            self._L.galphaReleaseMasterList(ctypes.byref(out))
+        return ml, sp
+
+    def classes(self):
+        """Classes of the last query: (points, edges, triangles) uint8 arrays."""
+        nt, ne, _ = self.counts()
+        pt = np.empty(self._npoints, np.uint8)
+        ed = np.empty(ne, np.uint8)
+        tr = np.empty(nt, np.uint8)
+        _check(self._L.galphaCopyClasses(self._h, pt.ctypes.data if len(pt) else None,
+                                         ed.ctypes.data if len(ed) else None,
+                                         tr.ctypes.data if len(tr) else None), "galphaCopyClasses")
+        return pt, ed, tr
 
     def counts(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -344,7 +408,8 @@ class AlphaShapes2D:
 
     After compute_alpha_shapes(): ``spectrum`` (float64, [0] = 0 sentinel),
     ``point_list`` / ``edge_list`` / ``tri_list`` (structured arrays with the
-    reference's field names), ``alpha`` and ``alpha_index`` as in the reference.
+    reference's field names), ``master_list`` (ALPHA_DTYPE) and
+    ``spec_pointers``, ``alpha`` and ``alpha_index`` as in the reference.
     """
 
     def __init__(self, params, dt, engine=None):
@@ -355,6 +420,8 @@ class AlphaShapes2D:
         self.point_list = None
         self.edge_list = None
         self.tri_list = None
+        self.master_list = None
+        self.spec_pointers = None
         self.alpha = 0.0
         self.alpha_index = 0
 
@@ -366,6 +433,7 @@ class AlphaShapes2D:
         self.edge_list = r["edge_list"]
         self.tri_list = r["tri_list"]
         self.stats = {k: r[k] for k in ("exactCompares", "exactTies", "exactAttached")}
+        self.master_list, self.spec_pointers = eng.master_list()
         return self
 
     computeAlphaShapes = compute_alpha_shapes

@@ -481,4 +481,103 @@ int stage_alpha(Ctx &c)
     return GPUDT_OK;
 }
 
+// ------------------------------------------------------------ alpha query
+// Classification of every simplex of the alpha complex at a value alpha
+// (a squared radius, the unit of the spectrum), from the intervals above:
+// R = the largest rank with spectrum[R] <= alpha, then
+//   triangle:  ro <= R                                    -> interior
+//   edge:      nu_max != 0 (finite) && nu_max <= R        -> interior
+//              nu_min <= R                                -> regular
+//              ro != 0 (unattached) && ro <= R            -> singular
+//   point:     (nu_min, nu_max) the same way, with the singular interval
+//              starting at rank 0 (every vertex is in the complex at alpha >= 0)
+//   otherwise exterior.  Points dropped as duplicates (no incident edge) are
+// exterior.  These are the interval semantics of kernel.cu:427-624 that the
+// reference's viewer draws from (Visualizer.cu:296-337: an edge is drawn from
+// its ro / nu_min entry until its nu_max entry, a triangle from its ro entry).
+namespace {
+
+struct QueryRank {
+    const double *spectrum;
+    int nSpec;
+    double alpha, q;
+    int by_quantile;
+    Counters *ct;
+    __device__ void operator()(long long) const
+    {
+        double a = alpha;
+        if (by_quantile) {
+            double qq = q < 0.0 ? 0.0 : (q > 1.0 ? 1.0 : q);
+            int k = (int)llrint(qq * (double)(nSpec - 1));
+            a = spectrum[k];
+        }
+        int R = -1;
+        if (a >= 0.0) {
+            int lo = 0, hi = nSpec - 1;  // spectrum[0] = 0 <= a
+            while (lo < hi) {
+                int mid = lo + (hi - lo + 1) / 2;
+                if (spectrum[mid] <= a) lo = mid;
+                else hi = mid - 1;
+            }
+            R = lo;
+        }
+        ct->qrank = R;
+        ct->qalpha = a;
+        for (int k = 0; k < 12; k++) ct->qcount[k] = 0;
+    }
+};
+
+__device__ __forceinline__ int interval_class(int ro, int nu_min, int nu_max, int R)
+{
+    if (nu_max > 0 && nu_max <= R) return 3;
+    if (nu_min <= R) return 2;
+    if (ro >= 0 && ro <= R) return 1;
+    return 0;
+}
+
+struct QueryClassify {
+    const int2 *pt;
+    const int *edge_ro;
+    const int2 *edge_nu;
+    const int *tri_ro;
+    uint8_t *cls;
+    int N, nE, nT;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        int i = (int)ii;
+        const int R = ct->qrank;
+        int type, k;
+        if (i < N) {
+            type = 0;
+            int2 v = pt[i];
+            k = (v.x < 0 || R < 0) ? 0 : interval_class(0, v.x, v.y, R);
+        } else if (i < N + nE) {
+            type = 1;
+            int e = i - N;
+            int ro = edge_ro[e];
+            int2 nu = edge_nu[e];
+            k = R < 0 ? 0 : interval_class(ro != 0 ? ro : -1, nu.x, nu.y, R);
+        } else {
+            type = 2;
+            k = (R >= 0 && tri_ro[i - N - nE] <= R) ? 3 : 0;
+        }
+        cls[i] = (uint8_t)k;
+        int bin = type * 4 + k;
+        unsigned peers = __match_any_sync(__activemask(), bin);
+        if ((peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(&ct->qcount[bin], __popc(peers));
+    }
+};
+
+}  // namespace
+
+int alpha_query(Ctx &c, double alpha, double q, bool by_quantile)
+{
+    launch_n(c, QueryRank{c.spectrum, c.nSpec, alpha, q, by_quantile ? 1 : 0, c.ctr}, 1);
+    long long n = (long long)c.N + c.nE + c.nT_out;
+    launch_n(c, QueryClassify{c.pt_nu, c.edge_ro, c.edge_nu, c.tri_ro, c.qclass, c.N, c.nE, c.nT_out, c.ctr}, n);
+    GALPHA_CUDA(cudaGetLastError());
+    return read_counters(c);
+}
+
 }  // namespace galpha

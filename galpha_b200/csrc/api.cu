@@ -113,6 +113,7 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(spectrum, double, 3 * cap);
     TAKE(outtri, gpudtTriangle, cap);
     TAKE(edge_aos, galphaEdgeInterval, 2 * cap);
+    TAKE(qclass, uint8_t, V + 3 * cap);
     TAKE(ctr, Counters, 1);
 #undef TAKE
     return total + 4096;
@@ -193,7 +194,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
     for (int k = 0; k < 8; k++) c.kev_rec[k] = false;
-    c.have_mesh = c.have_alpha = false;
+    c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
     int nonempty = has_triangles(c, d_xy, n);
     if (nonempty < 0) return stage_fail(c, nonempty, "precheck");
@@ -363,6 +364,7 @@ int galphaDestroy(galphaHandle h)
     if (c.stream) cudaStreamSynchronize(c.stream);
     if (h->H.arena.base) cudaFree(h->H.arena.base);
     if (h->H.d_xy) cudaFree(h->H.d_xy);
+    if (c.ml_buf) cudaFree(c.ml_buf);
     if (c.hctr) cudaFreeHost(c.hctr);
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2 && c.events; k++) cudaEventDestroy(c.ev[k]);
     for (int k = 0; k < 8 && c.events; k++) cudaEventDestroy(c.kev[k]);
@@ -399,7 +401,17 @@ int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, doub
         r = stage_alpha(c);
         if (!r) c.have_alpha = true;
         ev_record(c, 9);
+        if (!r && withAlpha >= 2) {
+            r = master_list(c);
+            ev_record(c, 10);
+        }
         if (!r) fill_times(c, 9);
+        if (!r && withAlpha >= 2 && c.events) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, c.ev[9], c.ev[10]) == cudaSuccess) c.st.ms[GALPHA_STAGE_MASTER] = ms;
+            if (cudaEventElapsedTime(&ms, c.ev[0], c.ev[10]) == cudaSuccess) c.st.ms[GALPHA_STAGE_TOTAL] = ms;
+            cudaGetLastError();
+        }
     } else if (!r) {
         fill_times(c, 8);
     }
@@ -463,6 +475,57 @@ int galphaGetCounts(galphaHandle h, int *nTris, int *nEdges, int *nSpectrum)
     if (nTris) *nTris = c.have_mesh ? c.nT_out : 0;
     if (nEdges) *nEdges = c.have_alpha ? c.nE : 0;
     if (nSpectrum) *nSpectrum = c.have_alpha ? c.nSpec : 0;
+    return GPUDT_OK;
+}
+
+static int run_query(galphaHandle h, double alpha, double q, bool by_quantile, galphaQueryResult *res)
+{
+    if (!h || !res) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    if (!c.have_alpha) {
+        g_err = "galphaQuery: no alpha result on this handle";
+        return GPUDT_ERR_ARG;
+    }
+    cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
+    int r = alpha_query(c, alpha, q, by_quantile);
+    if (r) return r;
+    if (c.hctr->err) return c.hctr->err;
+    res->alpha = c.hctr->qalpha;
+    res->rank = c.hctr->qrank;
+    for (int k = 0; k < 4; k++) {
+        res->nPoints[k] = c.hctr->qcount[k];
+        res->nEdges[k] = c.hctr->qcount[4 + k];
+        res->nTris[k] = c.hctr->qcount[8 + k];
+    }
+    return GPUDT_OK;
+}
+
+int galphaQuery(galphaHandle h, double alpha, galphaQueryResult *res)
+{
+    return run_query(h, alpha, 0.0, false, res);
+}
+
+int galphaQueryQuantile(galphaHandle h, double q, galphaQueryResult *res)
+{
+    return run_query(h, 0.0, q, true, res);
+}
+
+int galphaCopyClasses(galphaHandle h, unsigned char *pointClass, unsigned char *edgeClass, unsigned char *triClass)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    if (!c.have_alpha) return GPUDT_ERR_ARG;
+    cudaStream_t s = c.stream;
+    if (pointClass && c.N > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(pointClass, c.qclass, (size_t)c.N, cudaMemcpyDeviceToHost, s));
+    if (edgeClass && c.nE > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(edgeClass, c.qclass + c.N, (size_t)c.nE, cudaMemcpyDeviceToHost, s));
+    if (triClass && c.nT_out > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(triClass, c.qclass + c.N + c.nE, (size_t)c.nT_out, cudaMemcpyDeviceToHost, s));
+    GALPHA_CUDA(cudaStreamSynchronize(s));
     return GPUDT_OK;
 }
 
@@ -596,11 +659,68 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
     launch_n(c, AosToSoa{c.outtri, c.cv, c.cn}, dt->nTris);
     c.nT_out = dt->nTris;
     c.have_mesh = true;
-    c.have_alpha = false;
+    c.have_alpha = c.have_master = false;
     r = stage_alpha(c);
     if (r) return r;
     c.have_alpha = true;
     return download_alpha(c, out);
+}
+
+static const int kMinusOneHost = -1;
+
+int galphaMasterList(galphaHandle h, GAlphaMasterList *out)
+{
+    if (!h || !out) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    if (!c.have_alpha) {
+        g_err = "galphaMasterList: no alpha result on this handle";
+        return GPUDT_ERR_ARG;
+    }
+    cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
+    if (!c.have_master) {
+        int r = master_list(c);
+        if (r) return r;
+    }
+    bool caller = out->master_list && out->spec_pointers;
+    if (caller) {
+        if (out->nMaster < c.nMaster || out->nSpecPointers < c.nSpecPtr) {
+            g_err = "galphaMasterList: output buffers too small";
+            return GPUDT_ERR_ARG;
+        }
+    } else {
+        out->master_list = (galphaAlpha *)malloc(sizeof(galphaAlpha) * (size_t)(c.nMaster > 0 ? c.nMaster : 1));
+        out->spec_pointers = (int *)malloc(sizeof(int) * (size_t)(c.nSpecPtr > 0 ? c.nSpecPtr : 1));
+        if (!out->master_list || !out->spec_pointers) {
+            free(out->master_list);
+            free(out->spec_pointers);
+            out->master_list = nullptr;
+            out->spec_pointers = nullptr;
+            return GPUDT_ERR_NOMEM;
+        }
+    }
+    if (c.nMaster > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(out->master_list, c.ml_out, sizeof(galphaAlpha) * (size_t)c.nMaster,
+                                    cudaMemcpyDeviceToHost, c.stream));
+    if (c.nMaster > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(out->spec_pointers, c.ml_sp, sizeof(int) * (size_t)c.nSpecPtr,
+                                    cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    if (c.nMaster == 0) out->spec_pointers[0] = kMinusOneHost;
+    out->nMaster = c.nMaster;
+    out->nSpecPointers = c.nSpecPtr;
+    return GPUDT_OK;
+}
+
+void galphaReleaseMasterList(GAlphaMasterList *out)
+{
+    if (!out) return;
+    free(out->master_list);
+    free(out->spec_pointers);
+    out->master_list = nullptr;
+    out->spec_pointers = nullptr;
+    out->nMaster = out->nSpecPointers = 0;
 }
 
 void galphaReleaseOutput(GAlphaOutput *out)

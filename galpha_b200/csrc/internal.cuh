@@ -56,6 +56,10 @@ struct Counters {
     unsigned long long exact_incircle;
     unsigned long long filt_incircle;
     unsigned long long exact_attached;
+    int qcount[12];  // alpha query: [type*4 + class], type 0 points, 1 edges, 2 triangles
+    int qrank;       // alpha query: largest spectrum rank <= alpha (-1 if alpha < 0)
+    int qpad;
+    double qalpha;   // alpha query: the alpha value classified
 };
 
 // Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
@@ -130,6 +134,14 @@ struct Ctx {
     int *vals = nullptr, *vals2 = nullptr;                 // [nSpecIn]
     int *rank = nullptr;       // [nSpecIn]
     double *spectrum = nullptr;  // [nSpecIn + 1]
+    uint8_t *qclass = nullptr;   // alpha query classes: points [V], edges [2 cap], triangles [cap]
+    // master list (own allocation, made on first use)
+    char *ml_buf = nullptr;
+    size_t ml_bytes = 0;
+    galphaAlpha *ml_out = nullptr;  // [nMaster]
+    int *ml_sp = nullptr;           // [nSpecPtr]
+    int nMaster = 0, nSpecPtr = 0;
+    bool have_master = false;
     int *hist = nullptr;       // scan scratch
     int *rhist = nullptr;      // radix sort histograms
     gpudtTriangle *outtri = nullptr;  // [cap] AoS output staging
@@ -260,6 +272,8 @@ int stage_boundary(Ctx &c);
 int stage_flip(Ctx &c);
 int stage_compact(Ctx &c);
 int stage_alpha(Ctx &c);
+int alpha_query(Ctx &c, double alpha, double q, bool by_quantile);
+int master_list(Ctx &c);
 int alpha_from_host_mesh(Ctx &c, const double *h_xy, int n, const gpudtTriangle *tris, int nt);
 
 // Block-level kernels of the Voronoi stage (voronoi_kernels.cu)
@@ -272,6 +286,8 @@ int launch_vd_tri(Ctx &c);
 int launch_vd_repair(Ctx &c, int nflag);
 // LSD radix sort of (keys, vals) ascending (sort.cu)
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n);
+int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);
+long long radix_scratch_ints(long long n);
 
 // Prefix sums (scan.cu)
 int exclusive_scan_int(Ctx &c, const int *in, int *out, int n, int *total_dev);

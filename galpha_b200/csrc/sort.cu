@@ -1,24 +1,27 @@
-// sort.cu -- LSD radix sort of 64-bit keys with an int payload.
+// sort.cu -- stable LSD radix sort of 64- or 32-bit keys with an int payload.
 //
-// Replaces thrust::sort_by_key on the FP64 spectrum (Alpha_Shapes_2D.cu:317):
-// the keys are the IEEE bit patterns of positive doubles, so their unsigned
-// order is the numeric order.  8-bit digits; digits on which all keys agree are
-// skipped (an OR of key XOR first-key finds them).  Each pass: a per-block
-// shared-memory histogram, a scan of the digit-major histogram table, and a
-// stable scatter in which every warp ranks its 32 keys per round with
-// __match_any_sync.
+// Replaces thrust::sort_by_key on the FP64 spectrum (Alpha_Shapes_2D.cu:317,
+// keys = the IEEE bit patterns of positive doubles, whose unsigned order is
+// the numeric order) and on the master-list ranks (Alpha_Shapes_2D.cu:658).
+// 8-bit digits; digits on which all keys agree are skipped (an OR of
+// key XOR first-key finds them).  Each pass: a per-block shared-memory
+// histogram, a scan of the digit-major histogram table, and a scatter that
+// first sorts the block's 4096-key tile by digit in shared memory (warp ranks
+// from __match_any_sync, stable) and then writes each digit's run to its
+// global offset, so consecutive threads store consecutive addresses.
 #include <algorithm>
 #include "internal.cuh"
 
 namespace galpha {
 
-// ------------------------------------------------------------- radix sort
 constexpr int kRsThreads = 256;
 constexpr int kRsItems = 16;
 constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys per block
+constexpr int kRsWarps = kRsThreads / 32;
 
-__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const unsigned long long *__restrict__ keys, int n,
-                                                        int shift, int *__restrict__ hist, int nblocks)
+template <typename K>
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const K *__restrict__ keys, int n, int shift,
+                                                        int *__restrict__ hist, int nblocks)
 {
     __shared__ int h[256];
     h[threadIdx.x] = 0;
@@ -26,129 +29,184 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const unsigned long long
     long long base = (long long)blockIdx.x * kRsTile;
     for (int k = threadIdx.x; k < kRsTile; k += kRsThreads) {
         long long i = base + k;
-        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255], 1);
+        if (i < n) atomicAdd(&h[(int)((keys[i] >> shift) & 255)], 1);
     }
     __syncthreads();
     hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter: warp w owns tile elements [w*512, (w+1)*512) in 16 rounds of
-// 32; ranks within a round come from __match_any_sync on the digit.
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long long *__restrict__ kin,
-                                                           const int *__restrict__ vin,
-                                                           unsigned long long *__restrict__ kout,
-                                                           int *__restrict__ vout, int n, int shift,
-                                                           const int *__restrict__ hoff, int nblocks)
+template <typename K>
+struct RsSmem {
+    K key[kRsTile];
+    int val[kRsTile];
+    int wcnt[kRsWarps][256];  // per-warp digit counts, then tile-local offsets
+    int lstart[256];          // tile-local start of each digit's run
+    int gbase[256];           // global start of this tile's run of each digit
+};
+
+// Stable scatter of one tile: warp w owns tile elements [w*512, (w+1)*512) in
+// 16 rounds of 32; an element's tile-local rank is (digit run start) + (keys
+// of the same digit in earlier warps) + (earlier rounds of its warp) + (lower
+// lanes of its round).
+template <typename K>
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K *__restrict__ kin, const int *__restrict__ vin,
+                                                           K *__restrict__ kout, int *__restrict__ vout, int n,
+                                                           int shift, const int *__restrict__ hoff, int nblocks)
 {
-    __shared__ int wcnt[kRsThreads / 32][256];
-    __shared__ int boff[256];
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    RsSmem<K> &S = *reinterpret_cast<RsSmem<K> *>(rs_smem);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int d = lane; d < 256; d += 32) wcnt[w][d] = 0;
-    boff[threadIdx.x] = hoff[threadIdx.x * nblocks + blockIdx.x];
+    for (int d = lane; d < 256; d += 32) S.wcnt[w][d] = 0;
+    S.gbase[threadIdx.x] = hoff[threadIdx.x * nblocks + blockIdx.x];
     __syncwarp();
-    long long base = (long long)blockIdx.x * kRsTile + (long long)w * (kRsItems * 32);
-    unsigned long long key[kRsItems];
-    int dig[kRsItems];
-    unsigned lanemask_lt = (1u << lane) - 1u;
-    // sweep 1: per-warp digit counts
+    const long long tile0 = (long long)blockIdx.x * kRsTile;
+    const long long base = tile0 + (long long)w * (kRsItems * 32);
+    K key[kRsItems];
+    int val[kRsItems];
+    int rk[kRsItems];  // rank within the warp's keys of the same digit
+    const unsigned lanemask_lt = (1u << lane) - 1u;
 #pragma unroll
     for (int r = 0; r < kRsItems; r++) {
         long long i = base + r * 32 + lane;
         bool ok = i < n;
-        key[r] = ok ? kin[i] : 0ull;
-        dig[r] = ok ? (int)((key[r] >> shift) & 255) : 256 + lane;  // unique dummy digits
-        unsigned peers = __match_any_sync(0xffffffffu, dig[r]);
-        if (ok && (peers & lanemask_lt) == 0) wcnt[w][dig[r]] += __popc(peers);
+        key[r] = ok ? kin[i] : (K)0;
+        val[r] = ok ? vin[i] : 0;
+        const int dg = ok ? (int)((key[r] >> shift) & 255) : 256 + lane;  // unique dummy digits
+        unsigned peers = __match_any_sync(0xffffffffu, dg);
+        int before = ok ? S.wcnt[w][dg] : 0;
+        rk[r] = before + __popc(peers & lanemask_lt);
+        __syncwarp();
+        if (ok && (peers & lanemask_lt) == 0) S.wcnt[w][dg] = before + __popc(peers);
         __syncwarp();
     }
     __syncthreads();
-    // per digit: exclusive scan over warps
+    // per digit: totals over warps, then the digit-major exclusive scan
     {
-        int d = threadIdx.x;
+        const int d = threadIdx.x;
         int s = 0;
-        for (int q = 0; q < kRsThreads / 32; q++) {
-            int c = wcnt[q][d];
-            wcnt[q][d] = s;
+        for (int q = 0; q < kRsWarps; q++) {
+            int c = S.wcnt[q][d];
+            S.wcnt[q][d] = s;
             s += c;
         }
+        S.lstart[d] = s;  // digit total for now
     }
     __syncthreads();
-    // sweep 2: scatter
+    if (w == 0) {
+        int carry = 0;
+        for (int d0 = 0; d0 < 256; d0 += 32) {
+            int v = S.lstart[d0 + lane];
+            int incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            S.lstart[d0 + lane] = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+    __syncthreads();
 #pragma unroll
     for (int r = 0; r < kRsItems; r++) {
         long long i = base + r * 32 + lane;
-        bool ok = i < n;
-        unsigned peers = __match_any_sync(0xffffffffu, dig[r]);
-        int rank = __popc(peers & lanemask_lt);
-        int d = ok ? dig[r] : 0;
-        int pos = 0;
-        if (ok) pos = boff[d] + wcnt[w][d] + rank;
-        __syncwarp();
-        if (ok && (peers & lanemask_lt) == 0) wcnt[w][d] += __popc(peers);
-        __syncwarp();
-        if (ok) {
-            kout[pos] = key[r];
-            vout[pos] = vin[i];
+        if (i < n) {
+            const int dg = (int)((key[r] >> shift) & 255);
+            int p = S.lstart[dg] + S.wcnt[w][dg] + rk[r];
+            S.key[p] = key[r];
+            S.val[p] = val[r];
         }
+    }
+    __syncthreads();
+    const int cnt = (int)min((long long)kRsTile, (long long)n - tile0);
+    for (int p = threadIdx.x; p < cnt; p += kRsThreads) {
+        K k = S.key[p];
+        int d = (int)((k >> shift) & 255);
+        long long g = (long long)S.gbase[d] + (p - S.lstart[d]);
+        kout[g] = k;
+        vout[g] = S.val[p];
     }
 }
 
 // OR over all keys of (key XOR first key): the bits on which keys differ.
-// Reduced per warp and per block; one 64-bit atomic per block.
-__global__ void __launch_bounds__(256) k_or_xor(const unsigned long long *__restrict__ keys, long long n,
-                                                unsigned long long *acc)
+// Reduced per warp and per block; one atomic per block.
+template <typename K>
+__global__ void __launch_bounds__(256) k_or_xor(const K *__restrict__ keys, long long n, K *acc)
 {
-    __shared__ unsigned long long ws[8];
-    unsigned long long k0 = acc[0], x = 0;
+    __shared__ K ws[8];
+    K k0 = acc[0], x = 0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         x |= keys[i] ^ k0;
     for (int o = 16; o > 0; o >>= 1) x |= __shfl_xor_sync(0xffffffffu, x, o);
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = x;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < 8; w++) x |= ws[w];
+        for (int q = 1; q < 8; q++) x |= ws[q];
         if (x) atomicOr(&acc[1], x);
     }
 }
 
-// Sorts (keys, vals)[0..n) ascending; result in keys/vals.  Uses keys2/vals2.
-int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
+// Scratch ints needed by radix_sort_keys for n keys.
+long long radix_scratch_ints(long long n)
+{
+    return 8 + 256 * ((n + kRsTile - 1) / kRsTile + 1);
+}
+
+// Sorts (keys, vals)[0..n) ascending (stable); result in keys/vals.  Uses
+// keys2/vals2 and `scratch` (radix_scratch_ints(n) ints).
+template <typename K>
+static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int n, int *scratch)
 {
     if (n <= 1) return GPUDT_OK;
-    unsigned long long *acc = (unsigned long long *)c.rhist;
-    GALPHA_CUDA(cudaMemcpyAsync(acc, keys, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, c.stream));
-    GALPHA_CUDA(cudaMemsetAsync(acc + 1, 0, sizeof(unsigned long long), c.stream));
+    static_assert(sizeof(K) == 4 || sizeof(K) == 8, "32- or 64-bit keys");
+    const int smem = (int)sizeof(RsSmem<K>);
+    static bool attr_set[64];  // per key type and device: the opt-in above 48 KB, once
+    if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
+        GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+    }
+    K *acc = reinterpret_cast<K *>(scratch);
+    GALPHA_CUDA(cudaMemcpyAsync(acc, keys, sizeof(K), cudaMemcpyDeviceToDevice, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(acc + 1, 0, sizeof(K), c.stream));
     {
         long long blocks = std::min<long long>((n + 255) / 256, (long long)c.sm_count * 4);
-        k_or_xor<<<(unsigned)blocks, 256, 0, c.stream>>>(keys, n, acc);
+        k_or_xor<K><<<(unsigned)blocks, 256, 0, c.stream>>>(keys, n, acc);
         count_launch();
     }
-    unsigned long long hv[2];
+    K hv[2];
     GALPHA_CUDA(cudaMemcpyAsync(hv, acc, sizeof(hv), cudaMemcpyDeviceToHost, c.stream));
     GALPHA_CUDA(cudaStreamSynchronize(c.stream));
-    unsigned long long varying = hv[1];
-    int nblocks = (n + kRsTile - 1) / kRsTile;
-    int *hist = c.rhist + 8;
-    unsigned long long *ki = keys, *ko = keys2;
+    const unsigned long long varying = (unsigned long long)hv[1];
+    const int nblocks = (n + kRsTile - 1) / kRsTile;
+    int *hist = scratch + 8;
+    K *ki = keys, *ko = keys2;
     int *vi = vals, *vo = vals2;
-    for (int shift = 0; shift < 64; shift += 8) {
+    for (int shift = 0; shift < (int)(8 * sizeof(K)); shift += 8) {
         if (((varying >> shift) & 255ull) == 0) continue;
-        k_rs_hist<<<nblocks, kRsThreads, 0, c.stream>>>(ki, n, shift, hist, nblocks);
+        k_rs_hist<K><<<nblocks, kRsThreads, 0, c.stream>>>(ki, n, shift, hist, nblocks);
         count_launch();
         int r = exclusive_scan_int(c, hist, hist, 256 * nblocks, nullptr);
         if (r) return r;
-        k_rs_scatter<<<nblocks, kRsThreads, 0, c.stream>>>(ki, vi, ko, vo, n, shift, hist, nblocks);
+        k_rs_scatter<K><<<nblocks, kRsThreads, smem, c.stream>>>(ki, vi, ko, vo, n, shift, hist, nblocks);
         count_launch();
         GALPHA_CUDA(cudaGetLastError());
         std::swap(ki, ko);
         std::swap(vi, vo);
     }
     if (ki != keys) {
-        GALPHA_CUDA(cudaMemcpyAsync(keys, ki, sizeof(unsigned long long) * (size_t)n, cudaMemcpyDeviceToDevice,
-                                    c.stream));
+        GALPHA_CUDA(cudaMemcpyAsync(keys, ki, sizeof(K) * (size_t)n, cudaMemcpyDeviceToDevice, c.stream));
         GALPHA_CUDA(cudaMemcpyAsync(vals, vi, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, c.stream));
     }
     return GPUDT_OK;
+}
+
+int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
+{
+    return radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist);
+}
+
+int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch)
+{
+    return radix_sort_keys<unsigned int>(c, keys, vals, keys2, vals2, n, scratch);
 }
 
 }  // namespace galpha

@@ -68,6 +68,7 @@ typedef struct galpha_ctx *galphaHandle;
 #define GALPHA_STAGE_ALPHA     8  /* birth times + attached + sort + ranks + intervals */
 #define GALPHA_STAGE_DOWNLOAD  9
 #define GALPHA_STAGE_TOTAL     10
+#define GALPHA_STAGE_MASTER    11  /* master list (galphaRunDevice with withAlpha = 2) */
 
 /* Create a handle on CUDA device `device` (-1: current device).  Device memory
  * is reserved lazily and grown on demand; budgetBytes (0: no limit) caps it. */
@@ -93,7 +94,8 @@ int galphaComputeResident(galphaHandle h, GAlphaOutput *out);
 int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *dt, GAlphaOutput *out);
 
 /* Device-resident hot path: points already in device memory (d_xy: 2*n doubles).
- * Runs DT (+ alpha when withAlpha) and leaves every result on the device.
+ * Runs DT (+ alpha when withAlpha; + the master list when withAlpha = 2) and
+ * leaves every result on the device.
  * Returns the status; counts through galphaGetCounts. */
 int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY,
                     double maxX, double maxY, int fboSize, int withAlpha, gpudtStatus *st);
@@ -105,6 +107,69 @@ int galphaGetCounts(galphaHandle h, int *nTris, int *nEdges, int *nSpectrum);
 int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap);
 
 void galphaReleaseOutput(GAlphaOutput *out);
+
+/* Alpha (headers.h:80-86): one master-list entry.  st: 0 edge, 1 triangle,
+ * 2 vertex (simplex_type); at: 0 ro, 1 nu_min, 2 nu_max (alpha_type). */
+typedef struct {
+    int simplex_index;
+    int st;
+    int at;
+} galphaAlpha;
+
+/* master_list and spec_pointers of Alpha_Shapes_2D (compute_master_list,
+ * Alpha_Shapes_2D.cu:641-727): every interval end point (2 per vertex, 3 per
+ * edge, 1 per triangle) sorted stably by rank, rank-0 entries removed;
+ * spec_pointers = -1 followed by the first master-list index of each distinct
+ * rank.  When both pointers are set they are caller buffers (capacities in
+ * nMaster / nSpecPointers on input), else the arrays are malloc'd and freed by
+ * galphaReleaseMasterList. */
+typedef struct {
+    int nMaster;
+    galphaAlpha *master_list;
+    int nSpecPointers;
+    int *spec_pointers;
+} GAlphaMasterList;
+
+/* Master list of the resident alpha result (after galphaCompute,
+ * galphaComputeResident or galphaRunDevice with alpha). */
+int galphaMasterList(galphaHandle h, GAlphaMasterList *out);
+void galphaReleaseMasterList(GAlphaMasterList *out);
+
+/* Alpha-complex query on the resident result (after galphaCompute,
+ * galphaComputeResident or galphaRunDevice with alpha).  alpha is a squared
+ * radius (the unit of the spectrum).  With R the largest rank whose spectrum
+ * value is <= alpha, every simplex is classified from its interval
+ * (headers.h:48-64 ranks; interval meaning as kernel.cu:427-624):
+ *   GALPHA_INTERIOR  nu_max finite (!= 0) and <= R   (triangles: ro <= R)
+ *   GALPHA_REGULAR   nu_min <= R
+ *   GALPHA_SINGULAR  unattached edge with ro <= R; a vertex below nu_min
+ *   GALPHA_EXTERIOR  otherwise, every simplex when alpha < 0, and input
+ *                    points dropped as duplicates.
+ * The classes stay on the device (galphaCopyClasses) and the per-class counts
+ * are returned.  The reference exposes this only through its viewer
+ * (Visualizer.cu:296-337). */
+#define GALPHA_EXTERIOR 0
+#define GALPHA_SINGULAR 1
+#define GALPHA_REGULAR 2
+#define GALPHA_INTERIOR 3
+
+typedef struct {
+    double alpha;    /* the value classified (for a quantile query, the spectrum value chosen) */
+    int rank;        /* largest rank with spectrum[rank] <= alpha; -1 when alpha < 0 */
+    int nPoints[4];  /* counts per class, indexed by GALPHA_* */
+    int nEdges[4];
+    int nTris[4];
+} galphaQueryResult;
+
+int galphaQuery(galphaHandle h, double alpha, galphaQueryResult *res);
+
+/* The same at alpha = spectrum[round(q * (nSpectrum - 1))], q in [0, 1]. */
+int galphaQueryQuantile(galphaHandle h, double q, galphaQueryResult *res);
+
+/* Copy the classes of the last query (one byte per point / edge / triangle,
+ * in point, edge_list and tri_list order); any pointer may be NULL. */
+int galphaCopyClasses(galphaHandle h, unsigned char *pointClass, unsigned char *edgeClass,
+                      unsigned char *triClass);
 
 /* Edge numbering of a triangle-neighbour mesh that is already in device
  * memory, for callers that cannot allocate: a serving or rendering loop that

@@ -9,6 +9,8 @@ reference arm may import this module, and only as the checker.  It wraps
 * ``alpha(points, v, n)``   alpha spectrum + intervals (oracle/alpha.c), the
                             output of Alpha_Shapes_2D::computeAlphaShapes
                             (gpudt/AlphaShape/Alpha_Shapes_2D.cu:206-727)
+* ``master_list(...)``      master list + spec pointers (numpy restatement of
+                            compute_master_list, Alpha_Shapes_2D.cu:641-727)
 * exact predicates for cross-checks.
 """
 import ctypes
@@ -127,6 +129,34 @@ def alpha(points, vtx, nbr):
         "exact_compares": out.exact_compares,
         "exact_ties": out.exact_ties,
     }
+
+
+def master_list(point_nu, edge_ro, edge_nu_min, edge_nu_max, tri_ro):
+    """Master list of Alpha_Shapes_2D::compute_master_list (Alpha_Shapes_2D.cu:
+    641-727) from the intervals.  Entry k of the unsorted list follows the kernel
+    computeMasterList (kernel.cu:626-690): 2 per vertex (nu_min, nu_max), 3 per
+    edge (ro, nu_min, nu_max), 1 per triangle (ro); each is keyed by its rank.
+    thrust::sort_by_key on int keys is a stable radix sort, remove_if drops rank
+    0 keeping order, unique_by_key over a sequence keeps the first index of each
+    rank run, and -1 is prepended.  Returns (simplex_index, st, at, spec_pointers)
+    with st 0 edge / 1 triangle / 2 vertex and at 0 ro / 1 nu_min / 2 nu_max."""
+    point_nu = np.asarray(point_nu, dtype=np.int64).reshape(-1, 2)
+    n, ne, nt = len(point_nu), len(edge_ro), len(tri_ro)
+    ranks = np.concatenate([
+        point_nu.reshape(-1),
+        np.stack([np.asarray(edge_ro), np.asarray(edge_nu_min), np.asarray(edge_nu_max)], axis=1).reshape(-1),
+        np.asarray(tri_ro),
+    ]).astype(np.int64)
+    k = np.arange(len(ranks), dtype=np.int64)
+    st = np.concatenate([np.full(2 * n, 2), np.full(3 * ne, 0), np.full(nt, 1)])
+    at = np.concatenate([np.tile([1, 2], n), np.tile([0, 1, 2], ne), np.zeros(nt, np.int64)])
+    idx = np.concatenate([np.repeat(np.arange(n), 2), np.repeat(np.arange(ne), 3), np.arange(nt)])
+    order = np.argsort(ranks, kind="stable")
+    order = order[ranks[order] != 0]
+    r = ranks[order]
+    first = np.flatnonzero(np.concatenate([[True], r[1:] != r[:-1]])) if len(r) else np.zeros(0, np.int64)
+    spec_pointers = np.concatenate([[-1], first]).astype(np.int32)
+    return (idx[order].astype(np.int32), st[order].astype(np.int32), at[order].astype(np.int32), spec_pointers)
 
 
 def orient2d(a, b, c):

@@ -37,3 +37,28 @@ def compare_alpha(points, vtx, nbr, res, ulp_tol=4):
     if len(spec) == 1 and same_len:
         ok = tri_ok and edge_ok and pt_ok
     return ok, rep
+
+
+def classify_intervals(res, alpha):
+    """Alpha-complex classes (0 exterior, 1 singular, 2 regular, 3 interior)
+    of points, edges and triangles at ``alpha``, from the interval output
+    alone (numpy restatement of the rule documented for galphaQuery)."""
+    spec = np.asarray(res["spectrum"], dtype=np.float64)
+    R = -1 if alpha < 0 else int(np.searchsorted(spec, alpha, side="right") - 1)
+    pt, ed, tr = res["point_list"], res["edge_list"], res["tri_list"]
+
+    def interval(ro, nmin, nmax):
+        c = np.zeros(len(nmin), np.uint8)
+        c[(ro >= 0) & (ro <= R)] = 1
+        c[nmin <= R] = 2
+        c[(nmax > 0) & (nmax <= R)] = 3
+        return c
+
+    if R < 0:
+        return np.zeros(len(pt), np.uint8), np.zeros(len(ed), np.uint8), np.zeros(len(tr), np.uint8), R
+    pc = interval(np.zeros(len(pt), np.int64), pt["nu_min_rank"], pt["nu_max_rank"])
+    pc[pt["nu_min_rank"] < 0] = 0
+    ro = np.where(ed["ro_rank"] != 0, ed["ro_rank"], -1)
+    ec = interval(ro, ed["nu_min_rank"], ed["nu_max_rank"])
+    tc = np.where(tr["ro_rank"] <= R, 3, 0).astype(np.uint8)
+    return pc, ec, tc, R

@@ -75,20 +75,22 @@ def test_headers_compile_as_c_and_cpp(tmp_path):
 
 def test_struct_layouts_match_c(lib, tmp_path):
     """ctypes mirrors must have the C compiler's sizes and offsets."""
-    from galpha_b200.api import Status, _AlphaOut, _Output, _Params
+    from galpha_b200.api import ALPHA_DTYPE, QueryResult, Status, _AlphaOut, _MasterOut, _Output, _Params
 
     src = tmp_path / "sz.c"
     src.write_text('#include "gpudt.h"\n#include "galpha.h"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(GPUDTPARAMS), '
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(GPUDTPARAMS), '
                    'sizeof(GPUDTOUTPUT), sizeof(gpudtStatus), sizeof(GAlphaOutput), sizeof(gpudtTriangle), '
                    'sizeof(galphaEdgeInterval), sizeof(galphaPointInterval), offsetof(GPUDTPARAMS, fboSize), '
-                   'offsetof(gpudtStatus, ms)); return 0;}\n')
+                   'offsetof(gpudtStatus, ms), sizeof(galphaQueryResult), offsetof(galphaQueryResult, nTris), '
+                   'sizeof(galphaAlpha), sizeof(GAlphaMasterList)); return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", INC, str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     mine = [ctypes.sizeof(_Params), ctypes.sizeof(_Output), ctypes.sizeof(Status), ctypes.sizeof(_AlphaOut),
             G.TRIANGLE_DTYPE.itemsize, G.EDGE_INTERVAL_DTYPE.itemsize, G.POINT_INTERVAL_DTYPE.itemsize,
-            _Params.fboSize.offset, Status.ms.offset]
+            _Params.fboSize.offset, Status.ms.offset, ctypes.sizeof(QueryResult), QueryResult.nTris.offset,
+            ALPHA_DTYPE.itemsize, ctypes.sizeof(_MasterOut)]
     assert got == mine
 
 

@@ -243,3 +243,30 @@ def test_alpha_golden(name):
     a = O.alpha(pts, v, nb)
     assert np.array_equal(a["spectrum"], g["spectrum"])
     assert np.array_equal(a["point"], g["point"])
+
+
+def test_master_list_restatement_matches_loop():
+    """oracle.master_list (numpy) against a direct loop over the reference's
+    steps: stable sort by rank, drop rank 0, first index of each run, -1 first."""
+    g = np.load(os.path.join(GOLD, "golden_c1.npz"))
+    pts = np.concatenate([g["points"], g["points"][:5]])  # duplicates give rank -1 vertices
+    v, nb, _ = O.dt(pts)
+    a = O.alpha(pts, v, nb)
+    e = a["edge"]
+    idx, st, at, sp = O.master_list(a["point"], e[:, 2], e[:, 3], e[:, 4], a["tri_ro"])
+    n, ne, nt = len(a["point"]), len(e), len(a["tri_ro"])
+    entries = []
+    for k in range(2 * n + 3 * ne + nt):
+        if k < 2 * n:
+            r, ent = int(a["point"][k // 2][k % 2]), (k // 2, 2, 1 + k % 2)
+        elif k < 2 * n + 3 * ne:
+            q = k - 2 * n
+            r, ent = int(e[q // 3][2 + q % 3]), (q // 3, 0, q % 3)
+        else:
+            r, ent = int(a["tri_ro"][k - 2 * n - 3 * ne]), (k - 2 * n - 3 * ne, 1, 0)
+        entries.append((r, k, ent))
+    entries.sort()
+    kept = [(r, ent) for r, k, ent in entries if r != 0]
+    assert [x[1] for x in kept] == list(zip(idx.tolist(), st.tolist(), at.tolist()))
+    firsts = [-1] + [i for i in range(len(kept)) if i == 0 or kept[i][0] != kept[i - 1][0]]
+    assert firsts == sp.tolist()
