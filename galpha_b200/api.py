@@ -111,6 +111,13 @@ class _MasterOut(ctypes.Structure):
                 ("spec_pointers", ctypes.c_void_p)]
 
 
+class BatchSet(ctypes.Structure):
+    """galphaBatchSet: counts and bases of one set of a batch."""
+    _fields_ = [("nPoints", ctypes.c_int), ("pointBase", ctypes.c_int), ("nTris", ctypes.c_int),
+                ("triBase", ctypes.c_int), ("nEdges", ctypes.c_int), ("edgeBase", ctypes.c_int),
+                ("nSpectrum", ctypes.c_int), ("specBase", ctypes.c_int)]
+
+
 # alpha-complex classes (galpha.h GALPHA_*)
 EXTERIOR, SINGULAR, REGULAR, INTERIOR = 0, 1, 2, 3
 
@@ -152,6 +159,10 @@ def load(path=None):
     L.galphaQuery.argtypes = [vp, ctypes.c_double, ctypes.POINTER(QueryResult)]
     L.galphaQueryQuantile.argtypes = [vp, ctypes.c_double, ctypes.POINTER(QueryResult)]
     L.galphaCopyClasses.argtypes = [vp, vp, vp, vp]
+    L.galphaRunBatch.argtypes = [vp, ip, vp, vp, vp, ip, ctypes.POINTER(Status)]
+    L.galphaRunBatchHost.argtypes = [vp, ip, vp, vp, vp, ip, ctypes.POINTER(Status)]
+    L.galphaBatchSets.argtypes = [vp, vp]
+    L.galphaBatchCopy.argtypes = [vp, vp, vp, vp, vp, vp]
     L.galphaMasterList.argtypes = [vp, ctypes.POINTER(_MasterOut)]
     L.galphaReleaseMasterList.argtypes = [ctypes.POINTER(_MasterOut)]
     L.galphaLastError.restype = ctypes.c_char_p
@@ -351,6 +362,78 @@ class Engine:
         else:
             _check(self._L.galphaQuery(self._h, float(alpha), ctypes.byref(res)), "galphaQuery")
         return res
+
+    # ---------------------------------------------------------------- batches
+    @staticmethod
+    def batch_bounds(sets):
+        """Per-set (minX, minY, maxX, maxY) from the data, as GPUDTPARAMS would hold."""
+        b = np.zeros((len(sets), 4))
+        for k, p in enumerate(sets):
+            p = np.asarray(p, dtype=np.float64).reshape(-1, 2)
+            if len(p):
+                b[k, :2] = p.min(axis=0)
+                b[k, 2:] = p.max(axis=0)
+            else:
+                b[k] = (0.0, 0.0, 1.0, 1.0)
+        return b
+
+    def run_batch(self, sets, bounds=None, with_alpha=True):
+        """DT (+ alpha) of many independent point sets in one pipeline run
+        (galphaRunBatchHost).  sets: list of (n_k, 2) arrays."""
+        sizes = np.array([len(p) for p in sets], dtype=np.int32)
+        xy = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 2) for p in sets])
+                                  if len(sets) else np.zeros((0, 2)))
+        b = np.ascontiguousarray(self.batch_bounds(sets) if bounds is None else bounds, dtype=np.float64)
+        st = Status()
+        _check(self._L.galphaRunBatchHost(self._h, len(sets), sizes.ctypes.data, xy.ctypes.data if len(xy) else None,
+                                          b.ctypes.data, 1 if with_alpha else 0, ctypes.byref(st)),
+               "galphaRunBatchHost")
+        self._batch = (len(sets), bool(with_alpha))
+        return st
+
+    def run_batch_device(self, d_xy_ptr, sizes, bounds, with_alpha=True):
+        """The same on points already in device memory (galphaRunBatch)."""
+        sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+        b = np.ascontiguousarray(bounds, dtype=np.float64)
+        st = Status()
+        _check(self._L.galphaRunBatch(self._h, len(sizes), sizes.ctypes.data, ctypes.c_void_p(d_xy_ptr),
+                                      b.ctypes.data, 1 if with_alpha else 0, ctypes.byref(st)), "galphaRunBatch")
+        self._batch = (len(sizes), bool(with_alpha))
+        return st
+
+    def batch_sets(self):
+        k = self._batch[0]
+        arr = (BatchSet * k)()
+        _check(self._L.galphaBatchSets(self._h, arr), "galphaBatchSets")
+        return arr
+
+    def batch_results(self):
+        """Per-set results of the last batch: list of dicts with ``triangles``
+        (TRIANGLE_DTYPE, set-local indices) and, with alpha, ``spectrum``,
+        ``point_list``, ``edge_list``, ``tri_list``."""
+        k, alpha = self._batch
+        sets = self.batch_sets()
+        nt = sum(s.nTris for s in sets)
+        npt = sum(s.nPoints for s in sets)
+        ne = sum(s.nEdges for s in sets)
+        nsp = sum(s.nSpectrum for s in sets)
+        tri = np.empty(nt, TRIANGLE_DTYPE)
+        pt = np.empty(npt, POINT_INTERVAL_DTYPE) if alpha else None
+        ed = np.empty(ne, EDGE_INTERVAL_DTYPE) if alpha else None
+        tr = np.empty(nt, TRIANGLE_INTERVAL_DTYPE) if alpha else None
+        sp = np.empty(nsp, np.float64) if alpha else None
+        ptr = lambda a: a.ctypes.data if a is not None and len(a) else None
+        _check(self._L.galphaBatchCopy(self._h, ptr(tri), ptr(pt), ptr(ed), ptr(tr), ptr(sp)), "galphaBatchCopy")
+        out = []
+        for s in sets:
+            d = {"triangles": tri[s.triBase:s.triBase + s.nTris]}
+            if alpha:
+                d.update(spectrum=sp[s.specBase:s.specBase + s.nSpectrum],
+                         point_list=pt[s.pointBase:s.pointBase + s.nPoints],
+                         edge_list=ed[s.edgeBase:s.edgeBase + s.nEdges],
+                         tri_list=tr[s.triBase:s.triBase + s.nTris])
+            out.append(d)
+        return out
 
     def master_list(self):
         """master_list (ALPHA_DTYPE array) and spec_pointers of the resident alpha

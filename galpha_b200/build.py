@@ -15,7 +15,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libgalpha.so")
 OBJDIR = os.path.join(LIBDIR, "obj")
 
-SOURCES = ["api.cu", "dt_grid.cu", "voronoi_kernels.cu", "dt_mesh.cu", "alpha.cu", "sort.cu", "scan.cu", "master.cu", "noalloc.cu"]
+SOURCES = ["api.cu", "dt_grid.cu", "voronoi_kernels.cu", "dt_mesh.cu", "alpha.cu", "sort.cu", "scan.cu", "master.cu", "batch.cu", "noalloc.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -228,6 +228,7 @@ struct MarkRuns {
     int *unc;
     int n;
     Counters *ct;
+    const int *seg;  // set of each entry (batched stage) or nullptr
     __device__ void operator()(long long ii) const
     {
         int i = (int)ii;
@@ -235,7 +236,7 @@ struct MarkRuns {
             nr[0] = 0;
             return;
         }
-        if (i >= 2 && near_equal(keys[i - 1], keys[i])) {
+        if (i >= 2 && (!seg || seg[i] == seg[i - 1]) && near_equal(keys[i - 1], keys[i])) {
             nr[i] = 0;
             int k = atomicAdd(&ct->nlist, 1);
             unc[k] = i;
@@ -284,6 +285,7 @@ struct ExactAdjacent {
     const double2 *P;
     int nT;
     Counters *ct;
+    const int *seg;
     __device__ void operator()(long long ii) const
     {
         int i = unc[ii];
@@ -300,7 +302,7 @@ struct ExactAdjacent {
             atomicAdd(&ct->nties, 1);
         } else {
             int s = i - 1;
-            while (s >= 2 && near_equal(keys[s - 1], keys[s])) s--;
+            while (s >= 2 && (!seg || seg[s - 1] == seg[s]) && near_equal(keys[s - 1], keys[s])) s--;
             if (atomicCAS(&slowflag[s], 0, 1) == 0) {
                 int k = atomicAdd(&ct->nlist2, 1);
                 slow[k] = s;
@@ -321,11 +323,12 @@ struct ResolveRuns {
     const double2 *P;
     int n, nT;
     Counters *ct;
+    const int *seg;
     __device__ void operator()(long long ii) const
     {
         int s = runs[ii];
         int e = s;
-        while (e + 1 < n && near_equal(keys[e], keys[e + 1])) e++;
+        while (e + 1 < n && (!seg || seg[e] == seg[e + 1]) && near_equal(keys[e], keys[e + 1])) e++;
         if (e - s > kMaxSlowRun) {
             set_err(ct, GPUDT_ERR_EXACT, 113);
             return;
@@ -420,8 +423,90 @@ struct FixPt {
     }
 };
 
+// ------------------------------------------------------- batched segments
+// Set of each value-sorted entry (triangle, or the triangle that owns the edge).
+struct EntrySet {
+    const int *vals;
+    const int4 *edges;
+    const int *tset;
+    int nT;
+    unsigned *key;
+    int *pos;
+    __device__ void operator()(long long i) const
+    {
+        int v = vals[i];
+        int t = v < nT ? v : edges[v - nT].z;
+        key[i] = (unsigned)tset[t];
+        pos[i] = (int)i;
+    }
+};
+
+struct GatherEntries {
+    const unsigned long long *keys;
+    const int *vals, *pos;
+    const unsigned *setkey;
+    unsigned long long *okeys;
+    int *ovals, *seg;  // seg is indexed like the full entry array (entry 0 = sentinel)
+    __device__ void operator()(long long i) const
+    {
+        int p = pos[i];
+        okeys[i] = keys[p];
+        ovals[i] = vals[p];
+        seg[1 + i] = (int)setkey[i];
+        if (i == 0) seg[0] = -1;
+    }
+};
+
+// Per set: the global rank count before its first entry, and its number of
+// distinct values (entries of a set are contiguous; each set's first entry
+// starts a rank).
+struct SetRankBounds {
+    const int *seg, *nr, *excl;
+    int n;
+    int *firstexcl, *endrank;
+    __device__ void operator()(long long ii) const
+    {
+        int i = (int)ii;
+        if (i == 0) return;
+        int s = seg[i];
+        if (i == 1 || seg[i - 1] != s) firstexcl[s] = excl[i];
+        if (i == n - 1 || seg[i + 1] != s) endrank[s] = excl[i] + nr[i];
+    }
+};
+
+struct SetDistinct {
+    const int *firstexcl;
+    int *nd;  // in: end rank (0 for a set without entries); out: distinct values
+    __device__ void operator()(long long s) const { nd[s] -= firstexcl[s]; }
+};
+
+struct ScatterRanksSeg {
+    const unsigned long long *keys;
+    const int *vals, *nr, *excl, *seg, *firstexcl, *spec_off;
+    int *tri_ro, *edge_ro;
+    double *spectrum;
+    int nT;
+    __device__ void operator()(long long ii) const
+    {
+        int i = (int)ii;
+        if (i == 0) return;
+        int s = seg[i];
+        int r = excl[i] + nr[i] - firstexcl[s];
+        int v = vals[i];
+        if (v < nT) tri_ro[v] = r;
+        else edge_ro[v - nT] = r;
+        if (nr[i]) spectrum[spec_off[s] + s + r] = __longlong_as_double((long long)keys[i]);
+    }
+};
+
+struct SetSentinels {
+    const int *spec_off;
+    double *spectrum;
+    __device__ void operator()(long long s) const { spectrum[spec_off[s] + s] = 0.0; }
+};
+
 // ------------------------------------------------------------------ stage
-int stage_alpha(Ctx &c)
+int stage_alpha(Ctx &c, AlphaSegs *segs)
 {
     int r;
     const int nT = c.nT_out;
@@ -451,25 +536,56 @@ int stage_alpha(Ctx &c)
     c.nSpecIn = nIn;
     r = radix_sort(c, c.keys + 1, c.vals + 1, c.keys2, c.vals2, nIn - 1);
     if (r) return r;
+    if (segs) {
+        // stable sort by set: entries end up ordered by (set, value)
+        const int m = nIn - 1;
+        unsigned *ka = (unsigned *)c.keys2, *kb = ka + ((m + 63) & ~63);
+        launch_n(c, EntrySet{c.vals + 1, c.edges, segs->tset, nT, ka, c.vals2}, m);
+        r = radix_sort32(c, ka, c.vals2, kb, c.aux2, m, c.rhist);
+        if (r) return r;
+        unsigned long long *tk = (unsigned long long *)c.spectrum;
+        launch_n(c, GatherEntries{c.keys + 1, c.vals + 1, c.vals2, ka, tk, c.rank, segs->seg}, m);
+        GALPHA_CUDA(cudaMemcpyAsync(c.keys + 1, tk, sizeof(unsigned long long) * (size_t)m,
+                                    cudaMemcpyDeviceToDevice, c.stream));
+        GALPHA_CUDA(cudaMemcpyAsync(c.vals + 1, c.rank, sizeof(int) * (size_t)m, cudaMemcpyDeviceToDevice,
+                                    c.stream));
+    }
     // ranks
     int *nr = c.aux, *unc = c.list, *slow = c.list2, *slowflag = c.stamp;
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int), c.stream));
-    launch_n(c, MarkRuns{c.keys, nr, unc, nIn, c.ctr}, nIn);
+    launch_n(c, MarkRuns{c.keys, nr, unc, nIn, c.ctr, segs ? segs->seg : nullptr}, nIn);
     r = read_counters(c);
     if (r) return r;
     int nunc = c.hctr->nlist;
     if (nunc > 0) {
         GALPHA_CUDA(cudaMemsetAsync(slowflag, 0, sizeof(int) * (size_t)nIn, c.stream));
-        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, c.cv, c.edges, c.opos, nT, c.ctr}, nunc);
+        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, c.cv, c.edges, c.opos, nT, c.ctr,
+                                  segs ? segs->seg : nullptr},
+                 nunc);
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
         if (c.hctr->nlist2 > 0)
-            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, c.cv, c.edges, c.opos, nIn, nT, c.ctr}, c.hctr->nlist2);
+            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, c.cv, c.edges, c.opos, nIn, nT, c.ctr,
+                                    segs ? segs->seg : nullptr},
+                     c.hctr->nlist2);
     }
     r = exclusive_scan_int(c, nr, c.rank, nIn, &c.ctr->nlist);
     if (r) return r;
-    launch_n(c, ScatterRanks{c.keys, c.vals, nr, c.rank, c.tri_ro, c.edge_ro, c.spectrum, nT}, nIn);
+    if (!segs) {
+        launch_n(c, ScatterRanks{c.keys, c.vals, nr, c.rank, c.tri_ro, c.edge_ro, c.spectrum, nT}, nIn);
+    } else {
+        GALPHA_CUDA(cudaMemsetAsync(segs->nd, 0, sizeof(int) * (size_t)segs->K, c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(segs->firstexcl, 0, sizeof(int) * (size_t)segs->K, c.stream));
+        launch_n(c, SetRankBounds{segs->seg, nr, c.rank, nIn, segs->firstexcl, segs->nd}, nIn);
+        launch_n(c, SetDistinct{segs->firstexcl, segs->nd}, segs->K);
+        r = exclusive_scan_int(c, segs->nd, segs->spec_off, segs->K, nullptr);
+        if (r) return r;
+        launch_n(c, ScatterRanksSeg{c.keys, c.vals, nr, c.rank, segs->seg, segs->firstexcl, segs->spec_off,
+                                    c.tri_ro, c.edge_ro, c.spectrum, nT},
+                 nIn);
+        launch_n(c, SetSentinels{segs->spec_off, c.spectrum}, segs->K);
+    }
     launch_n(c, InitPt{c.pt_nu}, c.N);
     launch_n(c, EdgeIntervals{c.edges, c.cn, c.tri_ro, c.edge_ro, c.edge_nu, c.pt_nu}, nE);
     launch_n(c, FixPt{c.pt_nu}, c.N);
@@ -477,7 +593,7 @@ int stage_alpha(Ctx &c)
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->err) return c.hctr->err;
-    c.nSpec = c.hctr->nlist + 1;  // distinct ranks incl. the sentinel
+    c.nSpec = c.hctr->nlist + (segs ? segs->K : 1);  // distinct ranks incl. the sentinel(s)
     return GPUDT_OK;
 }
 

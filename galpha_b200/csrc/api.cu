@@ -50,6 +50,7 @@ struct Arena {
 
 struct Sizes {
     size_t V, T2, cap, lists, ntiles;
+    size_t occw = 0, bandw = 0;  // occupancy words (0: a single T x T texture)
 };
 
 static size_t plan(const Sizes &z, Ctx *c, Arena *A)
@@ -63,6 +64,7 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     size_t V = z.V, cap = z.cap, T2 = z.T2, L = z.lists;
     size_t T = (size_t)std::llround(std::sqrt((double)T2));
     size_t W2 = ((T >> 6) + 31) / 32;
+    const size_t occw = z.occw ? z.occw : T * (T / 32), bandw = z.bandw ? z.bandw : T * W2;
 #define TAKE(field, type, count) \
     {                            \
         void *p_ = take(sizeof(type) * (size_t)(count)); \
@@ -72,8 +74,8 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(pos, double2, V);
     TAKE(gpix, short2, V);
     TAKE(idmap, int, T2);
-    TAKE(occ, uint32_t, T * (T / 32));
-    TAKE(bandocc, uint32_t, T * W2);
+    TAKE(occ, uint32_t, occw);
+    TAKE(bandocc, uint32_t, bandw);
     TAKE(ycol, int16_t, T2);
     TAKE(colour, int, T2);
     TAKE(list, int, L);
@@ -122,19 +124,28 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
 struct HandleState {
     Ctx c;
     Arena arena;
+    BatchHost bh;
+    BatchDev bd;
     double *d_xy = nullptr;
     size_t d_xy_cap = 0;
 };
 
+static int ensure_sizes(HandleState &H, const Sizes &z);
+
 static int ensure(HandleState &H, int V, int T, long long nExtraTris)
 {
-    Ctx &c = H.c;
     Sizes z;
     z.V = (size_t)V;
     z.T2 = (size_t)T * T;
     z.cap = (size_t)2 * V + 64 + (size_t)(nExtraTris > 0 ? nExtraTris : 0);
     z.lists = std::max(z.cap * 3, z.V + 1);
     z.ntiles = ((size_t)(T - 1) * (T - 1) + 255) / 256 + 1;
+    return ensure_sizes(H, z);
+}
+
+static int ensure_sizes(HandleState &H, const Sizes &z)
+{
+    Ctx &c = H.c;
     size_t need = plan(z, nullptr, nullptr);
     if (c.budget > 0 && (long long)need > c.budget) {
         g_err = "device memory budget exceeded";
@@ -238,6 +249,99 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     c.st.exactIncircle = (long long)c.hctr->exact_incircle;
     c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
     c.have_mesh = true;
+    return GPUDT_OK;
+}
+
+// ------------------------------------------------------------------ batches
+struct EdgeBases {
+    const int *e_off, *tbase;
+    int nT, nE;
+    int *out;
+    __device__ void operator()(long long s) const
+    {
+        int t = tbase[s];
+        out[s] = t < nT ? e_off[t] : nE;
+    }
+};
+
+static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy, const double *bounds, int withAlpha)
+{
+    Ctx &c = H.c;
+    BatchHost &bh = H.bh;
+    bh.valid = false;
+    int r = batch_plan(bh, K, sizes, bounds);
+    if (r) {
+        g_err = "galphaRunBatch: invalid set sizes or bounds";
+        return r;
+    }
+    Sizes z;
+    z.V = (size_t)bh.N + bh.Fmax;
+    z.T2 = (size_t)bh.T2;
+    z.occw = (size_t)bh.occw;
+    z.bandw = (size_t)bh.band;
+    z.cap = 2 * z.V + 64;
+    z.lists = std::max(z.cap * 3, z.V + 1);
+    int Tmax = 128;
+    for (auto &C : bh.classes) Tmax = std::max(Tmax, C.T);
+    z.ntiles = std::max<size_t>(((size_t)(Tmax - 1) * (Tmax - 1) + 255) / 256 + 1, (size_t)bh.ntiles + 1);
+    r = ensure_sizes(H, z);
+    if (r) return r;
+    r = batch_buffers(c, H.bd, K, bh.N, (int)z.V, c.cap_tris, 3 * c.cap_tris + 8);
+    if (r) return r;
+    memset(&c.st, 0, sizeof(c.st));
+    for (int k = 0; k < 8; k++) c.kev_rec[k] = false;
+    c.have_mesh = c.have_alpha = c.have_master = false;
+    ev_record(c, 1);
+    const char *stage = "setup";
+#define STAGE(name, call)        \
+    stage = name;                \
+    r = (call);                  \
+    if (r) return stage_fail(c, r, stage)
+    STAGE("setup", batch_setup(c, H.bd, bh, d_xy));
+    STAGE("voronoi", batch_voronoi(c, H.bd, bh));
+    ev_record(c, 2);
+    STAGE("links", stage_links(c));
+    ev_record(c, 3);
+    STAGE("shift", stage_shift(c));
+    ev_record(c, 4);
+    STAGE("missing", stage_missing(c));
+    ev_record(c, 5);
+    STAGE("boundary", stage_boundary(c));
+    ev_record(c, 6);
+    STAGE("flip", stage_flip(c));
+    ev_record(c, 7);
+    STAGE("compact", batch_compact(c, H.bd, bh));
+    ev_record(c, 8);
+    c.have_mesh = true;
+    bh.alpha = false;
+    if (withAlpha) {
+        AlphaSegs segs{H.bd.tset, K, H.bd.seg, H.bd.firstexcl, H.bd.nd, H.bd.spec_off};
+        STAGE("alpha", stage_alpha(c, &segs));
+        c.have_alpha = true;
+        bh.alpha = true;
+        launch_n(c, EdgeBases{c.e_off, H.bd.tbase, c.nT_out, c.nE, H.bd.firstexcl}, K);
+        bh.ebase.resize(K);
+        bh.nd.resize(K);
+        bh.specoff.resize(K);
+        GALPHA_CUDA(cudaMemcpyAsync(bh.ebase.data(), H.bd.firstexcl, sizeof(int) * (size_t)K, cudaMemcpyDeviceToHost,
+                                    c.stream));
+        GALPHA_CUDA(cudaMemcpyAsync(bh.nd.data(), H.bd.nd, sizeof(int) * (size_t)K, cudaMemcpyDeviceToHost, c.stream));
+        GALPHA_CUDA(cudaMemcpyAsync(bh.specoff.data(), H.bd.spec_off, sizeof(int) * (size_t)K, cudaMemcpyDeviceToHost,
+                                    c.stream));
+        GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+        for (int s2 = 0; s2 < K; s2++) bh.specoff[s2] += s2;  // one rank-0 sentinel per set
+    }
+    ev_record(c, 9);
+#undef STAGE
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->err) return stage_fail(c, c.hctr->err, "final");
+    c.st.nVerts = c.V;
+    c.st.nFake = c.F;
+    c.st.exactOrient = (long long)c.hctr->exact_orient;
+    c.st.exactIncircle = (long long)c.hctr->exact_incircle;
+    c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
+    bh.valid = true;
     return GPUDT_OK;
 }
 
@@ -365,6 +469,7 @@ int galphaDestroy(galphaHandle h)
     if (h->H.arena.base) cudaFree(h->H.arena.base);
     if (h->H.d_xy) cudaFree(h->H.d_xy);
     if (c.ml_buf) cudaFree(c.ml_buf);
+    if (h->H.bd.buf) cudaFree(h->H.bd.buf);
     if (c.hctr) cudaFreeHost(c.hctr);
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2 && c.events; k++) cudaEventDestroy(c.ev[k]);
     for (int k = 0; k < 8 && c.events; k++) cudaEventDestroy(c.kev[k]);
@@ -664,6 +769,94 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
     if (r) return r;
     c.have_alpha = true;
     return download_alpha(c, out);
+}
+
+int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double *d_xy, const double *bounds,
+                   int withAlpha, gpudtStatus *st)
+{
+    if (!h || nSets <= 0 || !setSizes || !bounds) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
+    ev_record(c, 0);
+    int r = run_batch(h->H, nSets, setSizes, d_xy, bounds, withAlpha);
+    if (!r) fill_times(c, withAlpha ? 9 : 8);
+    c.st.status = r;
+    if (st) *st = c.st;
+    return r;
+}
+
+int galphaRunBatchHost(galphaHandle h, int nSets, const int *setSizes, const double *xy, const double *bounds,
+                       int withAlpha, gpudtStatus *st)
+{
+    if (!h || nSets <= 0 || !setSizes || !bounds) return GPUDT_ERR_ARG;
+    long long n = 0;
+    for (int s = 0; s < nSets; s++) n += setSizes[s] > 0 ? setSizes[s] : 0;
+    if (n > 0x3fffffffLL || (n > 0 && !xy)) return GPUDT_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        cudaSetDevice(h->H.c.device);
+        cudaGetLastError();
+        ev_record(h->H.c, 0);
+        int r = upload_points(h->H, (const gpudtVertex *)xy, (int)n);
+        if (r) return r;
+    }
+    return galphaRunBatch(h, nSets, setSizes, h->H.d_xy, bounds, withAlpha, st);
+}
+
+int galphaBatchSets(galphaHandle h, galphaBatchSet *sets)
+{
+    if (!h || !sets) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    BatchHost &bh = h->H.bh;
+    Ctx &c = h->H.c;
+    if (!bh.valid) return GPUDT_ERR_ARG;
+    for (int s = 0; s < bh.K; s++) {
+        galphaBatchSet &o = sets[s];
+        o.nPoints = bh.sets[s].n;
+        o.pointBase = bh.sets[s].vbase;
+        o.triBase = bh.tbase[s];
+        o.nTris = bh.tbase[s + 1] - bh.tbase[s];
+        if (bh.alpha) {
+            o.edgeBase = bh.ebase[s];
+            o.nEdges = (s + 1 < bh.K ? bh.ebase[s + 1] : c.nE) - bh.ebase[s];
+            o.specBase = bh.specoff[s];
+            o.nSpectrum = bh.nd[s] + 1;
+        } else {
+            o.edgeBase = o.nEdges = o.specBase = o.nSpectrum = 0;
+        }
+    }
+    return GPUDT_OK;
+}
+
+int galphaBatchCopy(galphaHandle h, gpudtTriangle *tris, galphaPointInterval *points, galphaEdgeInterval *edges,
+                    int *triRanks, double *spectrum)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    BatchHost &bh = h->H.bh;
+    Ctx &c = h->H.c;
+    if (!bh.valid) return GPUDT_ERR_ARG;
+    if (!bh.alpha && (points || edges || triRanks || spectrum)) return GPUDT_ERR_ARG;
+    cudaSetDevice(c.device);
+    cudaStream_t s = c.stream;
+    gpudtTriangle *dtri = h->H.bd.otri;
+    galphaEdgeInterval *dedge = c.edge_aos;
+    int r = batch_local_outputs(c, h->H.bd, tris ? dtri : nullptr, edges ? dedge : nullptr);
+    if (r) return r;
+    if (tris && c.nT_out > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(tris, dtri, sizeof(gpudtTriangle) * (size_t)c.nT_out, cudaMemcpyDeviceToHost, s));
+    if (edges && c.nE > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(edges, dedge, sizeof(galphaEdgeInterval) * (size_t)c.nE, cudaMemcpyDeviceToHost, s));
+    if (points && c.N > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(points, c.pt_nu, sizeof(int2) * (size_t)c.N, cudaMemcpyDeviceToHost, s));
+    if (triRanks && c.nT_out > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(triRanks, c.tri_ro, sizeof(int) * (size_t)c.nT_out, cudaMemcpyDeviceToHost, s));
+    if (spectrum && c.nSpec > 0)
+        GALPHA_CUDA(cudaMemcpyAsync(spectrum, c.spectrum, sizeof(double) * (size_t)c.nSpec, cudaMemcpyDeviceToHost, s));
+    GALPHA_CUDA(cudaStreamSynchronize(s));
+    return GPUDT_OK;
 }
 
 static const int kMinusOneHost = -1;

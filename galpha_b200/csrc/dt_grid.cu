@@ -34,7 +34,7 @@ namespace galpha {
 // ---------------------------------------------------------------- scaling
 // scale and shift are multiples of u = 2^e with scale/u < 2^37 and
 // |coordinate|/u < 2^51, so shift + g*scale is exact for |g| < 2^15.
-static void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale,
+void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale,
                          double &sx, double &sy)
 {
     int D = T - 2 * kMargin;  // usable pixels [kMargin, T-1-kMargin]
@@ -388,7 +388,15 @@ int stage_voronoi(Ctx &c)
         // an island component too large for a local repair: global path
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, 2 * sizeof(int), c.stream));  // ntris, nfree
     }
-    r0 = launch_row_pass(c);
+    return voronoi_global(c);
+}
+
+// Envelope colouring of the whole texture c.T x c.T at c.ycol / c.idmap into
+// c.colour, then the global island repair.
+int voronoi_global(Ctx &c)
+{
+    const int T = c.T;
+    int r0 = launch_row_pass(c);
     if (r0) return r0;
     GALPHA_CUDA(cudaGetLastError());
     // islands
@@ -399,7 +407,7 @@ int stage_voronoi(Ctx &c)
     int r = read_counters(c);
     if (r) return r;
     int total = c.hctr->nlist;
-    c.st.nIslandPixels = total;
+    c.st.nIslandPixels += total;
     if (total == 0) return GPUDT_OK;
     // iterate detection around newly marked pixels
     int from = 0, to = total, guard = 0;
@@ -415,7 +423,6 @@ int stage_voronoi(Ctx &c)
         if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
     }
     total = to;
-    c.st.nIslandPixels = total;
     // recolour
     guard = 0;
     while (true) {
@@ -430,23 +437,33 @@ int stage_voronoi(Ctx &c)
     return GPUDT_OK;
 }
 
-int stage_triangles(Ctx &c)
+// Dual triangles of c.colour appended at slot `base` (c.ctr->ntris = base + count).
+int emit_global(Ctx &c, int base)
 {
-    if (c.fused_done) return GPUDT_OK;  // emitted by the fused kernel
     const int T = c.T;
     long long nwin = (long long)(T - 1) * (T - 1);
     int ntiles = (int)((nwin + kEmitTile - 1) / kEmitTile);
-    int r0 = launch_emit(c, ntiles, nwin, false);
+    int r0 = launch_emit(c, ntiles, nwin, false, nullptr);
     if (r0) return r0;
-    int r = exclusive_scan_int(c, c.tilecount, c.tilecount, ntiles, &c.ctr->ntris);
+    int r = exclusive_scan_int(c, c.tilecount, c.tilecount, ntiles, &c.ctr->nlist2);
     if (r) return r;
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->err) return c.hctr->err;
-    if (c.hctr->ntris > c.cap_tris) return GPUDT_ERR_NOMEM;
-    r = launch_emit(c, ntiles, nwin, true);
+    const int total = c.hctr->nlist2;
+    if ((long long)base + total > c.cap_tris) return GPUDT_ERR_NOMEM;
+    r = launch_emit(c, ntiles, nwin, true, c.tv + base);
     if (r) return r;
+    const int nt = base + total;
+    GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->ntris, &nt, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));  // nt lives on this stack frame
     return GPUDT_OK;
+}
+
+int stage_triangles(Ctx &c)
+{
+    if (c.fused_done) return GPUDT_OK;  // emitted by the fused kernel
+    return emit_global(c, 0);
 }
 
 }  // namespace galpha

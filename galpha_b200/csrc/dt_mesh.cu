@@ -1163,7 +1163,8 @@ struct ReflexCheck {
     const double2 *pos;
     const int *vtri, *cand;
     const int8_t *vstate;
-    int *list;
+    int *list, *stamp;
+    int round;
     Counters *ct;
     __device__ void operator()(long long ii) const
     {
@@ -1171,40 +1172,62 @@ struct ReflexCheck {
         if (vtri[v] < 0) return;
         int u, w, tin, tout;
         if (!hull_neighbours(tv, tn, v, vtri[v], &u, &w, &tin, &tout)) return;
-        if (orientp(pos[u], pos[v], pos[w], ct) < 0) {
+        if (orientp(pos[u], pos[v], pos[w], ct) < 0 && atomicExch(&stamp[v], round) != round) {
             int k = atomicAdd(&ct->nlist, 1);
             list[k] = v;
         }
     }
 };
 
-// Sequential fill of reflex hull vertices (rare): adds triangle (u, w, v) for a
-// reflex v between hull neighbours u and w, then re-examines u and w.
-struct Convexify {
-    int4 *tv, *tn;
+// Parallel fill of reflex hull vertices, in rounds.  A reflex v (orient(u, v,
+// w) < 0 for its hull neighbours u, w) gets the triangle (u, w, v); an
+// operation claims u, v and w (minimum vertex id wins), so concurrent
+// operations touch disjoint hull triangles.  Winners requeue u and w (they may
+// have become reflex), losers requeue themselves.
+struct ConvexPropose {
+    const int4 *tv, *tn;
     const double2 *pos;
-    int *vtri, *freelist;
-    const int *list;
-    int nlist, cap;
+    const int *vtri, *list;
+    const int *n_in;
+    int *vote;
+    int4 *prop;  // (u, w, tin, tout) per list entry, u = -1: nothing to do
     Counters *ct;
-    __device__ void operator()(long long) const;
+    __device__ void operator()(long long ii) const
+    {
+        int v = list[ii];
+        prop[ii] = make_int4(-1, -1, -1, -1);
+        if (vtri[v] < 0) return;
+        int u, w, tin, tout;
+        if (!hull_neighbours(tv, tn, v, vtri[v], &u, &w, &tin, &tout)) return;
+        if (orientp(pos[u], pos[v], pos[w], ct) >= 0) return;
+        prop[ii] = make_int4(u, w, tin, tout);
+        atomicMin(&vote[u], v);
+        atomicMin(&vote[v], v);
+        atomicMin(&vote[w], v);
+    }
 };
 
-__device__ void Convexify::operator()(long long) const
-{
-    int stack[1024];
-    int sp = 0;
-    for (int k = 0; k < nlist && sp < 1024; k++) stack[sp++] = list[k];
-    for (int guard = 0; sp > 0; guard++) {
-        if (guard > (1 << 22)) {
-            set_err(ct, GPUDT_ERR_NOCONVERGE, 80);
+struct ConvexApply {
+    int4 *tv, *tn;
+    int *vtri, *freelist, *stamp;
+    const int *list, *vote;
+    const int4 *prop;
+    int *list_out, *n_out;
+    int cap, round;
+    Counters *ct;
+    __device__ void push(int x) const
+    {
+        if (atomicExch(&stamp[x], round) != round) list_out[atomicAdd(n_out, 1)] = x;
+    }
+    __device__ void operator()(long long ii) const
+    {
+        int4 p = prop[ii];
+        if (p.x < 0) return;
+        int v = list[ii], u = p.x, w = p.y, tin = p.z, tout = p.w;
+        if (vote[u] != v || vote[v] != v || vote[w] != v) {
+            push(v);
             return;
         }
-        int v = stack[--sp];
-        if (vtri[v] < 0) continue;
-        int u, w, tin, tout;
-        if (!hull_neighbours(tv, tn, v, vtri[v], &u, &w, &tin, &tout)) continue;
-        if (orientp(pos[u], pos[v], pos[w], ct) >= 0) continue;
         int s = alloc_slot(freelist, ct, cap);
         if (s < 0) return;
         // (u, w, v): opp u (0) = w->v, the reverse of hull edge v->w (tout);
@@ -1216,15 +1239,24 @@ __device__ void Convexify::operator()(long long) const
         vtri[u] = enc(s, 0);
         vtri[w] = enc(s, 1);
         vtri[v] = enc(s, 2);
-        if (sp + 2 <= 1024) {
-            stack[sp++] = u;
-            stack[sp++] = w;
-        } else {
-            set_err(ct, GPUDT_ERR_NOMEM, 81);
-            return;
-        }
+        push(u);
+        push(w);
     }
-}
+};
+
+struct ConvexReset {
+    const int4 *prop;
+    const int *list;
+    int *vote;
+    __device__ void operator()(long long ii) const
+    {
+        int4 p = prop[ii];
+        if (p.x < 0) return;
+        vote[p.x] = 0x7fffffff;
+        vote[p.y] = 0x7fffffff;
+        vote[list[ii]] = 0x7fffffff;
+    }
+};
 
 int stage_boundary(Ctx &c)
 {
@@ -1258,19 +1290,31 @@ int stage_boundary(Ctx &c)
     if (r) return r;
     int ncand = c.hctr->nlist2;
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-    launch_n(c, ReflexCheck{c.tv, c.tn, c.pos, c.vtri, cand, c.vstate, c.list, c.ctr}, ncand);
+    launch_n(c, ReflexCheck{c.tv, c.tn, c.pos, c.vtri, cand, c.vstate, c.list, c.stamp, next_round(c), c.ctr}, ncand);
     r = read_counters(c);
     if (r) return r;
-    if (c.hctr->nlist > 0) {
-        launch_n(c, Convexify{c.tv, c.tn, c.pos, c.vtri, c.freelist, c.list, c.hctr->nlist, c.cap_tris, c.ctr}, 1);
+    int n = c.hctr->nlist;
+    int *lin = c.list, *lout = c.list2;
+    int4 *prop = c.fwd;
+    for (int guard = 0; n > 0; guard++) {
+        if (guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        int round = next_round(c);
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+        launch_n(c, ConvexPropose{c.tv, c.tn, c.pos, c.vtri, lin, nullptr, c.vote, prop, c.ctr}, n);
+        launch_n(c, ConvexApply{c.tv, c.tn, c.vtri, c.freelist, c.stamp, lin, c.vote, prop, lout, &c.ctr->nlist2,
+                                c.cap_tris, round, c.ctr},
+                 n);
+        launch_n(c, ConvexReset{prop, lin, c.vote}, n);
         GALPHA_CUDA(cudaGetLastError());
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        if (c.hctr->nfree < 0) {
-            int z = 0;
-            GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->nfree, &z, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-        }
+        n = c.hctr->nlist2;
+        std::swap(lin, lout);
+    }
+    if (c.hctr->nfree < 0) {
+        int z = 0;
+        GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->nfree, &z, sizeof(int), cudaMemcpyHostToDevice, c.stream));
     }
     return GPUDT_OK;
 }
@@ -1504,6 +1548,11 @@ struct CompactWrite {
         out[k] = g;
     }
 };
+
+void launch_compact_write(Ctx &c, const int *newidx, int nslots)
+{
+    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri}, nslots);
+}
 
 int stage_compact(Ctx &c)
 {

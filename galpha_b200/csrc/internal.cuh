@@ -6,6 +6,7 @@
 // between stages read a small pinned counter block.
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include <stdint.h>
 #include <stddef.h>
 #include "../../include/gpudt.h"
@@ -271,7 +272,64 @@ int stage_missing(Ctx &c);
 int stage_boundary(Ctx &c);
 int stage_flip(Ctx &c);
 int stage_compact(Ctx &c);
-int stage_alpha(Ctx &c);
+// ------------------------------------------------------------------ batches
+// One point set of a batch: its grid scaling, its texture cell and its
+// vertex / fake ranges (batch.cu).
+struct SetDesc {
+    double scale, sx, sy, minX, minY, maxX, maxY;
+    long long tex;   // first pixel of the set's cell in ycol / idmap
+    long long occw;  // first word of the cell in occ
+    long long band;  // first word of the cell in bandocc
+    int n, vbase, fbase, nfake, nside, T, logT, W2, live;
+};
+
+struct BatchClass {   // cells of one texture size, stacked
+    int T, logT, W2, cells;
+    long long tex, occw, band;  // first pixel / words of the class
+    int tile0;                  // first fused tile of the class
+    std::vector<int> sets;      // set of each cell
+};
+
+struct BatchHost {
+    std::vector<SetDesc> sets;
+    std::vector<BatchClass> classes;
+    std::vector<int> tbase, ebase, nd, specoff;  // per set after a run (K + 1 entries for bases)
+    int K = 0, N = 0, Fmax = 0;
+    long long T2 = 0, occw = 0, band = 0;
+    int ntiles = 0;
+    bool alpha = false, valid = false;
+};
+
+struct BatchDev {
+    char *buf = nullptr;
+    size_t bytes = 0;
+    SetDesc *sets = nullptr;
+    int *vbases = nullptr, *fbases = nullptr, *vset = nullptr, *vsetall = nullptr, *first = nullptr,
+        *offline = nullptr, *esc = nullptr, *tset = nullptr, *tbase = nullptr, *seg = nullptr,
+        *firstexcl = nullptr, *nd = nullptr, *spec_off = nullptr;
+    gpudtTriangle *otri = nullptr;  // [cap] set-local output triangles
+};
+
+void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale, double &sx, double &sy);
+void launch_compact_write(Ctx &c, const int *newidx, int nslots);
+int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds);
+int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec);
+int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy);
+int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh);
+int batch_compact(Ctx &c, BatchDev &B, BatchHost &bh);
+int batch_local_outputs(Ctx &c, BatchDev &B, gpudtTriangle *tris, galphaEdgeInterval *edges);
+
+// Segments of a batched alpha stage: entries are ranked per point set (set of
+// a compacted triangle: tset), each set with its own rank 0 sentinel.
+struct AlphaSegs {
+    const int *tset;  // [nT] set of each compacted triangle
+    int K;            // number of sets
+    int *seg;         // [nSpecIn] scratch: set of each sorted entry
+    int *firstexcl;   // [K] global rank count before the set's first entry
+    int *nd;          // [K] distinct values of the set
+    int *spec_off;    // [K + 1] first spectrum slot of the set (its rank 0)
+};
+int stage_alpha(Ctx &c, AlphaSegs *segs = nullptr);
 int alpha_query(Ctx &c, double alpha, double q, bool by_quantile);
 int master_list(Ctx &c);
 int alpha_from_host_mesh(Ctx &c, const double *h_xy, int n, const gpudtTriangle *tris, int nt);
@@ -281,9 +339,17 @@ constexpr int kEmitThreads = 256;
 constexpr int kEmitTile = kEmitThreads;
 int launch_column_pass(Ctx &c, int W2);
 int launch_row_pass(Ctx &c);
-int launch_emit(Ctx &c, int ntiles, long long nwin, bool write);
+int launch_emit(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_out);
+int voronoi_global(Ctx &c);
+int emit_global(Ctx &c, int base);
 int launch_vd_tri(Ctx &c);
 int launch_vd_repair(Ctx &c, int nflag);
+int launch_vd_repair_cells(Ctx &c, int nflag, int T, int logT, int cells, const int16_t *ycol, const int *idmap,
+                           int *esc_cells);
+int launch_vd_tri_cells(Ctx &c, int T, int logT, int cells, const int16_t *ycol, const int *idmap, int2 *chunk,
+                        int *flagged);
+int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *occ, const uint32_t *bandocc,
+                             int16_t *ycol);
 // LSD radix sort of (keys, vals) ascending (sort.cu)
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n);
 int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);

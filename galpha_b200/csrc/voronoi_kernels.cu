@@ -19,6 +19,10 @@ __global__ void __launch_bounds__(256) k_column_pass(const uint32_t *__restrict_
                                                      const uint32_t *__restrict__ bandocc,
                                                      int16_t *__restrict__ ycol, int T, int W2)
 {
+    // blockIdx.z: texture cell of a batch (cells are stacked T x T textures)
+    occ += (size_t)blockIdx.z * T * (T >> 5);
+    bandocc += (size_t)blockIdx.z * T * W2;
+    ycol += (size_t)blockIdx.z * T * T;
     int x = blockIdx.x * 32 + threadIdx.x;
     int b = blockIdx.y * blockDim.y + threadIdx.y;
     int nb = T >> 6;
@@ -401,7 +405,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri(const int16_t *__restr
                                                           int2 *__restrict__ chunk, int *__restrict__ flagged,
                                                           int T, int logT, int cap, Counters *ct)
 {
-    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    // blockIdx.z: texture cell of a batch; tiles are numbered over all cells
+    const int tile = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    ycol += (size_t)blockIdx.z << (2 * logT);
+    idmap += (size_t)blockIdx.z << (2 * logT);
     __shared__ unsigned col[KT_CH][KT_CW];
     __shared__ int tile_island;
     const int x0 = blockIdx.x * KT_W, y0 = blockIdx.y * KT_H;
@@ -514,12 +521,16 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
                                                                  const int *__restrict__ idmap,
                                                                  int4 *__restrict__ tv, const int *__restrict__ tiles,
                                                                  const int *__restrict__ freelist, int tiles_x, int T,
-                                                                 int logT, int cap, Counters *ct)
+                                                                 int logT, int cap, int *esc_cells, Counters *ct)
 {
     __shared__ unsigned col[KS_H][KS_W];
     __shared__ unsigned nxt[KS_H][KS_W];
     __shared__ int changed, pending;
-    const int tile = tiles[blockIdx.x];
+    const int gtile = tiles[blockIdx.x];
+    const int tiles_y = (T - 1 + KT_H - 1) / KT_H;
+    const int cell = gtile / (tiles_x * tiles_y), tile = gtile - cell * tiles_x * tiles_y;
+    ycol += (size_t)cell << (2 * logT);
+    idmap += (size_t)cell << (2 * logT);
     const int x0 = (tile % tiles_x) * KT_W, y0 = (tile / tiles_x) * KT_H;
     const int gx = x0 - KS_M, gy = y0 - KS_M;  // pixel of col[0][0]
     const unsigned NONE = 0xffffffffu, ISL = 0xfffffffeu;
@@ -590,7 +601,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         }
         for (int k = threadIdx.x; k < (KT_H + 1) * (KT_W + 1); k += kFusedThreads) {
             int ly = k / (KT_W + 1) + KS_M, lx = k % (KT_W + 1) + KS_M;
-            if (nxt[ly][lx] == 1u) ct->escalate = 1;
+            if (nxt[ly][lx] == 1u) {
+                ct->escalate = 1;
+                if (esc_cells) esc_cells[cell] = 1;
+            }
         }
         __syncthreads();
     }
@@ -684,11 +698,12 @@ __global__ void k_redo_mark(const int *flagged, int nflag, unsigned char *redo, 
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nflag) return;
-    int t = flagged[i], tx = t % tiles_x, ty = t / tiles_x;
+    const int per = tiles_x * tiles_y;
+    int g = flagged[i], cell = g / per, t = g - cell * per, tx = t % tiles_x, ty = t / tiles_x;
     for (int dy = -1; dy <= 1; dy++)
         for (int dx = -1; dx <= 1; dx++) {
             int x = tx + dx, y = ty + dy;
-            if (x >= 0 && y >= 0 && x < tiles_x && y < tiles_y) redo[y * tiles_x + x] = 1;
+            if (x >= 0 && y >= 0 && x < tiles_x && y < tiles_y) redo[(size_t)cell * per + y * tiles_x + x] = 1;
         }
 }
 
@@ -712,9 +727,14 @@ __global__ void k_clamp_free(Counters *ct)
 
 int launch_vd_repair(Ctx &c, int nflag)
 {
-    const int T = c.T;
+    return launch_vd_repair_cells(c, nflag, c.T, c.logT, 1, c.ycol, c.idmap, nullptr);
+}
+
+int launch_vd_repair_cells(Ctx &c, int nflag, int T, int logT, int cells, const int16_t *ycol, const int *idmap,
+                           int *esc_cells)
+{
     int tiles_x = (T - 1 + KT_W - 1) / KT_W, tiles_y = (T - 1 + KT_H - 1) / KT_H;
-    int ntiles = tiles_x * tiles_y;
+    int ntiles = tiles_x * tiles_y * cells;
     unsigned char *redo = (unsigned char *)c.aux;
     GALPHA_CUDA(cudaMemsetAsync(redo, 0, (size_t)ntiles, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
@@ -726,8 +746,8 @@ int launch_vd_repair(Ctx &c, int nflag)
     int r = read_counters(c);
     if (r) return r;
     int nredo = c.hctr->nlist;
-    k_vd_tri_repair<<<nredo, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, c.list, c.freelist, tiles_x, T,
-                                                           c.logT, c.cap_tris, c.ctr);
+    k_vd_tri_repair<<<nredo, kFusedThreads, 0, c.stream>>>(ycol, idmap, c.tv, c.list, c.freelist, tiles_x, T, logT,
+                                                           c.cap_tris, esc_cells, c.ctr);
     count_launch();
     k_clamp_free<<<1, 1, 0, c.stream>>>(c.ctr);
     count_launch();
@@ -737,11 +757,16 @@ int launch_vd_repair(Ctx &c, int nflag)
 
 int launch_vd_tri(Ctx &c)
 {
-    const int T = c.T;
-    dim3 grid((T - 1 + KT_W - 1) / KT_W, (T - 1 + KT_H - 1) / KT_H);
+    return launch_vd_tri_cells(c, c.T, c.logT, 1, c.ycol, c.idmap, (int2 *)c.colour, c.list2);
+}
+
+// Tiles of all cells, numbered cell-major; chunk / flagged use that numbering.
+int launch_vd_tri_cells(Ctx &c, int T, int logT, int cells, const int16_t *ycol, const int *idmap, int2 *chunk,
+                        int *flagged)
+{
+    dim3 grid((T - 1 + KT_W - 1) / KT_W, (T - 1 + KT_H - 1) / KT_H, cells);
     kev_record(c, 0);
-    k_vd_tri<<<grid, kFusedThreads, 0, c.stream>>>(c.ycol, c.idmap, c.tv, (int2 *)c.colour, c.list2, T, c.logT,
-                                                    c.cap_tris, c.ctr);
+    k_vd_tri<<<grid, kFusedThreads, 0, c.stream>>>(ycol, idmap, c.tv, chunk, flagged, T, logT, c.cap_tris, c.ctr);
     count_launch();
     kev_record(c, 1);
     GALPHA_CUDA(cudaGetLastError());
@@ -751,10 +776,15 @@ int launch_vd_tri(Ctx &c)
 // ---------------------------------------------------------------- launchers
 int launch_column_pass(Ctx &c, int W2)
 {
-    const int T = c.T;
-    dim3 block(32, 8), grid(T / 32, ((T >> 6) + 7) / 8);
+    return launch_column_pass_cells(c, c.T, W2, 1, c.occ, c.bandocc, c.ycol);
+}
+
+int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *occ, const uint32_t *bandocc,
+                             int16_t *ycol)
+{
+    dim3 block(32, 8), grid(T / 32, ((T >> 6) + 7) / 8, cells);
     kev_record(c, 2);
-    k_column_pass<<<grid, block, 0, c.stream>>>(c.occ, c.bandocc, c.ycol, T, W2);
+    k_column_pass<<<grid, block, 0, c.stream>>>(occ, bandocc, ycol, T, W2);
     kev_record(c, 3);
     count_launch();
     GALPHA_CUDA(cudaGetLastError());
@@ -778,13 +808,13 @@ int launch_row_pass(Ctx &c)
     return GPUDT_OK;
 }
 
-int launch_emit(Ctx &c, int ntiles, long long nwin, bool write)
+int launch_emit(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_out)
 {
     kev_record(c, write ? 6 : 4);
     if (!write)
         k_emit_count<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.T, c.logT, nwin, c.ctr);
     else
-        k_emit_write<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.tv, c.T, c.logT, nwin);
+        k_emit_write<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, tv_out, c.T, c.logT, nwin);
     count_launch();
     kev_record(c, write ? 7 : 5);
     GALPHA_CUDA(cudaGetLastError());

@@ -108,6 +108,37 @@ int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap);
 
 void galphaReleaseOutput(GAlphaOutput *out);
 
+/* ------------------------------------------------------------ batches
+ * Many independent point sets in one pipeline run (no reference
+ * counterpart: the reference computes one set per gpudtComputeDT /
+ * Alpha_Shapes_2D call).  Set s has setSizes[s] points, stored after the
+ * points of sets 0..s-1 in one interleaved xy array, and the bounds
+ * bounds[4s .. 4s+3] = minX, minY, maxX, maxY (the GPUDTPARAMS fields, which
+ * must contain every point of the set).  Each set's result is exactly what a
+ * separate galphaRunDevice call gives (the texture size is chosen per set);
+ * the results are stored set after set: */
+typedef struct {
+    int nPoints, pointBase;  /* point_list rows of the set */
+    int nTris, triBase;      /* triangles and tri_list rows of the set */
+    int nEdges, edgeBase;    /* edge_list rows of the set */
+    int nSpectrum, specBase; /* spectrum values of the set, [specBase] = 0 (its rank 0) */
+} galphaBatchSet;
+
+/* d_xy: device memory.  withAlpha: 0 DT only, 1 DT + alpha. */
+int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double *d_xy, const double *bounds,
+                   int withAlpha, gpudtStatus *st);
+/* The same from host memory (copied to the device inside the call). */
+int galphaRunBatchHost(galphaHandle h, int nSets, const int *setSizes, const double *xy, const double *bounds,
+                       int withAlpha, gpudtStatus *st);
+/* Per-set counts and bases of the last batch (host array of nSets). */
+int galphaBatchSets(galphaHandle h, galphaBatchSet *sets);
+/* Copy the last batch's results to host buffers sized by galphaBatchSets
+ * (any pointer may be NULL).  Vertex, triangle and neighbour indices are local
+ * to each set, as a per-set gpudtComputeDT would return them; ranks are per
+ * set; spectrum holds every set's spectrum at its specBase. */
+int galphaBatchCopy(galphaHandle h, gpudtTriangle *tris, galphaPointInterval *points,
+                    galphaEdgeInterval *edges, int *triRanks, double *spectrum);
+
 /* Alpha (headers.h:80-86): one master-list entry.  st: 0 edge, 1 triangle,
  * 2 vertex (simplex_type); at: 0 ro, 1 nu_min, 2 nu_max (alpha_type). */
 typedef struct {

@@ -62,3 +62,20 @@ def classify_intervals(res, alpha):
     ec = interval(ro, ed["nu_min_rank"], ed["nu_max_rank"])
     tc = np.where(tr["ro_rank"] <= R, 3, 0).astype(np.uint8)
     return pc, ec, tc, R
+
+
+def canonical_alpha(vtx, res):
+    """Order-free view of an alpha result: triangle -> ro, edge -> (ro, nu_min,
+    nu_max) keyed by sorted vertex pair, plus the spectrum and point_list as
+    they are (both independent of triangle order)."""
+    vtx = np.asarray(vtx)
+    tri = {}
+    for t, r in zip(vtx.tolist(), res["tri_list"]["ro_rank"].tolist()):
+        k = t.index(min(t))
+        tri[tuple(t[k:] + t[:k])] = r
+    edge = {}
+    for E in res["edge_list"]:
+        t, i = int(E["tIndex"]), int(E["vOpp"])
+        a, b = int(vtx[t][(i + 1) % 3]), int(vtx[t][(i + 2) % 3])
+        edge[(min(a, b), max(a, b))] = (int(E["ro_rank"]), int(E["nu_min_rank"]), int(E["nu_max_rank"]))
+    return np.asarray(res["spectrum"]), tri, edge, np.asarray(res["point_list"])

@@ -1,0 +1,101 @@
+"""GPU tests of the batched pipeline (galphaRunBatch): every set's result
+equals a separate single-set run of the same points -- identical triangle set,
+spectrum, per-simplex ranks and intervals (order-free comparison, since the
+triangle order depends on the texture size) -- and, for inputs in general
+position, the oracle's Delaunay triangulation."""
+import numpy as np
+import pytest
+
+import galpha_b200 as G
+from galpha_b200 import datasets as D
+from alphacheck import canonical_alpha
+from dtcheck import canon_set
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_sets(seed):
+    rng = np.random.default_rng(seed)
+    sets = []
+    for k, n in enumerate([64, 100, 700, 3000, 9000, 25000, 200, 1500]):
+        sets.append(rng.random((n, 2)) * (1 + k))
+    r = np.sqrt(rng.random(2000)); a = 2 * np.pi * rng.random(2000)
+    sets.append(np.stack([r * np.cos(a), r * np.sin(a)], 1))                      # disk
+    r = np.sqrt(0.64 + 0.36 * rng.random(3000)); a = 2 * np.pi * rng.random(3000)
+    sets.append(np.stack([r * np.cos(a), r * np.sin(a)], 1) + 5.0)                # annulus
+    c = rng.random((6, 2)); sets.append(c[rng.integers(0, 6, 4000)] + rng.normal(0, 0.01, (4000, 2)))
+    lat = np.floor(rng.random((2500, 2)) * 24) / 24; sets.append(lat)             # lattice + duplicates
+    sets.append(np.stack([np.linspace(0, 1, 50), np.linspace(0, 2, 50)], 1))     # collinear
+    sets.append(np.array([[0.5, 0.5], [0.25, 0.75]]))                             # two points
+    sets.append(np.zeros((0, 2)))                                                 # empty
+    sets.append(np.repeat([[0.3, 0.3]], 10, axis=0))                              # one distinct point
+    sets.append(np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]))                   # one triangle
+    return sets
+
+
+def _single(engine, pts):
+    fbo = 256
+    while fbo < 4096 and fbo * fbo < 16 * len(pts):
+        fbo *= 2
+    dt = engine.triangulate(G.GPUDTParams(pts, fboSize=fbo))
+    return dt, engine.alpha_resident()
+
+
+def _compare(engine, sets, results):
+    for k, (pts, res) in enumerate(zip(sets, results)):
+        dt, ref = _single(engine, pts)
+        assert canon_set(res["triangles"]["vtx"]) == canon_set(dt.vtx), "set %d triangles" % k
+        # neighbour links are consistent and set-local
+        tri = res["triangles"]["tri"]
+        for t in range(len(tri)):
+            for i in range(3):
+                nb = tri[t][i]
+                if nb >= 0:
+                    assert tri[nb >> 2][nb & 3] == (t << 2) | i, "set %d links" % k
+        s1, t1, e1, p1 = canonical_alpha(res["triangles"]["vtx"], res)
+        s2, t2, e2, p2 = canonical_alpha(dt.vtx, ref)
+        np.testing.assert_array_equal(s1, s2, err_msg="set %d spectrum" % k)
+        assert t1 == t2, "set %d triangle ranks" % k
+        assert e1 == e2, "set %d edge intervals" % k
+        np.testing.assert_array_equal(p1, p2, err_msg="set %d point intervals" % k)
+
+
+def test_batch_matches_single_runs(engine):
+    sets = _mixed_sets(1)
+    beng = G.Engine()
+    try:
+        beng.run_batch(sets)
+        res = beng.batch_results()
+    finally:
+        beng.close()
+    assert len(res) == len(sets)
+    _compare(engine, sets, res)
+
+
+def test_batch_reuse_and_oracle(engine):
+    beng = G.Engine()
+    try:
+        a = _mixed_sets(2)[:6]
+        beng.run_batch(a)
+        beng.run_batch(a[::-1])          # a second batch on the same handle
+        res = beng.batch_results()
+    finally:
+        beng.close()
+    for pts, r in zip(a[::-1], res):
+        v, nb, _ = O.dt(pts)
+        assert canon_set(r["triangles"]["vtx"]) == canon_set(v)
+
+
+def test_batch_c4_sample(engine):
+    sets = D.c4_sets()[:48]
+    beng = G.Engine()
+    try:
+        st = beng.run_batch(sets)
+        res = beng.batch_results()
+    finally:
+        beng.close()
+    for pts, r in zip(sets, res):
+        v, nb, _ = O.dt(pts)
+        assert canon_set(r["triangles"]["vtx"]) == canon_set(v)
+        assert r["spectrum"][0] == 0.0 and np.all(np.diff(r["spectrum"]) > 0)
