@@ -163,6 +163,7 @@ def load(path=None):
     L.galphaRunBatchHost.argtypes = [vp, ip, vp, vp, vp, ip, ctypes.POINTER(Status)]
     L.galphaBatchSets.argtypes = [vp, vp]
     L.galphaBatchCopy.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.galphaBatchQuery.argtypes = [vp, vp, ip, vp]
     L.galphaMasterList.argtypes = [vp, ctypes.POINTER(_MasterOut)]
     L.galphaReleaseMasterList.argtypes = [ctypes.POINTER(_MasterOut)]
     L.galphaLastError.restype = ctypes.c_char_p
@@ -287,6 +288,7 @@ class Engine:
 
         With copy=False the triangle array is a view of a reused pinned buffer,
         valid until the next call on this engine."""
+        self._batch_active = False
         cp = params._c()
         cap = 2 * params.nPoints + 64
         buf = self._pool.get("tri", cap, TRIANGLE_DTYPE)
@@ -333,6 +335,7 @@ class Engine:
 
     def alpha_of(self, params, dt, copy=True):
         """Alpha spectrum + intervals of a given triangulation (Alpha_Shapes_2D(pInput, pDT))."""
+        self._batch_active = False
         cp = params._c()
         tri = np.ascontiguousarray(dt.triangles)
         o = _Output()
@@ -346,6 +349,7 @@ class Engine:
 
     def run_device(self, d_xy_ptr, n, bounds, fbo_size, with_alpha=True):
         """Hot path on device-resident points (d_xy_ptr: device address of 2n doubles)."""
+        self._batch_active = False
         st = Status()
         _check(self._L.galphaRunDevice(self._h, ctypes.c_void_p(d_xy_ptr), n, bounds[0], bounds[1], bounds[2],
                                        bounds[3], fbo_size, 1 if with_alpha else 0, ctypes.byref(st)),
@@ -389,6 +393,7 @@ class Engine:
                                           b.ctypes.data, 1 if with_alpha else 0, ctypes.byref(st)),
                "galphaRunBatchHost")
         self._batch = (len(sets), bool(with_alpha))
+        self._batch_active = True
         return st
 
     def run_batch_device(self, d_xy_ptr, sizes, bounds, with_alpha=True):
@@ -399,6 +404,7 @@ class Engine:
         _check(self._L.galphaRunBatch(self._h, len(sizes), sizes.ctypes.data, ctypes.c_void_p(d_xy_ptr),
                                       b.ctypes.data, 1 if with_alpha else 0, ctypes.byref(st)), "galphaRunBatch")
         self._batch = (len(sizes), bool(with_alpha))
+        self._batch_active = True
         return st
 
     def batch_sets(self):
@@ -435,6 +441,15 @@ class Engine:
             out.append(d)
         return out
 
+    def batch_query(self, values, by_quantile=False):
+        """Alpha-complex query on every set of the last batch (galphaBatchQuery):
+        values[s] is set s's alpha (or spectrum quantile).  Returns QueryResults."""
+        k = self._batch[0]
+        vals = np.ascontiguousarray(np.broadcast_to(np.asarray(values, dtype=np.float64), (k,)))
+        res = (QueryResult * k)()
+        _check(self._L.galphaBatchQuery(self._h, vals.ctypes.data, 1 if by_quantile else 0, res), "galphaBatchQuery")
+        return res
+
     def master_list(self):
         """master_list (ALPHA_DTYPE array) and spec_pointers of the resident alpha
         result (Alpha_Shapes_2D::compute_master_list)."""
@@ -454,7 +469,10 @@ class Engine:
     def classes(self):
         """Classes of the last query: (points, edges, triangles) uint8 arrays."""
         nt, ne, _ = self.counts()
-        pt = np.empty(self._npoints, np.uint8)
+        npts = self._npoints
+        if getattr(self, "_batch_active", False):
+            npts = sum(s.nPoints for s in self.batch_sets())
+        pt = np.empty(npts, np.uint8)
         ed = np.empty(ne, np.uint8)
         tr = np.empty(nt, np.uint8)
         _check(self._L.galphaCopyClasses(self._h, pt.ctypes.data if len(pt) else None,

@@ -685,7 +685,96 @@ struct QueryClassify {
     }
 };
 
+// Per set of a batch: the set's spectrum is spectrum[spec_off[s] + s ..] of
+// length nd[s] + 1 (its own rank-0 sentinel first).
+struct QueryRankSets {
+    const double *spectrum;
+    const int *spec_off, *nd;
+    const double *param;
+    int by_quantile;
+    int *R;
+    double *alpha;
+    __device__ void operator()(long long ss) const
+    {
+        int s = (int)ss;
+        const double *sp = spectrum + spec_off[s] + s;
+        int ns = nd[s] + 1;
+        double a = param[s];
+        if (by_quantile) {
+            double qq = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
+            a = sp[(int)llrint(qq * (double)(ns - 1))];
+        }
+        int r = -1;
+        if (a >= 0.0) {
+            int lo = 0, hi = ns - 1;
+            while (lo < hi) {
+                int mid = lo + (hi - lo + 1) / 2;
+                if (sp[mid] <= a) lo = mid;
+                else hi = mid - 1;
+            }
+            r = lo;
+        }
+        R[s] = r;
+        alpha[s] = a;
+    }
+};
+
+struct QueryClassifySets {
+    const int2 *pt;
+    const int *edge_ro;
+    const int2 *edge_nu;
+    const int4 *edges;
+    const int *tri_ro;
+    const int *vset, *tset, *R;
+    uint8_t *cls;
+    int *counts;  // [K][12]
+    int N, nE, nT;
+    __device__ void operator()(long long ii) const
+    {
+        int i = (int)ii;
+        int type, k, s;
+        if (i < N) {
+            type = 0;
+            s = vset[i];
+            int r = R[s];
+            int2 v = pt[i];
+            k = (v.x < 0 || r < 0) ? 0 : interval_class(0, v.x, v.y, r);
+        } else if (i < N + nE) {
+            type = 1;
+            int e = i - N;
+            s = tset[edges[e].z];
+            int r = R[s];
+            int ro = edge_ro[e];
+            int2 nu = edge_nu[e];
+            k = r < 0 ? 0 : interval_class(ro != 0 ? ro : -1, nu.x, nu.y, r);
+        } else {
+            type = 2;
+            int t = i - N - nE;
+            s = tset[t];
+            int r = R[s];
+            k = (r >= 0 && tri_ro[t] <= r) ? 3 : 0;
+        }
+        cls[i] = (uint8_t)k;
+        int bin = s * 12 + type * 4 + k;
+        unsigned peers = __match_any_sync(__activemask(), bin);
+        if ((peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(&counts[bin], __popc(peers));
+    }
+};
+
 }  // namespace
+
+int alpha_query_sets(Ctx &c, int K, const int *vset, const int *tset, const int *spec_off, const int *nd,
+                     const double *param, int by_quantile, int *R, double *alpha, int *counts)
+{
+    GALPHA_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * 12 * (size_t)K, c.stream));
+    launch_n(c, QueryRankSets{c.spectrum, spec_off, nd, param, by_quantile, R, alpha}, K);
+    long long n = (long long)c.N + c.nE + c.nT_out;
+    launch_n(c, QueryClassifySets{c.pt_nu, c.edge_ro, c.edge_nu, c.edges, c.tri_ro, vset, tset, R, c.qclass, counts,
+                                  c.N, c.nE, c.nT_out},
+             n);
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
+}
 
 int alpha_query(Ctx &c, double alpha, double q, bool by_quantile)
 {

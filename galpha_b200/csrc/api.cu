@@ -859,6 +859,42 @@ int galphaBatchCopy(galphaHandle h, gpudtTriangle *tris, galphaPointInterval *po
     return GPUDT_OK;
 }
 
+int galphaBatchQuery(galphaHandle h, const double *values, int byQuantile, galphaQueryResult *res)
+{
+    if (!h || !values || !res) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    BatchHost &bh = h->H.bh;
+    BatchDev &B = h->H.bd;
+    Ctx &c = h->H.c;
+    if (!bh.valid || !bh.alpha) {
+        g_err = "galphaBatchQuery: no batched alpha result on this handle";
+        return GPUDT_ERR_ARG;
+    }
+    cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
+    const int K = bh.K;
+    GALPHA_CUDA(cudaMemcpyAsync(B.qparam, values, sizeof(double) * (size_t)K, cudaMemcpyHostToDevice, c.stream));
+    int r = alpha_query_sets(c, K, B.vsetall, B.tset, B.spec_off, B.nd, B.qparam, byQuantile ? 1 : 0, B.qR, B.qalpha,
+                             B.qcounts);
+    if (r) return r;
+    std::vector<int> R(K), cnt(12 * (size_t)K);
+    std::vector<double> a(K);
+    GALPHA_CUDA(cudaMemcpyAsync(R.data(), B.qR, sizeof(int) * (size_t)K, cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaMemcpyAsync(a.data(), B.qalpha, sizeof(double) * (size_t)K, cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaMemcpyAsync(cnt.data(), B.qcounts, sizeof(int) * 12 * (size_t)K, cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    for (int s2 = 0; s2 < K; s2++) {
+        res[s2].alpha = a[s2];
+        res[s2].rank = R[s2];
+        for (int k = 0; k < 4; k++) {
+            res[s2].nPoints[k] = cnt[12 * (size_t)s2 + k];
+            res[s2].nEdges[k] = cnt[12 * (size_t)s2 + 4 + k];
+            res[s2].nTris[k] = cnt[12 * (size_t)s2 + 8 + k];
+        }
+    }
+    return GPUDT_OK;
+}
+
 static const int kMinusOneHost = -1;
 
 int galphaMasterList(galphaHandle h, GAlphaMasterList *out)

@@ -220,6 +220,24 @@ struct KillSetTris {
     }
 };
 
+// Before the links exist the triangle list is plain vertex triples, so the
+// slots released by KillSetTris are reclaimed by compacting the list.
+struct AliveFlag {
+    const int4 *tv;
+    int *flag;
+    __device__ void operator()(long long t) const { flag[t] = tv[t].x >= 0 ? 1 : 0; }
+};
+
+struct ScatterAlive {
+    const int4 *tv;
+    const int *flag, *pos;
+    int4 *out;
+    __device__ void operator()(long long t) const
+    {
+        if (flag[t]) out[pos[t]] = tv[t];
+    }
+};
+
 // ------------------------------------------------------- grouped compaction
 struct AliveBySet {
     const int4 *tv;
@@ -317,7 +335,8 @@ int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec)
     size_t need = al(sizeof(SetDesc) * (size_t)K) + 2 * al(4 * (size_t)(K + 1)) + al(4 * (size_t)N + 4) +
                   al(4 * (size_t)V + 4) + 3 * al(4 * (size_t)(K + 1)) + al(4 * (size_t)cap + 4) +
                   al(4 * (size_t)(K + 1)) + al(4 * (size_t)nspec + 4) + 3 * al(4 * (size_t)(K + 1)) +
-                  al(sizeof(gpudtTriangle) * (size_t)cap);
+                  al(sizeof(gpudtTriangle) * (size_t)cap) + 2 * al(8 * (size_t)(K + 1)) + al(4 * (size_t)(K + 1)) +
+                  al(48 * (size_t)(K + 1));
     if (need > B.bytes) {
         if (B.buf) cudaFree(B.buf);
         B.buf = nullptr;
@@ -346,6 +365,10 @@ int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec)
     B.nd = (int *)take(4 * (size_t)(K + 1));
     B.spec_off = (int *)take(4 * (size_t)(K + 1));
     B.otri = (gpudtTriangle *)take(sizeof(gpudtTriangle) * (size_t)cap);
+    B.qparam = (double *)take(8 * (size_t)(K + 1));
+    B.qalpha = (double *)take(8 * (size_t)(K + 1));
+    B.qR = (int *)take(4 * (size_t)(K + 1));
+    B.qcounts = (int *)take(48 * (size_t)(K + 1));
     (void)c;
     return GPUDT_OK;
 }
@@ -534,7 +557,19 @@ int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh)
                                     c.stream));
         r = read_counters(c);
         if (r) return r;
-        launch_n(c, KillSetTris{c.tv, B.vsetall, B.offline, c.freelist, c.ctr}, c.hctr->ntris);
+        {
+            const int nt = c.hctr->ntris;
+            launch_n(c, KillSetTris{c.tv, B.vsetall, B.offline, c.freelist, c.ctr}, nt);
+            launch_n(c, AliveFlag{c.tv, c.aux}, nt);
+            r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->ntris);
+            if (r) return r;
+            launch_n(c, ScatterAlive{c.tv, c.aux, c.aux2, c.tn}, nt);
+            r = read_counters(c);
+            if (r) return r;
+            GALPHA_CUDA(cudaMemcpyAsync(c.tv, c.tn, sizeof(int4) * (size_t)c.hctr->ntris, cudaMemcpyDeviceToDevice,
+                                        c.stream));
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nfree, 0, sizeof(int), c.stream));
+        }
         const int16_t *ycol0 = c.ycol;
         int *idmap0 = c.idmap;
         for (int z = 0; z < C.cells; z++) {

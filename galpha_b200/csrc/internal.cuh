@@ -308,6 +308,8 @@ struct BatchDev {
         *offline = nullptr, *esc = nullptr, *tset = nullptr, *tbase = nullptr, *seg = nullptr,
         *firstexcl = nullptr, *nd = nullptr, *spec_off = nullptr;
     gpudtTriangle *otri = nullptr;  // [cap] set-local output triangles
+    double *qparam = nullptr, *qalpha = nullptr;  // [K] per-set query values
+    int *qR = nullptr, *qcounts = nullptr;        // [K], [12 K]
 };
 
 void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale, double &sx, double &sy);
@@ -331,6 +333,8 @@ struct AlphaSegs {
 };
 int stage_alpha(Ctx &c, AlphaSegs *segs = nullptr);
 int alpha_query(Ctx &c, double alpha, double q, bool by_quantile);
+int alpha_query_sets(Ctx &c, int K, const int *vset, const int *tset, const int *spec_off, const int *nd,
+                     const double *param, int by_quantile, int *R, double *alpha, int *counts);
 int master_list(Ctx &c);
 int alpha_from_host_mesh(Ctx &c, const double *h_xy, int n, const gpudtTriangle *tris, int nt);
 

@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
 {
     __shared__ unsigned col[KS_H][KS_W];
     __shared__ unsigned nxt[KS_H][KS_W];
-    __shared__ int changed, pending;
+    __shared__ int changed, pending, bad;
     const int gtile = tiles[blockIdx.x];
     const int tiles_y = (T - 1 + KT_H - 1) / KT_H;
     const int cell = gtile / (tiles_x * tiles_y), tile = gtile - cell * tiles_x * tiles_y;
@@ -644,7 +644,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         __syncthreads();
         if (!pending) break;
     }
-    // emit the tile's windows
+    // emit the tile's windows; a recolouring that leaves a window without a
+    // consistent dual (an unresolved island, or three colours not in
+    // counterclockwise order) sends the texture to the envelope path instead
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
     int n = 0;
     unsigned tri[2 * (KT_H * KT_W / kFusedThreads)][3];
     for (int k = threadIdx.x; k < KT_H * KT_W; k += kFusedThreads) {
@@ -654,7 +658,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         int py = ly + KS_M, px = lx + KS_M;
         unsigned c[4] = {col[py][px], col[py][px + 1], col[py + 1][px + 1], col[py + 1][px]};
         if (c[0] >= ISL || c[1] >= ISL || c[2] >= ISL || c[3] >= ISL) {
-            set_err(ct, GPUDT_ERR_TOPOLOGY, 15);
+            bad = 1;
             continue;
         }
         if (c[0] == c[2] || c[1] == c[3]) continue;
@@ -663,19 +667,26 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         for (int q = 0; q < 4; q++)
             if (c[q] != c[(q + 3) & 3]) L[m++] = c[q];
         if (m == 3) {
-            if (orient_pk(L[0], L[1], L[2]) <= 0) set_err(ct, GPUDT_ERR_TOPOLOGY, 16);
+            if (orient_pk(L[0], L[1], L[2]) <= 0) bad = 1;
             tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
         } else if (m == 4) {
             if (orient_pk(L[0], L[1], L[2]) > 0 && orient_pk(L[0], L[2], L[3]) > 0) {
                 tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
                 tri[n][0] = L[0]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
             } else {
-                if (orient_pk(L[1], L[2], L[3]) <= 0 || orient_pk(L[1], L[3], L[0]) <= 0)
-                    set_err(ct, GPUDT_ERR_TOPOLOGY, 17);
+                if (orient_pk(L[1], L[2], L[3]) <= 0 || orient_pk(L[1], L[3], L[0]) <= 0) bad = 1;
                 tri[n][0] = L[1]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
                 tri[n][0] = L[1]; tri[n][1] = L[3]; tri[n][2] = L[0]; n++;
             }
         }
+    }
+    __syncthreads();
+    if (bad) {
+        if (threadIdx.x == 0) {
+            ct->escalate = 1;
+            if (esc_cells) esc_cells[cell] = 1;
+        }
+        return;
     }
     for (int q = 0; q < n; q++) {
         // reuse the slots released by the redo set first, then the tail

@@ -1,0 +1,121 @@
+"""Request loop for DT + alpha-spectrum requests (the serving form of the engine).
+
+Requests arrive over time, each a point set followed by alpha queries at
+spectrum quantiles.  The loop admits every request that has arrived into one
+micro-batch, bounded by an estimate of its device-memory footprint, runs the
+batch through one batched pipeline pass (``Engine.run_batch``: DT + spectrum
+of every set at once), answers the queries on the meshes while they are still
+resident (``Engine.batch_query``, all sets at once per query), and records each
+request's latency from its arrival to the end of its batch.
+
+The reference has no serving path: it computes one set per
+gpudtComputeDT / Alpha_Shapes_2D call on the default stream.
+"""
+import collections
+import time
+
+import numpy as np
+
+# Device bytes per point of a batched run with alpha: texture cells (about 10
+# to 40 pixels per point at 10 B per pixel), triangle slots (2 per vertex with
+# their links, free lists and relink records) and the alpha arrays.
+BYTES_PER_POINT = 2048
+
+
+class Request:
+    __slots__ = ("rid", "arrival", "points", "quantiles", "start", "done", "results")
+
+    def __init__(self, rid, arrival, points, quantiles=(0.1, 0.5, 0.9)):
+        self.rid = rid
+        self.arrival = float(arrival)
+        self.points = points
+        self.quantiles = tuple(quantiles)
+        self.start = None
+        self.done = None
+        self.results = None
+
+    @property
+    def latency(self):
+        return None if self.done is None else self.done - self.arrival
+
+
+def poisson_arrivals(rate, duration, seed):
+    """Arrival times of a Poisson stream (rate per second) over [0, duration)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            return np.array(out)
+        out.append(t)
+
+
+class Server:
+    """Micro-batching request loop on one engine (one device).
+
+    hbm_budget: device bytes the batches may use (admission control);
+    max_batch_points: an additional cap that bounds the latency of a batch.
+    """
+
+    def __init__(self, engine, hbm_budget=120e9, max_batch_points=1 << 25, bytes_per_point=BYTES_PER_POINT):
+        self.engine = engine
+        self.max_points = int(min(max_batch_points, hbm_budget // bytes_per_point))
+        self.batches = []
+
+    def _admit(self, queue):
+        batch, pts = [], 0
+        while queue:
+            n = len(queue[0].points)
+            if batch and pts + n > self.max_points:
+                break
+            batch.append(queue.popleft())
+            pts += n
+        return batch, pts
+
+    def run(self, requests, clock=time.perf_counter, sleep=time.sleep):
+        """Serve requests (sorted by arrival, times in seconds from the start of
+        the run) in real time; returns them with start/done/results filled."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        queue = collections.deque()
+        t0 = clock()
+        while pending or queue:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+            if not queue:
+                sleep(max(0.0, pending[0].arrival - now))
+                continue
+            batch, pts = self._admit(queue)
+            start = clock() - t0
+            self.engine.run_batch([r.points for r in batch])
+            nq = max(len(r.quantiles) for r in batch)
+            answers = []
+            for k in range(nq):
+                qs = [r.quantiles[k] if k < len(r.quantiles) else r.quantiles[-1] for r in batch]
+                answers.append(self.engine.batch_query(qs, by_quantile=True))
+            done = clock() - t0
+            for i, r in enumerate(batch):
+                r.start = start
+                r.done = done
+                r.results = [answers[k][i] for k in range(len(r.quantiles))]
+            self.batches.append((start, done, len(batch), pts))
+        return requests
+
+
+def summary(requests, batches=None):
+    """p50 / p99 latency (ms), served requests and points per second."""
+    lat = np.array([r.latency for r in requests if r.latency is not None])
+    pts = sum(len(r.points) for r in requests if r.done is not None)
+    span = max(r.done for r in requests) - min(r.arrival for r in requests) if len(lat) else 0.0
+    out = {
+        "requests": int(len(lat)),
+        "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
+        "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
+        "mean_ms": float(lat.mean() * 1e3) if len(lat) else None,
+        "requests_per_s": float(len(lat) / span) if span > 0 else None,
+        "mpoints_per_s": float(pts / span / 1e6) if span > 0 else None,
+    }
+    if batches:
+        out["batches"] = len(batches)
+        out["mean_batch_requests"] = float(np.mean([b[2] for b in batches]))
+    return out

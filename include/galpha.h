@@ -202,6 +202,12 @@ int galphaQueryQuantile(galphaHandle h, double q, galphaQueryResult *res);
 int galphaCopyClasses(galphaHandle h, unsigned char *pointClass, unsigned char *edgeClass,
                       unsigned char *triClass);
 
+/* Alpha-complex query (as galphaQuery) on every set of the last batch at
+ * once: values[s] is set s's alpha, or its spectrum quantile when byQuantile
+ * is set; res[s] receives set s's counts.  The per-simplex classes, in batch
+ * order, are then available through galphaCopyClasses. */
+int galphaBatchQuery(galphaHandle h, const double *values, int byQuantile, galphaQueryResult *res);
+
 /* Edge numbering of a triangle-neighbour mesh that is already in device
  * memory, for callers that cannot allocate: a serving or rendering loop that
  * has reserved its device memory up front and cannot give any to a library

@@ -99,3 +99,32 @@ def test_batch_c4_sample(engine):
         v, nb, _ = O.dt(pts)
         assert canon_set(r["triangles"]["vtx"]) == canon_set(v)
         assert r["spectrum"][0] == 0.0 and np.all(np.diff(r["spectrum"]) > 0)
+
+
+def test_batch_query_matches_interval_rule(engine):
+    from alphacheck import classify_intervals
+
+    sets = _mixed_sets(3)[:10] + _mixed_sets(3)[-4:]
+    beng = G.Engine()
+    try:
+        beng.run_batch(sets)
+        res = beng.batch_results()
+        info = beng.batch_sets()
+        rng = np.random.default_rng(0)
+        for mode, vals in (("q", [0.1] * len(sets)), ("q", [0.9] * len(sets)),
+                           ("q", rng.random(len(sets)).tolist()),
+                           ("a", [float(r["spectrum"][len(r["spectrum"]) // 2]) for r in res])):
+            qr = beng.batch_query(vals, by_quantile=(mode == "q"))
+            pc, ec, tc = beng.classes()
+            for k, r in enumerate(res):
+                wp, we, wt, R = classify_intervals(r, qr[k].alpha)
+                assert qr[k].rank == R, k
+                si = info[k]
+                np.testing.assert_array_equal(pc[si.pointBase:si.pointBase + si.nPoints], wp)
+                np.testing.assert_array_equal(ec[si.edgeBase:si.edgeBase + si.nEdges], we)
+                np.testing.assert_array_equal(tc[si.triBase:si.triBase + si.nTris], wt)
+                assert list(qr[k].nTris) == np.bincount(wt, minlength=4).tolist()
+                assert list(qr[k].nEdges) == np.bincount(we, minlength=4).tolist()
+                assert list(qr[k].nPoints) == np.bincount(wp, minlength=4).tolist()
+    finally:
+        beng.close()
