@@ -14,6 +14,13 @@ triangulation + alpha spectrum with per-simplex intervals.
 Between timed steps a 512 MiB buffer is written (L2 flush); the step's own
 working set (~3.5 GB) is far larger than L2 as well.
 
+Two more legs share the JSON line (rank 0, N = 1):
+  batched  c4: 4096 independent sets in one batched pipeline run
+           (galphaRunBatch), against plain per-set galphaRunDevice calls on
+           a sample, plus end to end through galphaRunBatchHost.
+  serving  c5: a Poisson request stream served by micro-batches with
+           quantile alpha queries on the resident meshes; p50 / p99 latency.
+
 Multi-GPU: a single DT does not shard (the flip, insertion and sort stages are
 global), so N GPUs run N independent replicas of the workload ("replicas
 only", weak scaling); value = all points triangulated / max time over ranks.
@@ -47,6 +54,8 @@ def parse():
     ap.add_argument("--n", type=int, default=None, help="override the point count")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched (c4) and serving (c5) legs")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving leg")
     return ap.parse_args()
 
 
@@ -154,6 +163,113 @@ def reference_arm(a):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- batched / serving
+def batched_leg(G, D, torch, stream, reps=3):
+    """c4: 4096 independent sets (sizes log-uniform in [64, 65536], unit
+    square / disk / annulus) in one batched pipeline run, against the plain
+    per-set calls (galphaRunDevice per set, texture size per set as a user of
+    the reference picks fboSize) on every 16th set."""
+    import numpy as np
+
+    sets = D.c4_sets()
+    sizes = np.array([len(p) for p in sets], np.int32)
+    xy = np.ascontiguousarray(np.concatenate(sets))
+    bounds = G.Engine.batch_bounds(sets)
+    d_xy = torch.from_numpy(xy).cuda()
+    eng = G.Engine()
+    eng.set_stream(stream.cuda_stream)
+    L = G.load()
+    st = eng.run_batch_device(d_xy.data_ptr(), sizes, bounds)  # warm-up (arena growth)
+    torch.cuda.synchronize()
+    ts = []
+    l0 = L.galphaLaunchCount()
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = eng.run_batch_device(d_xy.data_ptr(), sizes, bounds)
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    launches = (L.galphaLaunchCount() - l0) // reps
+    ms = sum(ts) / len(ts)
+    # end to end: host points in, every set's triangles and alpha arrays out
+    te = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        eng.run_batch(sets, bounds=bounds)
+        res = eng.batch_results()
+        te.append((time.perf_counter() - t0) * 1e3)
+    d2h = sum(r["triangles"].nbytes + r["spectrum"].nbytes + r["point_list"].nbytes + r["edge_list"].nbytes
+              + r["tri_list"].nbytes for r in res)
+    # plain per-set calls on a sample
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    sample = list(range(0, len(sets), 16))
+    npts = int(sum(sizes[k] for k in sample))
+    for k in sample[:4]:
+        fbo = 256
+        while fbo < 8192 and fbo * fbo < 16 * sizes[k]:
+            fbo *= 2
+        eng.run_device(d_xy.data_ptr() + 16 * int(off[k]), int(sizes[k]), tuple(bounds[k]), fbo, True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in sample:
+        fbo = 256
+        while fbo < 8192 and fbo * fbo < 16 * sizes[k]:
+            fbo *= 2
+        eng.run_device(d_xy.data_ptr() + 16 * int(off[k]), int(sizes[k]), tuple(bounds[k]), fbo, True)
+    e1.record(stream)
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    eng.close()
+    n = int(sizes.sum())
+    value = n / (ms / 1e3) / 1e6
+    plain = npts / (plain_ms / 1e3) / 1e6
+    return {
+        "config": {"workload": "c4: %d sets, sizes log-uniform in [64, 65536], unit square / disk / annulus, FP64, "
+                               "DT + alpha spectrum + intervals per set" % len(sets), "points": n},
+        "value": value, "unit": UNIT, "ms_per_batch": ms, "gpu_launches": int(launches),
+        "plain_per_set": {"value": plain, "unit": UNIT, "sets": len(sample), "points": npts, "ms": plain_ms},
+        "speedup_vs_plain": value / plain,
+        "e2e": {"value": n / (min(te) / 1e3) / 1e6, "unit": UNIT, "ms": min(te), "h2d_bytes": int(xy.nbytes),
+                "d2h_bytes": int(d2h)},
+        "stages_ms": {nm: float(st.ms[i]) for i, nm in enumerate(
+            ["upload", "voronoi", "triangles", "shift", "missing", "boundary", "flip", "compact", "alpha"])},
+        "stats": {k: getattr(st, k) for k in ("nVerts", "nMissing", "nRepairTiles", "nEscalated", "nFlips",
+                                              "flipRounds", "exactOrient", "exactIncircle")},
+    }
+
+
+def serving_leg(G, D, seconds, rate=2000.0):
+    """c5: Poisson requests (rate per s) over `seconds`, sizes log-uniform in
+    [1000, 1048576], half uniform and half Gaussian clusters (the c3 blob
+    recipe), each followed by alpha queries at spectrum quantiles 0.1 / 0.5 /
+    0.9 on its resident mesh; micro-batches admitted under a 120 GB budget."""
+    import numpy as np
+    from galpha_b200 import serving as S
+
+    rng = np.random.default_rng(55)
+    pool = []
+    for k in range(96):
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(1048576))))
+        pool.append(D.uniform_points(n, 5000 + k) if k % 2 == 0 else D.gaussian_blobs(n, 5000 + k))
+    arrivals = S.poisson_arrivals(rate, seconds, 77)
+    pick = rng.integers(0, len(pool), len(arrivals))
+    eng = G.Engine()
+    warm = [S.Request(i, 0.0, pool[i]) for i in range(8)]
+    S.Server(eng).run(warm)
+    reqs = [S.Request(i, t, pool[pick[i]]) for i, t in enumerate(arrivals)]
+    srv = S.Server(eng, hbm_budget=120e9)
+    srv.run(reqs)
+    eng.close()
+    out = S.summary(reqs, srv.batches)
+    out["config"] = {"workload": "c5: Poisson %.0f req/s for %.1f s (of the 60 s stream), sizes log-uniform in "
+                                 "[1000, 1048576], 50/50 uniform / Gaussian clusters, 3 quantile queries per request, "
+                                 "120 GB admission budget" % (rate, seconds), "pool_sets": len(pool)}
+    out["offered_mpoints_per_s"] = float(sum(len(r.points) for r in reqs) / seconds / 1e6)
+    return out
+
+
 # ------------------------------------------------------------ GPU arm
 def main():
     a = parse()
@@ -214,6 +330,7 @@ def main():
         stages.append(list(st.ms))
         kernels.append(list(st.kernelMs))
         stats = {k: getattr(st, k) for k in ("nVerts", "nFake", "nDuplicates", "nMissing", "nBadShift", "nIslandPixels",
+                                             "nRepairTiles", "nEscalated",
                                              "nFlips", "flipRounds", "shiftRounds", "missingRounds", "exactOrient",
                                              "exactIncircle", "filteredIncircle")}
     torch.cuda.synchronize()
@@ -288,6 +405,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_baseline()
+    batched = serving = None
+    if rank == 0 and world == 1 and not a.no_batch:
+        batched = batched_leg(G, D, torch, stream)
+        serving = serving_leg(G, D, a.serve_seconds)
 
     if rank == 0:
         line = {
@@ -307,6 +428,8 @@ def main():
                            "emit": sum(k[2] for k in kernels) / len(kernels)},
             "counts": {"triangles": nt, "edges": ne, "spectrum": ns},
             "pipeline_stats": stats,
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     eng.close()

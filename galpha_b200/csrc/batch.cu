@@ -535,7 +535,7 @@ int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh)
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
         int nflag = c.hctr->nisland;
-        c.st.nIslandPixels += nflag;
+        c.st.nRepairTiles += nflag;
         if (nflag == 0) continue;
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->escalate, 0, sizeof(int), c.stream));
         GALPHA_CUDA(cudaMemsetAsync(B.esc, 0, sizeof(int) * (size_t)C.cells, c.stream));
@@ -552,7 +552,10 @@ int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh)
                                     c.stream));
         GALPHA_CUDA(cudaStreamSynchronize(c.stream));
         for (int z = 0; z < C.cells; z++)
-            if (esc[z]) setesc[C.sets[z]] = 1;
+            if (esc[z]) {
+                setesc[C.sets[z]] = 1;
+                c.st.nEscalated++;
+            }
         GALPHA_CUDA(cudaMemcpyAsync(B.offline, setesc.data(), sizeof(int) * (size_t)bh.K, cudaMemcpyHostToDevice,
                                     c.stream));
         r = read_counters(c);

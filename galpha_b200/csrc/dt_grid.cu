@@ -370,7 +370,7 @@ int stage_voronoi(Ctx &c)
         if (r0) return r0;
         if (c.hctr->err) return c.hctr->err;
         int nflag = c.hctr->nisland;
-        c.st.nIslandPixels = nflag;  // tiles with island pixels, repaired locally
+        c.st.nRepairTiles = nflag;
         bool local_ok = true;
         if (nflag > 0) {
             GALPHA_CUDA(cudaMemsetAsync(&c.ctr->escalate, 0, sizeof(int), c.stream));
@@ -386,6 +386,7 @@ int stage_voronoi(Ctx &c)
             return GPUDT_OK;
         }
         // an island component too large for a local repair: global path
+        c.st.nEscalated = 1;
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, 2 * sizeof(int), c.stream));  // ntris, nfree
     }
     return voronoi_global(c);

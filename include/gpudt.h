@@ -75,11 +75,13 @@ typedef struct {
     int nDuplicates;         /* exact duplicates dropped */
     int nMissing;            /* sites inserted by point location */
     int nBadShift;           /* sites that could not be shifted (removed, re-inserted) */
-    int nIslandPixels;       /* discrete-Voronoi island pixels recoloured */
+    int nIslandPixels;       /* island pixels recoloured on the envelope (global) path */
     int nFlips;              /* Lawson flips performed */
     int flipRounds;          /* flip rounds */
     int shiftRounds;         /* shifting rounds */
     int missingRounds;       /* insertion rounds */
+    int nRepairTiles;        /* fused-path tiles with islands, repaired locally */
+    int nEscalated;          /* textures (point sets) redone on the envelope path */
     long long exactOrient;   /* orientation tests that needed exact arithmetic */
     long long exactIncircle; /* in-circle tests that needed exact arithmetic */
     long long filteredIncircle; /* in-circle tests decided by the FP64 filter */
