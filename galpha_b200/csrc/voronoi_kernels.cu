@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
 {
     __shared__ unsigned col[KS_H][KS_W];
     __shared__ unsigned nxt[KS_H][KS_W];
-    __shared__ int changed, pending, bad;
+
     const int gtile = tiles[blockIdx.x];
     const int tiles_y = (T - 1 + KT_H - 1) / KT_H;
     const int cell = gtile / (tiles_x * tiles_y), tile = gtile - cell * tiles_x * tiles_y;
@@ -542,9 +542,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
     __syncthreads();
     // mark island components: a pixel whose toward-site neighbours (all inside
     // the region) carry neither its colour is marked; repeat
+    // (the round flags are block-wide reductions, __syncthreads_or, so every
+    // thread leaves a loop after the same round)
     for (int round = 0; round < KS_M; round++) {
-        if (threadIdx.x == 0) changed = 0;
-        __syncthreads();
+        int mine = 0;
         for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
             int ly = k / KS_W, lx = k - ly * KS_W;
             unsigned c = col[ly][lx];
@@ -558,7 +559,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
                       (dx != 0 && dy != 0 && col[ly + dy][lx + dx] == c);
             if (!ok) {
                 nxt[ly][lx] = ISL;
-                changed = 1;
+                mine = 1;
             }
         }
         __syncthreads();
@@ -566,8 +567,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
             int ly = k / KS_W, lx = k - ly * KS_W;
             col[ly][lx] = nxt[ly][lx];
         }
-        __syncthreads();
-        if (!changed) break;
+        if (!__syncthreads_or(mine)) break;
     }
     // components that reach the region border may extend past the redo set:
     // flood the island pixels from the border zone; if one of the tile's own
@@ -580,8 +580,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         }
         __syncthreads();
         for (int round = 0; round < KS_W + KS_H; round++) {
-            if (threadIdx.x == 0) changed = 0;
-            __syncthreads();
+            int mine = 0;
             for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
                 int ly = k / KS_W, lx = k - ly * KS_W;
                 if (col[ly][lx] != ISL || nxt[ly][lx]) continue;
@@ -593,11 +592,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
                     }
                 if (hit) {
                     nxt[ly][lx] = 1u;
-                    changed = 1;
+                    mine = 1;
                 }
             }
-            __syncthreads();
-            if (!changed) break;
+            if (!__syncthreads_or(mine)) break;
         }
         for (int k = threadIdx.x; k < (KT_H + 1) * (KT_W + 1); k += kFusedThreads) {
             int ly = k / (KT_W + 1) + KS_M, lx = k % (KT_W + 1) + KS_M;
@@ -610,8 +608,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
     }
     // recolour
     for (int round = 0; round < 4 * KS_M; round++) {
-        if (threadIdx.x == 0) pending = 0;
-        __syncthreads();
+        int mine = 0;
         for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
             int ly = k / KS_W, lx = k - ly * KS_W;
             unsigned c = col[ly][lx];
@@ -634,21 +631,19 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
                     }
                 }
             nxt[ly][lx] = bc;
-            if (bc == ISL) pending = 1;
+            if (bc == ISL) mine = 1;
         }
         __syncthreads();
         for (int k = threadIdx.x; k < KS_H * KS_W; k += kFusedThreads) {
             int ly = k / KS_W, lx = k - ly * KS_W;
             col[ly][lx] = nxt[ly][lx];
         }
-        __syncthreads();
-        if (!pending) break;
+        if (!__syncthreads_or(mine)) break;
     }
     // emit the tile's windows; a recolouring that leaves a window without a
     // consistent dual (an unresolved island, or three colours not in
     // counterclockwise order) sends the texture to the envelope path instead
-    if (threadIdx.x == 0) bad = 0;
-    __syncthreads();
+    int mybad = 0;
     int n = 0;
     unsigned tri[2 * (KT_H * KT_W / kFusedThreads)][3];
     for (int k = threadIdx.x; k < KT_H * KT_W; k += kFusedThreads) {
@@ -658,7 +653,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         int py = ly + KS_M, px = lx + KS_M;
         unsigned c[4] = {col[py][px], col[py][px + 1], col[py + 1][px + 1], col[py + 1][px]};
         if (c[0] >= ISL || c[1] >= ISL || c[2] >= ISL || c[3] >= ISL) {
-            bad = 1;
+            mybad = 1;
             continue;
         }
         if (c[0] == c[2] || c[1] == c[3]) continue;
@@ -667,21 +662,20 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
         for (int q = 0; q < 4; q++)
             if (c[q] != c[(q + 3) & 3]) L[m++] = c[q];
         if (m == 3) {
-            if (orient_pk(L[0], L[1], L[2]) <= 0) bad = 1;
+            if (orient_pk(L[0], L[1], L[2]) <= 0) mybad = 1;
             tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
         } else if (m == 4) {
             if (orient_pk(L[0], L[1], L[2]) > 0 && orient_pk(L[0], L[2], L[3]) > 0) {
                 tri[n][0] = L[0]; tri[n][1] = L[1]; tri[n][2] = L[2]; n++;
                 tri[n][0] = L[0]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
             } else {
-                if (orient_pk(L[1], L[2], L[3]) <= 0 || orient_pk(L[1], L[3], L[0]) <= 0) bad = 1;
+                if (orient_pk(L[1], L[2], L[3]) <= 0 || orient_pk(L[1], L[3], L[0]) <= 0) mybad = 1;
                 tri[n][0] = L[1]; tri[n][1] = L[2]; tri[n][2] = L[3]; n++;
                 tri[n][0] = L[1]; tri[n][1] = L[3]; tri[n][2] = L[0]; n++;
             }
         }
     }
-    __syncthreads();
-    if (bad) {
+    if (__syncthreads_or(mybad)) {
         if (threadIdx.x == 0) {
             ct->escalate = 1;
             if (esc_cells) esc_cells[cell] = 1;
