@@ -70,7 +70,7 @@ class Status(ctypes.Structure):
         ("nDuplicates", ctypes.c_int), ("nMissing", ctypes.c_int), ("nBadShift", ctypes.c_int),
         ("nIslandPixels", ctypes.c_int), ("nFlips", ctypes.c_int), ("flipRounds", ctypes.c_int),
         ("shiftRounds", ctypes.c_int), ("missingRounds", ctypes.c_int),
-        ("nRepairTiles", ctypes.c_int), ("nEscalated", ctypes.c_int),
+        ("nRepairTiles", ctypes.c_int), ("nEscalated", ctypes.c_int), ("nEnvelopeCells", ctypes.c_int),
         ("exactOrient", ctypes.c_longlong), ("exactIncircle", ctypes.c_longlong),
         ("filteredIncircle", ctypes.c_longlong),
         ("ms", ctypes.c_float * 12),

@@ -283,10 +283,11 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     z.lists = std::max(z.cap * 3, z.V + 1);
     int Tmax = 128;
     for (auto &C : bh.classes) Tmax = std::max(Tmax, C.T);
-    z.ntiles = std::max<size_t>(((size_t)(Tmax - 1) * (Tmax - 1) + 255) / 256 + 1, (size_t)bh.ntiles + 1);
+    z.ntiles = std::max<size_t>(((size_t)(Tmax - 1) * (Tmax - 1) + 255) / 256 + 1,
+                                (size_t)bh.T2 / 256 + bh.K + 1);  // envelope emission tiles of all cells
     r = ensure_sizes(H, z);
     if (r) return r;
-    r = batch_buffers(c, H.bd, K, bh.N, (int)z.V, c.cap_tris, 3 * c.cap_tris + 8);
+    r = batch_buffers(c, H.bd, K, bh.N, (int)z.V, c.cap_tris, 3 * c.cap_tris + 8, bh.ntiles);
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
     for (int k = 0; k < 8; k++) c.kev_rec[k] = false;

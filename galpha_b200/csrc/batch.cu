@@ -329,14 +329,14 @@ struct LocalEdges {
 
 }  // namespace
 
-int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec)
+int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, int ntiles)
 {
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t need = al(sizeof(SetDesc) * (size_t)K) + 2 * al(4 * (size_t)(K + 1)) + al(4 * (size_t)N + 4) +
                   al(4 * (size_t)V + 4) + 3 * al(4 * (size_t)(K + 1)) + al(4 * (size_t)cap + 4) +
                   al(4 * (size_t)(K + 1)) + al(4 * (size_t)nspec + 4) + 3 * al(4 * (size_t)(K + 1)) +
                   al(sizeof(gpudtTriangle) * (size_t)cap) + 2 * al(8 * (size_t)(K + 1)) + al(4 * (size_t)(K + 1)) +
-                  al(48 * (size_t)(K + 1));
+                  al(48 * (size_t)(K + 1)) + al(4 * (size_t)(K + 1)) + al(8 * (size_t)(ntiles + 1));
     if (need > B.bytes) {
         if (B.buf) cudaFree(B.buf);
         B.buf = nullptr;
@@ -369,6 +369,8 @@ int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec)
     B.qalpha = (double *)take(8 * (size_t)(K + 1));
     B.qR = (int *)take(4 * (size_t)(K + 1));
     B.qcounts = (int *)take(48 * (size_t)(K + 1));
+    B.cellmap = (int *)take(4 * (size_t)(K + 1));
+    B.chunk = (int2 *)take(8 * (size_t)(ntiles + 1));
     (void)c;
     return GPUDT_OK;
 }
@@ -516,83 +518,104 @@ int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy)
     return c.hctr->err;
 }
 
-// Colouring + dual triangles, one launch per cell size.  A set whose island
-// repair cannot stay local is redone alone on the envelope path.
+// Colouring + dual triangles, per cell size.  Cells whose interior is mostly
+// empty (holes, gaps between clusters) make the window scan of the fused
+// kernel long and its islands frequent; they take the envelope path
+// (per-row lower envelope, cost independent of emptiness).  So does a cell
+// whose island repair cannot stay local.
 int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh)
 {
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, 2 * sizeof(int), c.stream));  // ntris, nfree
+    int *const colour0 = c.colour;
+    int16_t *const ycol0 = c.ycol;
+    int *const idmap0 = c.idmap;
     for (auto &C : bh.classes) {
-        int live = 0;
-        for (int s : C.sets) live += bh.sets[s].live;
-        if (!live) continue;
+        std::vector<int> fused, env;  // launch lists of cell indices within the class
+        std::vector<int> occ(C.cells, 0);
         int r = launch_column_pass_cells(c, C.T, C.W2, C.cells, c.occ + C.occw, c.bandocc + C.band, c.ycol + C.tex);
         if (r) return r;
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nisland, 0, sizeof(int), c.stream));
-        r = launch_vd_tri_cells(c, C.T, C.logT, C.cells, c.ycol + C.tex, c.idmap + C.tex, (int2 *)c.colour,
-                                c.list2);
+        r = cell_occupancy(c, c.bandocc + C.band, C.T, C.W2, C.cells, B.esc, occ.data());
         if (r) return r;
-        r = read_counters(c);
-        if (r) return r;
-        if (c.hctr->err) return c.hctr->err;
-        int nflag = c.hctr->nisland;
-        c.st.nRepairTiles += nflag;
-        if (nflag == 0) continue;
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->escalate, 0, sizeof(int), c.stream));
-        GALPHA_CUDA(cudaMemsetAsync(B.esc, 0, sizeof(int) * (size_t)C.cells, c.stream));
-        r = launch_vd_repair_cells(c, nflag, C.T, C.logT, C.cells, c.ycol + C.tex, c.idmap + C.tex, B.esc);
-        if (r) return r;
-        r = read_counters(c);
-        if (r) return r;
-        if (c.hctr->err) return c.hctr->err;
-        if (!c.hctr->escalate) continue;
-        // sets whose islands reach past the repair margin: drop their
-        // triangles and colour their cells alone on the envelope path
-        std::vector<int> esc(C.cells), setesc(bh.K, 0);
-        GALPHA_CUDA(cudaMemcpyAsync(esc.data(), B.esc, sizeof(int) * (size_t)C.cells, cudaMemcpyDeviceToHost,
-                                    c.stream));
-        GALPHA_CUDA(cudaStreamSynchronize(c.stream));
-        for (int z = 0; z < C.cells; z++)
-            if (esc[z]) {
-                setesc[C.sets[z]] = 1;
-                c.st.nEscalated++;
-            }
-        GALPHA_CUDA(cudaMemcpyAsync(B.offline, setesc.data(), sizeof(int) * (size_t)bh.K, cudaMemcpyHostToDevice,
-                                    c.stream));
-        r = read_counters(c);
-        if (r) return r;
-        {
-            const int nt = c.hctr->ntris;
-            launch_n(c, KillSetTris{c.tv, B.vsetall, B.offline, c.freelist, c.ctr}, nt);
-            launch_n(c, AliveFlag{c.tv, c.aux}, nt);
-            r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->ntris);
+        for (int z = 0; z < C.cells; z++) {
+            const SetDesc &S = bh.sets[C.sets[z]];
+            if (!S.live) continue;
+            const double D = S.T - 2 * kMargin;
+            const bool dense = (double)S.n * 256.0 >= D * D;
+            const bool filled = occupancy_ok(C.T, occ[z]);
+            (dense && filled ? fused : env).push_back(z);
+        }
+        if (!fused.empty()) {
+            const int nf = (int)fused.size();
+            GALPHA_CUDA(cudaMemcpyAsync(B.cellmap, fused.data(), sizeof(int) * (size_t)nf, cudaMemcpyHostToDevice,
+                                        c.stream));
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nisland, 0, sizeof(int), c.stream));
+            r = launch_vd_tri_cells(c, C.T, C.logT, nf, c.ycol + C.tex, c.idmap + C.tex, B.chunk, c.list2, B.cellmap);
             if (r) return r;
-            launch_n(c, ScatterAlive{c.tv, c.aux, c.aux2, c.tn}, nt);
             r = read_counters(c);
             if (r) return r;
-            GALPHA_CUDA(cudaMemcpyAsync(c.tv, c.tn, sizeof(int4) * (size_t)c.hctr->ntris, cudaMemcpyDeviceToDevice,
-                                        c.stream));
-            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nfree, 0, sizeof(int), c.stream));
+            if (c.hctr->err) return c.hctr->err;
+            const int nflag = c.hctr->nisland;
+            c.st.nRepairTiles += nflag;
+            if (nflag > 0) {
+                GALPHA_CUDA(cudaMemsetAsync(&c.ctr->escalate, 0, sizeof(int), c.stream));
+                GALPHA_CUDA(cudaMemsetAsync(B.esc, 0, sizeof(int) * (size_t)nf, c.stream));
+                r = launch_vd_repair_cells(c, nflag, C.T, C.logT, nf, c.ycol + C.tex, c.idmap + C.tex, B.esc,
+                                           B.cellmap, B.chunk);
+                if (r) return r;
+                r = read_counters(c);
+                if (r) return r;
+                if (c.hctr->err) return c.hctr->err;
+                if (c.hctr->escalate) {
+                    // drop the escalated cells' triangles, reclaim their slots,
+                    // and colour those cells on the envelope path below
+                    std::vector<int> esc(nf), setesc(bh.K, 0);
+                    GALPHA_CUDA(cudaMemcpyAsync(esc.data(), B.esc, sizeof(int) * (size_t)nf, cudaMemcpyDeviceToHost,
+                                                c.stream));
+                    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+                    for (int k = 0; k < nf; k++)
+                        if (esc[k]) {
+                            setesc[C.sets[fused[k]]] = 1;
+                            env.push_back(fused[k]);
+                            c.st.nEscalated++;
+                        }
+                    GALPHA_CUDA(cudaMemcpyAsync(B.offline, setesc.data(), sizeof(int) * (size_t)bh.K,
+                                                cudaMemcpyHostToDevice, c.stream));
+                    const int nt = c.hctr->ntris;
+                    launch_n(c, KillSetTris{c.tv, B.vsetall, B.offline, c.freelist, c.ctr}, nt);
+                    launch_n(c, AliveFlag{c.tv, c.aux}, nt);
+                    r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->ntris);
+                    if (r) return r;
+                    launch_n(c, ScatterAlive{c.tv, c.aux, c.aux2, c.tn}, nt);
+                    r = read_counters(c);
+                    if (r) return r;
+                    GALPHA_CUDA(cudaMemcpyAsync(c.tv, c.tn, sizeof(int4) * (size_t)c.hctr->ntris,
+                                                cudaMemcpyDeviceToDevice, c.stream));
+                    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nfree, 0, sizeof(int), c.stream));
+                }
+            }
         }
-        const int16_t *ycol0 = c.ycol;
-        int *idmap0 = c.idmap;
-        for (int z = 0; z < C.cells; z++) {
-            if (!esc[z]) continue;
-            const SetDesc &S = bh.sets[C.sets[z]];
-            c.T = S.T;
-            c.logT = S.logT;
-            c.ycol = const_cast<int16_t *>(ycol0) + S.tex;
-            c.idmap = idmap0 + S.tex;
-            r = voronoi_global(c);
+        if (!env.empty()) {
+            const int ne = (int)env.size();
+            GALPHA_CUDA(cudaMemcpyAsync(B.cellmap, env.data(), sizeof(int) * (size_t)ne, cudaMemcpyHostToDevice,
+                                        c.stream));
+            c.T = C.T;
+            c.logT = C.logT;
+            c.ycol = ycol0 + C.tex;
+            c.idmap = idmap0 + C.tex;
+            c.colour = colour0 + C.tex;
+            r = voronoi_global(c, ne, B.cellmap);
             if (!r) {
                 r = read_counters(c);
-                if (!r) r = emit_global(c, c.hctr->ntris);
+                if (!r) r = emit_global(c, c.hctr->ntris, ne, B.cellmap);
             }
-            c.ycol = const_cast<int16_t *>(ycol0);
+            c.ycol = ycol0;
             c.idmap = idmap0;
+            c.colour = colour0;
+            c.T = 0;
+            c.logT = 0;
             if (r) return r;
+            c.st.nEnvelopeCells += ne;
         }
-        c.T = 0;
-        c.logT = 0;
     }
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;

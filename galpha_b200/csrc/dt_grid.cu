@@ -164,18 +164,24 @@ __device__ __forceinline__ bool isolated(const int *colour, const short2 *gpix, 
     return true;
 }
 
+// Pixel indices of the island lists are cell-major over a stack of T x T
+// cells: p = (cell << 2 logT) + (y << logT) + x (cell 0 for a single texture).
 struct IslandDetectAll {
     const int *colour;
     const short2 *gpix;
     int *list;
     Counters *ct;
     int T, logT, cap;
+    const int *cellmap;  // launch cell -> texture cell (nullptr: identity)
     __device__ void operator()(long long i) const
     {
-        int x = (int)(i & (T - 1)), y = (int)(i >> logT);
-        if (isolated(colour, gpix, T, logT, x, y)) {
+        const int z = (int)(i >> (2 * logT));
+        const long long local = i & (((long long)1 << (2 * logT)) - 1);
+        const long long cell = cellmap ? cellmap[z] : z;
+        int x = (int)(local & (T - 1)), y = (int)(local >> logT);
+        if (isolated(colour + (cell << (2 * logT)), gpix, T, logT, x, y)) {
             int k = atomicAdd(&ct->nlist, 1);
-            if (k < cap) list[k] = (int)i;
+            if (k < cap) list[k] = (int)((cell << (2 * logT)) + local);
             else set_err(ct, GPUDT_ERR_NOMEM, 1);
         }
     }
@@ -198,15 +204,17 @@ struct IslandDetectNear {
     __device__ void operator()(long long i) const
     {
         int p = list[from + i];
-        int x = p & (T - 1), y = p >> logT;
+        const int cell = p >> (2 * logT), local = p & ((1 << (2 * logT)) - 1);
+        const int *col = colour + ((size_t)cell << (2 * logT));
+        int x = local & (T - 1), y = local >> logT;
         for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
                 int xx = x + dx, yy = y + dy;
                 if ((dx == 0 && dy == 0) || xx < 0 || yy < 0 || xx >= T || yy >= T) continue;
-                if (isolated(colour, gpix, T, logT, xx, yy)) {
+                if (isolated(col, gpix, T, logT, xx, yy)) {
                     // a pixel next to several new islands is listed once per
                     // neighbour; the set (not the multiplicity) is what matters
-                    int q = (yy << logT) + xx;
+                    int q = (cell << (2 * logT)) + (yy << logT) + xx;
                     int k = atomicAdd(&ct->nlist, 1);
                     if (k < cap) list[k] = q;
                     else set_err(ct, GPUDT_ERR_NOMEM, 2);
@@ -231,14 +239,16 @@ struct IslandPropose {
             cand[i] = colour[p];
             return;
         }
-        int x = p & (T - 1), y = p >> logT;
+        const int cell = p >> (2 * logT), local = p & ((1 << (2 * logT)) - 1);
+        const int *col = colour + ((size_t)cell << (2 * logT));
+        int x = local & (T - 1), y = local >> logT;
         long long best = -1;
         int bestc = -1;
         for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
                 int xx = x + dx, yy = y + dy;
                 if ((dx == 0 && dy == 0) || xx < 0 || yy < 0 || xx >= T || yy >= T) continue;
-                int c = colour[((size_t)yy << logT) + xx];
+                int c = col[((size_t)yy << logT) + xx];
                 if (c < 0) continue;
                 short2 s = gpix[c];
                 long long d = (long long)(s.x - x) * (s.x - x) + (long long)(s.y - y) * (s.y - y);
@@ -303,6 +313,48 @@ int has_triangles(Ctx &c, const double *d_xy, int n)
     return c.hctr->changed > 0 ? 1 : 0;
 }
 
+// Occupied 64 x 64 blocks of each cell, counted away from the ring of fake
+// sites (interior blocks only) from the per-column band bitmaps.
+struct CellOccupancy {
+    const uint32_t *bandocc;
+    int T, W2, nb;  // nb = T / 64 blocks per side
+    int *count;     // [cells]
+    __device__ void operator()(long long i) const
+    {
+        const int inner = nb - 2;
+        const int z = (int)(i / ((long long)inner * inner));
+        const int rem = (int)(i - (long long)z * inner * inner);
+        const int bx = 1 + rem / inner, by = 1 + rem % inner;
+        const uint32_t *b = bandocc + (size_t)z * T * W2;
+        uint32_t any = 0;
+        for (int x = 64 * bx; x < 64 * bx + 64; x++) any |= b[(size_t)x * W2 + (by >> 5)];
+        if ((any >> (by & 31)) & 1u) atomicAdd(&count[z], 1);
+    }
+};
+
+// Interior-block occupancy of `cells` stacked T x T cells into host[cells]
+// (dev: cells ints of device scratch).
+int cell_occupancy(Ctx &c, const uint32_t *bandocc, int T, int W2, int cells, int *dev, int *host)
+{
+    const int nb = T / 64;
+    for (int z = 0; z < cells; z++) host[z] = 0;
+    if (nb <= 2) return GPUDT_OK;
+    GALPHA_CUDA(cudaMemsetAsync(dev, 0, sizeof(int) * (size_t)cells, c.stream));
+    launch_n(c, CellOccupancy{bandocc, T, W2, nb, dev}, (long long)cells * (nb - 2) * (nb - 2));
+    GALPHA_CUDA(cudaMemcpyAsync(host, dev, sizeof(int) * (size_t)cells, cudaMemcpyDeviceToHost, c.stream));
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    return GPUDT_OK;
+}
+
+// The fused path pays a window scan as long as the distance to the nearest
+// site, so it is used only when at least 60 % of the interior 64 x 64 blocks
+// hold a site.
+bool occupancy_ok(int T, int occupied)
+{
+    const int nb = T / 64;
+    return nb <= 2 || occupied >= 0.6 * (nb - 2) * (nb - 2);
+}
+
 // ------------------------------------------------------------------ stages
 int stage_setup(Ctx &c, const double *d_xy, int n, double minX, double minY, double maxX, double maxY, int T)
 {
@@ -361,7 +413,10 @@ int stage_voronoi(Ctx &c)
     // make the per-pixel window scan long, so they take the envelope path.
     c.fused_done = false;
     long long D = T - 2 * kMargin;
-    if ((long long)c.N * 256 >= D * D) {
+    int occupied = 0;
+    r0 = cell_occupancy(c, c.bandocc, T, W2, 1, c.aux, &occupied);
+    if (r0) return r0;
+    if ((long long)c.N * 256 >= D * D && occupancy_ok(T, occupied)) {
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, sizeof(int), c.stream));
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nisland, 0, sizeof(int), c.stream));
         r0 = launch_vd_tri(c);
@@ -389,22 +444,24 @@ int stage_voronoi(Ctx &c)
         c.st.nEscalated = 1;
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ntris, 0, 2 * sizeof(int), c.stream));  // ntris, nfree
     }
-    return voronoi_global(c);
+    c.st.nEnvelopeCells = 1;
+    return voronoi_global(c, 1, nullptr);
 }
 
-// Envelope colouring of the whole texture c.T x c.T at c.ycol / c.idmap into
-// c.colour, then the global island repair.
-int voronoi_global(Ctx &c)
+// Envelope colouring of `cells` textures of size c.T x c.T (cell cellmap[z],
+// or z, of the stack at c.ycol / c.idmap / c.colour), then the global island
+// repair over all of them.
+int voronoi_global(Ctx &c, int cells, const int *cellmap)
 {
     const int T = c.T;
-    int r0 = launch_row_pass(c);
+    int r0 = launch_row_pass_cells(c, cells, cellmap);
     if (r0) return r0;
     GALPHA_CUDA(cudaGetLastError());
     // islands
-    long long npix = (long long)T * T;
+    long long npix = (long long)T * T * cells;
     int cap = (int)std::min<long long>(npix, (long long)c.cap_tris * 3);
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-    launch_n(c, IslandDetectAll{c.colour, c.gpix, c.list, c.ctr, T, c.logT, cap}, npix);
+    launch_n(c, IslandDetectAll{c.colour, c.gpix, c.list, c.ctr, T, c.logT, cap, cellmap}, npix);
     int r = read_counters(c);
     if (r) return r;
     int total = c.hctr->nlist;
@@ -415,8 +472,7 @@ int voronoi_global(Ctx &c)
     while (from < to) {
         if (to > cap) return GPUDT_ERR_NOMEM;
         launch_n(c, IslandMark{c.colour, c.list, from}, to - from);
-        launch_n(c, IslandDetectNear{c.colour, c.gpix, c.list, c.ctr, T, c.logT, from, cap},
-                 to - from);
+        launch_n(c, IslandDetectNear{c.colour, c.gpix, c.list, c.ctr, T, c.logT, from, cap}, to - from);
         r = read_counters(c);
         if (r) return r;
         from = to;
@@ -438,22 +494,23 @@ int voronoi_global(Ctx &c)
     return GPUDT_OK;
 }
 
-// Dual triangles of c.colour appended at slot `base` (c.ctr->ntris = base + count).
-int emit_global(Ctx &c, int base)
+// Dual triangles of the coloured cells appended at slot `base`
+// (c.ctr->ntris = base + count).
+int emit_global(Ctx &c, int base, int cells, const int *cellmap)
 {
     const int T = c.T;
     long long nwin = (long long)(T - 1) * (T - 1);
     int ntiles = (int)((nwin + kEmitTile - 1) / kEmitTile);
-    int r0 = launch_emit(c, ntiles, nwin, false, nullptr);
+    int r0 = launch_emit_cells(c, ntiles, nwin, false, nullptr, cells, cellmap);
     if (r0) return r0;
-    int r = exclusive_scan_int(c, c.tilecount, c.tilecount, ntiles, &c.ctr->nlist2);
+    int r = exclusive_scan_int(c, c.tilecount, c.tilecount, ntiles * cells, &c.ctr->nlist2);
     if (r) return r;
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->err) return c.hctr->err;
     const int total = c.hctr->nlist2;
     if ((long long)base + total > c.cap_tris) return GPUDT_ERR_NOMEM;
-    r = launch_emit(c, ntiles, nwin, true, c.tv + base);
+    r = launch_emit_cells(c, ntiles, nwin, true, c.tv + base, cells, cellmap);
     if (r) return r;
     const int nt = base + total;
     GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->ntris, &nt, sizeof(int), cudaMemcpyHostToDevice, c.stream));
@@ -464,7 +521,7 @@ int emit_global(Ctx &c, int base)
 int stage_triangles(Ctx &c)
 {
     if (c.fused_done) return GPUDT_OK;  // emitted by the fused kernel
-    return emit_global(c, 0);
+    return emit_global(c, 0, 1, nullptr);
 }
 
 }  // namespace galpha

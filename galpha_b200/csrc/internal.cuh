@@ -310,12 +310,14 @@ struct BatchDev {
     gpudtTriangle *otri = nullptr;  // [cap] set-local output triangles
     double *qparam = nullptr, *qalpha = nullptr;  // [K] per-set query values
     int *qR = nullptr, *qcounts = nullptr;        // [K], [12 K]
+    int *cellmap = nullptr;                       // [K] launch cell -> cell of a class
+    int2 *chunk = nullptr;                        // [fused tiles] (first slot, count) per tile
 };
 
 void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale, double &sx, double &sy);
 void launch_compact_write(Ctx &c, const int *newidx, int nslots);
 int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds);
-int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec);
+int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, int ntiles);
 int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy);
 int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh);
 int batch_compact(Ctx &c, BatchDev &B, BatchHost &bh);
@@ -344,14 +346,18 @@ constexpr int kEmitTile = kEmitThreads;
 int launch_column_pass(Ctx &c, int W2);
 int launch_row_pass(Ctx &c);
 int launch_emit(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_out);
-int voronoi_global(Ctx &c);
-int emit_global(Ctx &c, int base);
+int voronoi_global(Ctx &c, int cells, const int *cellmap);
+int cell_occupancy(Ctx &c, const uint32_t *bandocc, int T, int W2, int cells, int *dev, int *host);
+bool occupancy_ok(int T, int occupied);
+int emit_global(Ctx &c, int base, int cells, const int *cellmap);
 int launch_vd_tri(Ctx &c);
 int launch_vd_repair(Ctx &c, int nflag);
 int launch_vd_repair_cells(Ctx &c, int nflag, int T, int logT, int cells, const int16_t *ycol, const int *idmap,
-                           int *esc_cells);
+                           int *esc_cells, const int *cellmap, const int2 *chunk);
 int launch_vd_tri_cells(Ctx &c, int T, int logT, int cells, const int16_t *ycol, const int *idmap, int2 *chunk,
-                        int *flagged);
+                        int *flagged, const int *cellmap);
+int launch_row_pass_cells(Ctx &c, int cells, const int *cellmap);
+int launch_emit_cells(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_out, int cells, const int *cellmap);
 int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *occ, const uint32_t *bandocc,
                              int16_t *ycol);
 // LSD radix sort of (keys, vals) ascending (sort.cu)

@@ -115,8 +115,16 @@ constexpr int16_t kDead = -2;  // nxt[] marker of an element popped from the env
 
 __global__ void __launch_bounds__(kRowThreads) k_row_pass(const int16_t *__restrict__ ycol,
                                                           const int *__restrict__ idmap,
-                                                          int *__restrict__ colour, int T, int logT)
+                                                          int *__restrict__ colour, int T, int logT,
+                                                          const int *__restrict__ cellmap)
 {
+    // blockIdx.y: texture cell (cellmap[z], or z) of a batch
+    {
+        const size_t off = (size_t)(cellmap ? cellmap[blockIdx.y] : blockIdx.y) << (2 * logT);
+        ycol += off;
+        idmap += off;
+        colour += off;
+    }
     extern __shared__ __align__(16) unsigned char smem[];
     int16_t *ys = (int16_t *)smem;       // [T]
     int16_t *nxt = ys + T;               // [T]
@@ -304,11 +312,15 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *total)
     return excl;
 }
 
+// Blocks are numbered cell-major: tiles_per_cell consecutive blocks per cell.
 __global__ void __launch_bounds__(kEmitThreads) k_emit_count(const int *__restrict__ colour,
                                                              const short2 *__restrict__ gpix, int *tilecount,
-                                                             int T, int logT, long long nwin, Counters *ct)
+                                                             int T, int logT, long long nwin, Counters *ct,
+                                                             const int *__restrict__ cellmap, int tiles_per_cell)
 {
-    long long w = (long long)blockIdx.x * kEmitThreads + threadIdx.x;
+    const int z = blockIdx.x / tiles_per_cell;
+    colour += (size_t)(cellmap ? cellmap[z] : z) << (2 * logT);
+    long long w = (long long)(blockIdx.x - z * tiles_per_cell) * kEmitThreads + threadIdx.x;
     int n = 0, bad = 0;
     if (w < nwin) {
         int x = (int)(w % (T - 1)), y = (int)(w / (T - 1));
@@ -324,9 +336,12 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit_count(const int *__restri
 __global__ void __launch_bounds__(kEmitThreads) k_emit_write(const int *__restrict__ colour,
                                                              const short2 *__restrict__ gpix,
                                                              const int *__restrict__ tileoff, int4 *tv, int T,
-                                                             int logT, long long nwin)
+                                                             int logT, long long nwin,
+                                                             const int *__restrict__ cellmap, int tiles_per_cell)
 {
-    long long w = (long long)blockIdx.x * kEmitThreads + threadIdx.x;
+    const int z = blockIdx.x / tiles_per_cell;
+    colour += (size_t)(cellmap ? cellmap[z] : z) << (2 * logT);
+    long long w = (long long)(blockIdx.x - z * tiles_per_cell) * kEmitThreads + threadIdx.x;
     int n = 0, bad = 0;
     int3 t[2];
     if (w < nwin) {
@@ -403,12 +418,17 @@ __device__ __forceinline__ long long orient_pk(unsigned a, unsigned b, unsigned 
 __global__ void __launch_bounds__(kFusedThreads) k_vd_tri(const int16_t *__restrict__ ycol,
                                                           const int *__restrict__ idmap, int4 *__restrict__ tv,
                                                           int2 *__restrict__ chunk, int *__restrict__ flagged,
-                                                          int T, int logT, int cap, Counters *ct)
+                                                          int T, int logT, int cap, Counters *ct,
+                                                          const int *__restrict__ cellmap)
 {
-    // blockIdx.z: texture cell of a batch; tiles are numbered over all cells
+    // blockIdx.z: texture cell (cellmap[z], or z) of a batch; tiles are
+    // numbered over the launched cells
     const int tile = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    ycol += (size_t)blockIdx.z << (2 * logT);
-    idmap += (size_t)blockIdx.z << (2 * logT);
+    {
+        const size_t off = (size_t)(cellmap ? cellmap[blockIdx.z] : blockIdx.z) << (2 * logT);
+        ycol += off;
+        idmap += off;
+    }
     __shared__ unsigned col[KT_CH][KT_CW];
     __shared__ int tile_island;
     const int x0 = blockIdx.x * KT_W, y0 = blockIdx.y * KT_H;
@@ -521,7 +541,8 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
                                                                  const int *__restrict__ idmap,
                                                                  int4 *__restrict__ tv, const int *__restrict__ tiles,
                                                                  const int *__restrict__ freelist, int tiles_x, int T,
-                                                                 int logT, int cap, int *esc_cells, Counters *ct)
+                                                                 int logT, int cap, int *esc_cells, Counters *ct,
+                                                                 const int *__restrict__ cellmap)
 {
     __shared__ unsigned col[KS_H][KS_W];
     __shared__ unsigned nxt[KS_H][KS_W];
@@ -529,8 +550,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_vd_tri_repair(const int16_t *
     const int gtile = tiles[blockIdx.x];
     const int tiles_y = (T - 1 + KT_H - 1) / KT_H;
     const int cell = gtile / (tiles_x * tiles_y), tile = gtile - cell * tiles_x * tiles_y;
-    ycol += (size_t)cell << (2 * logT);
-    idmap += (size_t)cell << (2 * logT);
+    {
+        const size_t off = (size_t)(cellmap ? cellmap[cell] : cell) << (2 * logT);
+        ycol += off;
+        idmap += off;
+    }
     const int x0 = (tile % tiles_x) * KT_W, y0 = (tile / tiles_x) * KT_H;
     const int gx = x0 - KS_M, gy = y0 - KS_M;  // pixel of col[0][0]
     const unsigned NONE = 0xffffffffu, ISL = 0xfffffffeu;
@@ -732,11 +756,11 @@ __global__ void k_clamp_free(Counters *ct)
 
 int launch_vd_repair(Ctx &c, int nflag)
 {
-    return launch_vd_repair_cells(c, nflag, c.T, c.logT, 1, c.ycol, c.idmap, nullptr);
+    return launch_vd_repair_cells(c, nflag, c.T, c.logT, 1, c.ycol, c.idmap, nullptr, nullptr, (const int2 *)c.colour);
 }
 
 int launch_vd_repair_cells(Ctx &c, int nflag, int T, int logT, int cells, const int16_t *ycol, const int *idmap,
-                           int *esc_cells)
+                           int *esc_cells, const int *cellmap, const int2 *chunk)
 {
     int tiles_x = (T - 1 + KT_W - 1) / KT_W, tiles_y = (T - 1 + KT_H - 1) / KT_H;
     int ntiles = tiles_x * tiles_y * cells;
@@ -745,14 +769,13 @@ int launch_vd_repair_cells(Ctx &c, int nflag, int T, int logT, int cells, const 
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
     k_redo_mark<<<(nflag + 127) / 128, 128, 0, c.stream>>>(c.list2, nflag, redo, tiles_x, tiles_y);
     count_launch();
-    k_redo_collect<<<(ntiles + 255) / 256, 256, 0, c.stream>>>(redo, ntiles, (const int2 *)c.colour, c.tv, c.list,
-                                                                c.freelist, c.ctr);
+    k_redo_collect<<<(ntiles + 255) / 256, 256, 0, c.stream>>>(redo, ntiles, chunk, c.tv, c.list, c.freelist, c.ctr);
     count_launch();
     int r = read_counters(c);
     if (r) return r;
     int nredo = c.hctr->nlist;
     k_vd_tri_repair<<<nredo, kFusedThreads, 0, c.stream>>>(ycol, idmap, c.tv, c.list, c.freelist, tiles_x, T, logT,
-                                                           c.cap_tris, esc_cells, c.ctr);
+                                                           c.cap_tris, esc_cells, c.ctr, cellmap);
     count_launch();
     k_clamp_free<<<1, 1, 0, c.stream>>>(c.ctr);
     count_launch();
@@ -762,16 +785,18 @@ int launch_vd_repair_cells(Ctx &c, int nflag, int T, int logT, int cells, const 
 
 int launch_vd_tri(Ctx &c)
 {
-    return launch_vd_tri_cells(c, c.T, c.logT, 1, c.ycol, c.idmap, (int2 *)c.colour, c.list2);
+    return launch_vd_tri_cells(c, c.T, c.logT, 1, c.ycol, c.idmap, (int2 *)c.colour, c.list2, nullptr);
 }
 
-// Tiles of all cells, numbered cell-major; chunk / flagged use that numbering.
+// Tiles of all launched cells, numbered cell-major; chunk / flagged use that
+// numbering.  cellmap (or identity) gives the texture cell of launch cell z.
 int launch_vd_tri_cells(Ctx &c, int T, int logT, int cells, const int16_t *ycol, const int *idmap, int2 *chunk,
-                        int *flagged)
+                        int *flagged, const int *cellmap)
 {
     dim3 grid((T - 1 + KT_W - 1) / KT_W, (T - 1 + KT_H - 1) / KT_H, cells);
     kev_record(c, 0);
-    k_vd_tri<<<grid, kFusedThreads, 0, c.stream>>>(ycol, idmap, c.tv, chunk, flagged, T, logT, c.cap_tris, c.ctr);
+    k_vd_tri<<<grid, kFusedThreads, 0, c.stream>>>(ycol, idmap, c.tv, chunk, flagged, T, logT, c.cap_tris, c.ctr,
+                                                    cellmap);
     count_launch();
     kev_record(c, 1);
     GALPHA_CUDA(cudaGetLastError());
@@ -798,15 +823,23 @@ int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *o
 
 int launch_row_pass(Ctx &c)
 {
+    return launch_row_pass_cells(c, 1, nullptr);
+}
+
+// Rows of `cells` texture cells of size c.T at c.ycol / c.idmap / c.colour
+// (cell cellmap[z], or z).
+int launch_row_pass_cells(Ctx &c, int cells, const int *cellmap)
+{
     const int T = c.T;
     size_t sm = sizeof(int16_t) * (3 * (size_t)T + (T & 1)) + sizeof(int) * (size_t)T;
-    static int configured = 0;
-    if (configured < (int)sm) {
+    static int configured[64];
+    const int dv = c.device >= 0 && c.device < 64 ? c.device : 0;
+    if (configured[dv] < (int)sm) {
         GALPHA_CUDA(cudaFuncSetAttribute(k_row_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        configured = (int)sm;
+        configured[dv] = (int)sm;
     }
     kev_record(c, 0);
-    k_row_pass<<<T, kRowThreads, sm, c.stream>>>(c.ycol, c.idmap, c.colour, T, c.logT);
+    k_row_pass<<<dim3(T, cells), kRowThreads, sm, c.stream>>>(c.ycol, c.idmap, c.colour, T, c.logT, cellmap);
     kev_record(c, 1);
     count_launch();
     GALPHA_CUDA(cudaGetLastError());
@@ -815,11 +848,20 @@ int launch_row_pass(Ctx &c)
 
 int launch_emit(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_out)
 {
+    return launch_emit_cells(c, ntiles, nwin, write, tv_out, 1, nullptr);
+}
+
+// ntiles blocks per cell; `cells` cells of size c.T at c.colour (cellmap[z], or z).
+int launch_emit_cells(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_out, int cells, const int *cellmap)
+{
     kev_record(c, write ? 6 : 4);
+    const long long blocks = (long long)ntiles * cells;
     if (!write)
-        k_emit_count<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.T, c.logT, nwin, c.ctr);
+        k_emit_count<<<(unsigned)blocks, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, c.T, c.logT, nwin,
+                                                                      c.ctr, cellmap, ntiles);
     else
-        k_emit_write<<<ntiles, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, tv_out, c.T, c.logT, nwin);
+        k_emit_write<<<(unsigned)blocks, kEmitThreads, 0, c.stream>>>(c.colour, c.gpix, c.tilecount, tv_out, c.T,
+                                                                      c.logT, nwin, cellmap, ntiles);
     count_launch();
     kev_record(c, write ? 7 : 5);
     GALPHA_CUDA(cudaGetLastError());

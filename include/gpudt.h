@@ -82,6 +82,7 @@ typedef struct {
     int missingRounds;       /* insertion rounds */
     int nRepairTiles;        /* fused-path tiles with islands, repaired locally */
     int nEscalated;          /* textures (point sets) redone on the envelope path */
+    int nEnvelopeCells;      /* textures (point sets) coloured on the envelope path */
     long long exactOrient;   /* orientation tests that needed exact arithmetic */
     long long exactIncircle; /* in-circle tests that needed exact arithmetic */
     long long filteredIncircle; /* in-circle tests decided by the FP64 filter */

@@ -65,11 +65,13 @@ def test_batch_matches_single_runs(engine):
     sets = _mixed_sets(1)
     beng = G.Engine()
     try:
-        beng.run_batch(sets)
+        st = beng.run_batch(sets)
         res = beng.batch_results()
     finally:
         beng.close()
     assert len(res) == len(sets)
+    # the annulus and the clusters leave most of their cells empty: envelope path
+    assert st.nEnvelopeCells >= 1
     _compare(engine, sets, res)
 
 
