@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(kRowThreads) k_row_pass(const int16_t *__restr
 
     const int y = blockIdx.x;
     const int tid = threadIdx.x;
-    const int S = T / kRowThreads;
+    const int S = T >= kRowThreads ? T / kRowThreads : 1;  // columns per thread (T < 256: one, or none)
     // 1. load the row of column candidates (16-byte vectors)
     {
         const int4 *src = (const int4 *)(ycol + (size_t)y * T);
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kRowThreads) k_row_pass(const int16_t *__restr
     {
         int head = -1, tail = -1;
         int x0 = tid * S;
-        for (int x = x0; x < x0 + S; x++) {
+        for (int x = x0; x < x0 + S && x < T; x++) {
             int yc = ys[x];
             if (yc < 0) continue;
             Par cur{x, par_c(x, yc, y)};
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kRowThreads) k_row_pass(const int16_t *__restr
     // 4. colour: every live element paints its own interval
     {
         int x0 = tid * S;
-        for (int x = x0; x < x0 + S; x++) {
+        for (int x = x0; x < x0 + S && x < T; x++) {
             int yc = ys[x];
             if (yc < 0) continue;
             int nx = nxt[x];
