@@ -253,12 +253,13 @@ def serving_leg(G, D, seconds, rate=2000.0):
     for k in range(96):
         n = int(np.exp(rng.uniform(np.log(1000), np.log(1048576))))
         pool.append(D.uniform_points(n, 5000 + k) if k % 2 == 0 else D.gaussian_blobs(n, 5000 + k))
+    bounds = G.Engine.batch_bounds(pool)  # the clients' GPUDTPARAMS bounds
     arrivals = S.poisson_arrivals(rate, seconds, 77)
     pick = rng.integers(0, len(pool), len(arrivals))
     eng = G.Engine()
-    warm = [S.Request(i, 0.0, pool[i]) for i in range(8)]
+    warm = [S.Request(i, 0.0, pool[i], bounds=bounds[i]) for i in range(len(pool))]
     S.Server(eng).run(warm)
-    reqs = [S.Request(i, t, pool[pick[i]]) for i, t in enumerate(arrivals)]
+    reqs = [S.Request(i, t, pool[pick[i]], bounds=bounds[pick[i]]) for i, t in enumerate(arrivals)]
     srv = S.Server(eng, hbm_budget=120e9)
     srv.run(reqs)
     eng.close()

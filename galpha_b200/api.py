@@ -376,8 +376,8 @@ class Engine:
         for k, p in enumerate(sets):
             p = np.asarray(p, dtype=np.float64).reshape(-1, 2)
             if len(p):
-                b[k, :2] = p.min(axis=0)
-                b[k, 2:] = p.max(axis=0)
+                x, y = p[:, 0], p[:, 1]  # column reductions: several times faster than axis=0
+                b[k] = (x.min(), y.min(), x.max(), y.max())
             else:
                 b[k] = (0.0, 0.0, 1.0, 1.0)
         return b
@@ -386,8 +386,11 @@ class Engine:
         """DT (+ alpha) of many independent point sets in one pipeline run
         (galphaRunBatchHost).  sets: list of (n_k, 2) arrays."""
         sizes = np.array([len(p) for p in sets], dtype=np.int32)
-        xy = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 2) for p in sets])
-                                  if len(sets) else np.zeros((0, 2)))
+        n = int(sizes.sum())
+        # staged in a reused pinned buffer: one DMA copy to the device
+        xy = self._pool.get("batch_xy", 2 * n, np.float64)[: 2 * n].reshape(-1, 2)
+        if n:
+            np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 2) for p in sets], out=xy)
         b = np.ascontiguousarray(self.batch_bounds(sets) if bounds is None else bounds, dtype=np.float64)
         st = Status()
         _check(self._L.galphaRunBatchHost(self._h, len(sets), sizes.ctypes.data, xy.ctypes.data if len(xy) else None,

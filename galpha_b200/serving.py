@@ -23,12 +23,19 @@ BYTES_PER_POINT = 2048
 
 
 class Request:
-    __slots__ = ("rid", "arrival", "points", "quantiles", "start", "done", "results")
+    """A DT + alpha-spectrum request: points, their bounds (minX, minY, maxX,
+    maxY, as the caller fills GPUDTPARAMS; computed if not given) and the
+    spectrum quantiles to query on the resulting mesh."""
+    __slots__ = ("rid", "arrival", "points", "bounds", "quantiles", "start", "done", "results")
 
-    def __init__(self, rid, arrival, points, quantiles=(0.1, 0.5, 0.9)):
+    def __init__(self, rid, arrival, points, quantiles=(0.1, 0.5, 0.9), bounds=None):
         self.rid = rid
         self.arrival = float(arrival)
         self.points = points
+        if bounds is None and len(points):
+            x, y = points[:, 0], points[:, 1]
+            bounds = (x.min(), y.min(), x.max(), y.max())
+        self.bounds = bounds if bounds is not None else (0.0, 0.0, 1.0, 1.0)
         self.quantiles = tuple(quantiles)
         self.start = None
         self.done = None
@@ -87,7 +94,7 @@ class Server:
                 continue
             batch, pts = self._admit(queue)
             start = clock() - t0
-            self.engine.run_batch([r.points for r in batch])
+            self.engine.run_batch([r.points for r in batch], bounds=np.array([r.bounds for r in batch], np.float64))
             nq = max(len(r.quantiles) for r in batch)
             answers = []
             for k in range(nq):

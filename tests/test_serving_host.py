@@ -24,7 +24,8 @@ class FakeEngine:
         self.batches = []
         self.queries = []
 
-    def run_batch(self, sets):
+    def run_batch(self, sets, bounds=None):
+        assert bounds is not None and len(bounds) == len(sets)
         self.batches.append([len(p) for p in sets])
         self.clock.t += 1e-3 + 1e-6 * sum(len(p) for p in sets)
 
