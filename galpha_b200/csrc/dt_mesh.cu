@@ -1324,6 +1324,9 @@ int stage_boundary(Ctx &c)
 // the host looks at the counters only every kFlipSync rounds.
 constexpr int kFlipSync = 4;
 
+// Each edge is tested from one side: when both triangles are in this round's
+// list (all of them in the first round; else stamp == prev_round), from the
+// lower index; the other side's proposal for the edge is made by that one.
 struct FlipCheck {
     const int4 *tv, *tn;
     const double2 *pos;
@@ -1331,6 +1334,8 @@ struct FlipCheck {
     int *vote, *prop, *target, *cands;
     int *cand_n;
     Counters *ct;
+    const int *stamp;
+    int prev_round;  // -1: every triangle is listed
     __device__ void operator()(long long ii) const
     {
         int t = act[ii];
@@ -1342,6 +1347,7 @@ struct FlipCheck {
             int e = nb[i];
             if (e < 0) continue;
             int u = dtri(e);
+            if (u < t && (prev_round < 0 || stamp[u] == prev_round)) continue;  // u tests this edge
             int d = geti(tv[u], dori(e));
             double2 A = pos[x[p1(i)]], B = pos[x[m1(i)]], C = pos[x[i]], D = pos[d];
             double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
@@ -1486,19 +1492,21 @@ int stage_flip(Ctx &c)
     launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
     const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
-    int rounds = 0, done = 0;
+    int rounds = 0, done = 0, prev_round = -1;
     while (!done) {
         for (int k = 0; k < kFlipSync; k++) {
             int p = rounds & 1;
             int round = next_round(c);
             launch_n(c, FlipRoundStart{p, c.ctr}, 1);
-            launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand, c.ctr},
+            launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand, c.ctr,
+                                    stamp, prev_round},
                        &c.ctr->act[p], capn);
             launch_dev(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, lists[1 - p],
                                     &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr},
                        &c.ctr->cand, capn);
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
             launch_dev(c, FlipReset{c.vote, target, cands}, &c.ctr->cand, capn);
+            prev_round = round;
             rounds++;
         }
         GALPHA_CUDA(cudaGetLastError());
