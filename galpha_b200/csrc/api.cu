@@ -248,6 +248,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     c.st.exactOrient = (long long)c.hctr->exact_orient;
     c.st.exactIncircle = (long long)c.hctr->exact_incircle;
     c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
+    for (int k = 0; k < 64; k++) c.st.filteredIncircle += (long long)c.hctr->filt_spread[k];
     c.have_mesh = true;
     return GPUDT_OK;
 }
@@ -342,6 +343,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     c.st.exactOrient = (long long)c.hctr->exact_orient;
     c.st.exactIncircle = (long long)c.hctr->exact_incircle;
     c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
+    for (int k = 0; k < 64; k++) c.st.filteredIncircle += (long long)c.hctr->filt_spread[k];
     bh.valid = true;
     return GPUDT_OK;
 }

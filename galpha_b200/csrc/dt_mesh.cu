@@ -1338,40 +1338,46 @@ struct FlipCheck {
     int prev_round;  // -1: every triangle is listed
     __device__ void operator()(long long ii) const
     {
-        int t = act[ii];
-        int4 v = tv[t];
-        if (v.x < 0) return;
-        int4 n = tn[t];
-        int x[3] = {v.x, v.y, v.z}, nb[3] = {n.x, n.y, n.z};
-        for (int i = 0; i < 3; i++) {
-            int e = nb[i];
-            if (e < 0) continue;
-            int u = dtri(e);
-            if (u < t && (prev_round < 0 || stamp[u] == prev_round)) continue;  // u tests this edge
-            int d = geti(tv[u], dori(e));
-            double2 A = pos[x[p1(i)]], B = pos[x[m1(i)]], C = pos[x[i]], D = pos[d];
-            double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
-            int s = incircle_filter(pa, pb, pc, pd);
-            if (s == 2) {
-                atomicAdd(&ct->exact_incircle, 1ull);
-                s = incircle_exact(pa, pb, pc, pd);
-                if (s == EXACT_OVERFLOW) {
-                    set_err(ct, GPUDT_ERR_EXACT, 90);
-                    return;
+        const int t = act[ii];
+        const int4 v = tv[t];
+        int ci = -1, cu = -1, nfilt = 0;
+        bool err = false;
+        if (v.x >= 0) {
+            const int4 n = tn[t];
+            const int x[3] = {v.x, v.y, v.z}, nb[3] = {n.x, n.y, n.z};
+            for (int i = 0; i < 3 && ci < 0 && !err; i++) {
+                const int e = nb[i];
+                if (e < 0) continue;
+                const int u = dtri(e);
+                if (u < t && (prev_round < 0 || stamp[u] == prev_round)) continue;  // u tests this edge
+                const int d = geti(tv[u], dori(e));
+                const double2 A = pos[x[p1(i)]], B = pos[x[m1(i)]], C = pos[x[i]], D = pos[d];
+                double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
+                int s = incircle_filter(pa, pb, pc, pd);
+                if (s == 2) {
+                    atomicAdd(&ct->exact_incircle, 1ull);
+                    s = incircle_exact(pa, pb, pc, pd);
+                    if (s == EXACT_OVERFLOW) err = true;
+                } else {
+                    nfilt++;
                 }
-            } else {
-                warp_count(&ct->filt_incircle);
-            }
-            if (s > 0) {
-                prop[t] = i;
-                target[t] = u;
-                atomicMin(&vote[t], t);
-                atomicMin(&vote[u], t);
-                int k = atomicAdd(cand_n, 1);
-                cands[k] = t;
-                return;
+                if (!err && s > 0) {
+                    ci = i;
+                    cu = u;
+                }
             }
         }
+        if (err) set_err(ct, GPUDT_ERR_EXACT, 90);
+        warp_add_spread(ct->filt_spread, nfilt);
+        const bool has = ci >= 0;
+        if (has) {
+            prop[t] = ci;
+            target[t] = cu;
+            atomicMin(&vote[t], t);
+            atomicMin(&vote[cu], t);
+        }
+        const int slot = warp_reserve(cand_n, has ? 1 : 0);
+        if (has) cands[slot] = t;
     }
 };
 
@@ -1383,60 +1389,62 @@ struct FlipApply {
     Relink *rec;
     int round;
     Counters *ct;
-    __device__ void add_next(int x) const
-    {
-        if (x < 0) return;
-        if (atomicExch(&stamp[x], round) != round) {
-            int k = atomicAdd(next_n, 1);
-            next[k] = x;
-        }
-    }
+    __device__ bool fresh(int x) const { return x >= 0 && atomicExch(&stamp[x], round) != round; }
     __device__ void operator()(long long ii) const
     {
-        int t = cands[ii];
-        int u = target[t];
-        if (vote[t] != t || vote[u] != t) {
-            add_next(t);
-            return;
+        const int t = cands[ii];
+        const int u = target[t];
+        const bool win = vote[t] == t && vote[u] == t;
+        int nx[6], nn = 0;
+        Relink r4[4];
+        if (!win) {
+            if (fresh(t)) nx[nn++] = t;
+        } else {
+            const int i = prop[t];
+            const int4 tvv = tv[t], tnn = tn[t];
+            const int e = geti(tnn, i);
+            const int j = dori(e);
+            const int4 uvv = tv[u], unn = tn[u];
+            const int a = geti(tvv, i), b = geti(tvv, p1(i)), cc = geti(tvv, m1(i)), d = geti(uvv, j);
+            const int ot1 = geti(tnn, p1(i)), ot2 = geti(tnn, m1(i));
+            const int ou1 = geti(unn, p1(j)), ou2 = geti(unn, m1(j));
+            epoch[t] = round;
+            epoch[u] = round;
+            tv[t] = make_int4(a, b, d, 0);
+            tv[u] = make_int4(d, cc, a, 0);
+            tn[t] = make_int4(-1, enc(u, 1), -1, 0);
+            tn[u] = make_int4(-1, enc(t, 1), -1, 0);
+            int4 ft = make_int4(0, 0, 0, 0), fu = make_int4(0, 0, 0, 0);
+            seti(ft, i, -1);
+            seti(ft, p1(i), enc(u, 0));
+            seti(ft, m1(i), enc(t, 2));
+            seti(fu, j, -1);
+            seti(fu, p1(j), enc(t, 0));
+            seti(fu, m1(j), enc(u, 2));
+            fwd[t] = ft;
+            fwd[u] = fu;
+            r4[0] = Relink{enc(t, 0), ou1};
+            r4[1] = Relink{enc(t, 2), ot2};
+            r4[2] = Relink{enc(u, 0), ot1};
+            r4[3] = Relink{enc(u, 2), ou2};
+            vtri[a] = enc(t, 0);
+            vtri[b] = enc(t, 1);
+            vtri[d] = enc(t, 2);
+            vtri[cc] = enc(u, 1);
+            if (fresh(t)) nx[nn++] = t;
+            if (fresh(u)) nx[nn++] = u;
+            if (ou1 >= 0 && fresh(dtri(ou1))) nx[nn++] = dtri(ou1);
+            if (ot2 >= 0 && fresh(dtri(ot2))) nx[nn++] = dtri(ot2);
+            if (ot1 >= 0 && fresh(dtri(ot1))) nx[nn++] = dtri(ot1);
+            if (ou2 >= 0 && fresh(dtri(ou2))) nx[nn++] = dtri(ou2);
         }
-        int i = prop[t];
-        int4 tvv = tv[t], tnn = tn[t];
-        int e = geti(tnn, i);
-        int j = dori(e);
-        int4 uvv = tv[u], unn = tn[u];
-        int a = geti(tvv, i), b = geti(tvv, p1(i)), cc = geti(tvv, m1(i)), d = geti(uvv, j);
-        int ot1 = geti(tnn, p1(i)), ot2 = geti(tnn, m1(i));
-        int ou1 = geti(unn, p1(j)), ou2 = geti(unn, m1(j));
-        epoch[t] = round;
-        epoch[u] = round;
-        tv[t] = make_int4(a, b, d, 0);
-        tv[u] = make_int4(d, cc, a, 0);
-        tn[t] = make_int4(-1, enc(u, 1), -1, 0);
-        tn[u] = make_int4(-1, enc(t, 1), -1, 0);
-        int4 ft = make_int4(0, 0, 0, 0), fu = make_int4(0, 0, 0, 0);
-        seti(ft, i, -1);
-        seti(ft, p1(i), enc(u, 0));
-        seti(ft, m1(i), enc(t, 2));
-        seti(fu, j, -1);
-        seti(fu, p1(j), enc(t, 0));
-        seti(fu, m1(j), enc(u, 2));
-        fwd[t] = ft;
-        fwd[u] = fu;
-        push_rec(rec, ct, enc(t, 0), ou1);
-        push_rec(rec, ct, enc(t, 2), ot2);
-        push_rec(rec, ct, enc(u, 0), ot1);
-        push_rec(rec, ct, enc(u, 2), ou2);
-        vtri[a] = enc(t, 0);
-        vtri[b] = enc(t, 1);
-        vtri[d] = enc(t, 2);
-        vtri[cc] = enc(u, 1);
-        atomicAdd(&ct->nflips, 1);
-        add_next(t);
-        add_next(u);
-        if (ou1 >= 0) add_next(dtri(ou1));
-        if (ot2 >= 0) add_next(dtri(ot2));
-        if (ot1 >= 0) add_next(dtri(ot1));
-        if (ou2 >= 0) add_next(dtri(ou2));
+        // one atomic per warp for each of the records, the flip count and the next list
+        const int rb = warp_reserve(&ct->nrec, win ? 4 : 0);
+        if (win)
+            for (int k = 0; k < 4; k++) rec[rb + k] = r4[k];
+        warp_reserve(&ct->nflips, win ? 1 : 0);
+        const int nb = warp_reserve(next_n, nn);
+        for (int k = 0; k < nn; k++) next[nb + k] = nx[k];
     }
 };
 

@@ -57,6 +57,7 @@ struct Counters {
     unsigned long long exact_incircle;
     unsigned long long filt_incircle;
     unsigned long long exact_attached;
+    unsigned long long filt_spread[64];  // in-circle tests decided by the filter, spread over 64 counters
     int qcount[12];  // alpha query: [type*4 + class], type 0 points, 1 edges, 2 triangles
     int qrank;       // alpha query: largest spectrum rank <= alpha (-1 if alpha < 0)
     int qpad;
@@ -235,6 +236,38 @@ __device__ __forceinline__ void warp_count(unsigned long long *c)
 {
     unsigned m = __activemask();
     if ((int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(c, (unsigned long long)__popc(m));
+}
+
+// Adds every calling thread's cnt with one atomic per warp, into one of 64
+// counters chosen by warp (a single hot counter serialises on the L2 atomics).
+__device__ __forceinline__ void warp_add_spread(unsigned long long *arr, int cnt)
+{
+    const unsigned m = __activemask();
+    const int tot = __reduce_add_sync(m, cnt);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && tot)
+        atomicAdd(&arr[((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & 63], (unsigned long long)tot);
+}
+
+// Reserves cnt consecutive slots of *counter for every calling thread with one
+// atomic per warp; returns the thread's first slot.  The calling lanes are a
+// prefix of the warp in grid-stride loops; any other set falls back to one
+// atomic per thread.
+__device__ __forceinline__ int warp_reserve(int *counter, int cnt)
+{
+    const unsigned m = __activemask();
+    if (m & (m + 1u)) return cnt ? atomicAdd(counter, cnt) : 0;
+    const int lane = threadIdx.x & 31;
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(m, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int last = 31 - __clz(m);
+    const int tot = __shfl_sync(m, incl, last);
+    int base = 0;
+    if (lane == last && tot) base = atomicAdd(counter, tot);
+    base = __shfl_sync(m, base, last);
+    return base + incl - cnt;
 }
 
 // 32-bit invertible mix (murmur3 finaliser): a random-looking priority per id.
