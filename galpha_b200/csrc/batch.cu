@@ -138,7 +138,8 @@ struct BSetupSites {
             py = iy + kMargin;
             vstate[v] = VS_UNDECIDED;
         } else {
-            short2 q = RingPixB{S.T, S.nside}(v - N - S.fbase);
+            const int k = v - N - S.fbase;
+            short2 q = RingPixB{S.T, S.nside}(k);
             px = q.x;
             py = q.y;
             p = make_double2(S.sx + (px - kMargin) * S.scale, S.sy + (py - kMargin) * S.scale);

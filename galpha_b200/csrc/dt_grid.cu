@@ -74,7 +74,7 @@ struct SetupSites {
     uint32_t *occ, *bandocc;
     int8_t *vstate;
     int *vtri, *vround, *anchor;
-    int N, T, logT, W2;
+    int N, F, T, logT, W2;
     double scale, sx, sy, minX, minY, maxX, maxY;
     RingPix ring;
     Counters *ct;
@@ -383,6 +383,7 @@ int stage_setup(Ctx &c, const double *d_xy, int n, double minX, double minY, dou
     s.vround = c.vround;
     s.anchor = c.anchor;
     s.N = c.N;
+    s.F = c.F;
     s.T = T;
     s.logT = c.logT;
     s.W2 = W2;

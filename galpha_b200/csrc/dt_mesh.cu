@@ -965,52 +965,85 @@ int stage_missing(Ctx &c)
 // other classes that are still present, so they are not adjacent and their
 // fans are disjoint; the priority test below only matters in the rare case of
 // an edge cutting a texture corner.
+constexpr int kMaxChain = 256;
+
+// Selection of fake sites to remove together: a fake whose fan (walked once
+// each way from vtri) holds no competing fake of lower priority -- in the
+// first pass only fakes of its ring class (ring position modulo 4) compete,
+// later every remaining fake does.  The selected fake's fan is stored (slot
+// and index of f, packed, and the outer neighbour across the chain edge) so
+// that the removal reads it with independent loads instead of walking again;
+// fans of selected fakes are disjoint, so they stay valid until the removal.
 struct FakeSelect {
     const int4 *tv, *tn;
     const int8_t *vstate;
     const int *vtri;
-    int *list;
-    int *count;
-    int N, F, cls;
+    int *list, *fanoff, *fanlen;
+    int2 *fan;
+    int *count, *fan_n;
+    int N, cls;  // cls < 0: every remaining fake competes by priority
     Counters *ct;
-    __device__ bool conflicts(int f, int g, uint32_t pf) const
+    __device__ bool conflicts(int g, uint32_t pf) const
     {
-        return g >= N && vstate[g] == VS_FAKE && ((g - N) & 3) == cls && prio((uint32_t)g) < pf;
+        return g >= N && vstate[g] == VS_FAKE && (cls < 0 || ((g - N) & 3) == cls) && prio((uint32_t)g) < pf;
     }
     __device__ void operator()(long long ii) const
     {
-        if (((int)ii & 3) != cls) return;
-        int f = N + (int)ii;
-        if (vstate[f] != VS_FAKE) return;
-        uint32_t pf = prio((uint32_t)f);
-        // rotate clockwise to the hull, checking neighbours on the way
-        int e = vtri[f];
-        for (int guard = 0; guard < 8 * kMaxFan; guard++) {
-            int t = dtri(e), i = dori(e);
-            int4 w = tv[t];
-            int a = geti(w, p1(i)), b = geti(w, m1(i));
-            if (conflicts(f, a, pf) || conflicts(f, b, pf)) return;
-            int nx = geti(tn[t], m1(i));  // across (f, a)
-            if (nx < 0) break;
-            e = enc(dtri(nx), m1(dori(nx)));
-            if (e == vtri[f]) {
-                set_err(ct, GPUDT_ERR_TOPOLOGY, 70);
-                return;
+        const int f = N + (int)ii;
+        constexpr int M = kMaxChain;
+        int2 E[2 * M];  // (packed f-corner, outer neighbour) per fan triangle
+        int lo = M, hi = M;
+        bool pick = (cls < 0 || ((int)ii & 3) == cls) && vstate[f] == VS_FAKE;
+        if (pick) {
+            const uint32_t pf = prio((uint32_t)f);
+            const int e0 = vtri[f];
+            int e = e0;
+            for (;;) {  // counterclockwise from e0
+                const int t = dtri(e), i = dori(e);
+                const int4 w = tv[t], n = tn[t];
+                if (conflicts(geti(w, p1(i)), pf) || conflicts(geti(w, m1(i)), pf)) {
+                    pick = false;
+                    break;
+                }
+                E[hi++] = make_int2(e, geti(n, i));
+                const int nx = geti(n, p1(i));  // across (b, f)
+                if (nx < 0) break;
+                e = enc(dtri(nx), p1(dori(nx)));
+                if (e == e0 || hi >= 2 * M) {
+                    set_err(ct, GPUDT_ERR_TOPOLOGY, 70);
+                    pick = false;
+                    break;
+                }
+            }
+            e = e0;
+            while (pick) {  // clockwise from e0
+                const int nx = geti(tn[dtri(e)], m1(dori(e)));  // across (f, a)
+                if (nx < 0) break;
+                e = enc(dtri(nx), m1(dori(nx)));
+                const int t = dtri(e), i = dori(e);
+                const int4 w = tv[t];
+                if (conflicts(geti(w, p1(i)), pf)) {
+                    pick = false;
+                    break;
+                }
+                if (lo <= 0 || hi - lo >= M) {
+                    set_err(ct, GPUDT_ERR_TOPOLOGY, 71);
+                    pick = false;
+                    break;
+                }
+                E[--lo] = make_int2(e, geti(tn[t], i));
             }
         }
-        // the counterclockwise side
-        e = vtri[f];
-        for (int guard = 0; guard < 8 * kMaxFan; guard++) {
-            int t = dtri(e), i = dori(e);
-            int4 w = tv[t];
-            if (conflicts(f, geti(w, m1(i)), pf)) return;
-            int nx = geti(tn[t], p1(i));  // across (b, f)
-            if (nx < 0) break;
-            e = enc(dtri(nx), p1(dori(nx)));
+        const int d = pick ? hi - lo : 0;
+        const int k = warp_reserve(count, pick ? 1 : 0);
+        const int base = warp_reserve(fan_n, d);
+        if (pick) {
+            list[k] = f;
+            fanoff[k] = base;
+            fanlen[k] = d;
+            for (int q = 0; q < d; q++) fan[base + q] = E[lo + q];
         }
-        int k = atomicAdd(count, 1);
-        list[k] = f;
-        atomicAdd(&ct->changed, 1);
+        warp_reserve(&ct->changed, pick ? 1 : 0);
     }
 };
 
@@ -1023,12 +1056,12 @@ struct ZeroInts {
     }
 };
 
-constexpr int kMaxChain = 256;
 
 struct FakeRemove {
     int4 *tv, *tn, *fwd;
     int *epoch, *freelist, *vtri;
-    const int *list;
+    const int *list, *fanoff, *fanlen;
+    const int2 *fan;
     const double2 *pos;
     int8_t *vstate;
     Relink *rec;
@@ -1037,58 +1070,52 @@ struct FakeRemove {
     Counters *ct;
     __device__ void operator()(long long ii) const
     {
-        int f = list[ii];
-        // clockwise-most triangle
-        int e = vtri[f];
-        for (int guard = 0;; guard++) {
-            if (guard > 8 * kMaxFan) {
-                set_err(ct, GPUDT_ERR_TOPOLOGY, 71);
-                return;
-            }
-            int t = dtri(e), i = dori(e);
-            int nx = geti(tn[t], m1(i));
-            if (nx < 0) break;
-            e = enc(dtri(nx), m1(dori(nx)));
+        const int f = list[ii];
+        // f's fan as stored by FakeSelect: triangle k (slot Fs, f's index Fi,
+        // outer neighbour O across the chain edge U[k] -> U[k+1])
+        constexpr int M = kMaxChain;
+        int Fs[M], Fi[M], O[M];
+        const int lo = 0, hi = fanlen[ii], base = fanoff[ii];
+        for (int k = 0; k < hi; k++) {
+            const int2 q = fan[base + k];
+            Fs[k] = dtri(q.x);
+            Fi[k] = dori(q.x);
+            O[k] = q.y;
         }
-        int U[kMaxChain + 1], Fs[kMaxChain], Fi[kMaxChain], O[kMaxChain];
-        int d = 0;
-        for (;;) {
-            if (d >= kMaxChain) {
-                set_err(ct, GPUDT_ERR_TOPOLOGY, 72);
-                return;
-            }
-            int t = dtri(e), i = dori(e);
-            int4 w = tv[t];
-            U[d] = geti(w, p1(i));
-            Fs[d] = t;
-            Fi[d] = i;
-            O[d] = geti(tn[t], i);
-            d++;
-            U[d] = geti(w, m1(i));
-            int nx = geti(tn[t], p1(i));
-            if (nx < 0) break;
-            e = enc(dtri(nx), p1(dori(nx)));
+        const int d = hi - lo;
+        if (d > M) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 73);
+            return;
         }
-        for (int k = 0; k < d; k++) epoch[Fs[k]] = round;
+        // chain U[0..d] and its positions (independent loads, issued together)
+        int U[M + 1];
+        double2 P[M + 1];
+        for (int k = 0; k < d; k++) {
+            const int4 w = tv[Fs[lo + k]];
+            U[k] = geti(w, p1(Fi[lo + k]));
+            if (k == d - 1) U[d] = geti(w, m1(Fi[lo + k]));
+        }
+        for (int k = 0; k <= d; k++) P[k] = pos[U[k]];
+        for (int k = 0; k < d; k++) epoch[Fs[lo + k]] = round;
         // stack rule over the chain U[0..d]
-        int S[kMaxChain + 1], SO[kMaxChain + 1];  // SO[k]: owner of chain edge S[k-1] -> S[k]
+        int S[M + 1], SO[M + 1];  // SO[k]: owner of chain edge S[k-1] -> S[k]
         int top = 0, used = 0;
         auto owner_link = [&](int ownv, int loc) {
             if (ownv <= -2) {
                 int k = -2 - ownv;
-                set_fwd(fwd, Fs[k], Fi[k], loc);
-                push_rec(rec, ct, loc, O[k]);
+                set_fwd(fwd, Fs[lo + k], Fi[lo + k], loc);
+                push_rec(rec, ct, loc, O[lo + k]);
             } else {
                 set_link(tn, loc, ownv);
                 set_link(tn, ownv, loc);
             }
         };
         for (int k = 0; k <= d; k++) {
-            int wv = U[k];
+            const int wv = U[k];
             int wown = k > 0 ? -2 - (k - 1) : -1;
-            while (top >= 2 && orientp(pos[S[top - 2]], pos[S[top - 1]], pos[wv], ct) > 0) {
-                int s = Fs[used++];
-                int A = S[top - 2], B = S[top - 1];
+            while (top >= 2 && orientp(P[S[top - 2]], P[S[top - 1]], P[k], ct) > 0) {
+                const int s = Fs[lo + used++];
+                const int A = U[S[top - 2]], B = U[S[top - 1]];
                 tv[s] = make_int4(A, B, wv, 0);
                 tn[s] = make_int4(-1, -1, -1, 0);
                 // opp wv (2): A->B owned by SO[top-1]; opp A (0): B->wv owned by wown;
@@ -1101,26 +1128,26 @@ struct FakeRemove {
                 vtri[wv] = enc(s, 2);
                 top--;
             }
-            S[top] = wv;
+            S[top] = k;  // stack of chain positions
             SO[top] = wown;
             top++;
         }
         // remaining chain edges are hull edges now
         for (int k = 1; k < top; k++) {
-            int ownv = SO[k];
+            const int ownv = SO[k];
             if (ownv <= -2) {
-                int q = -2 - ownv;
-                set_fwd(fwd, Fs[q], Fi[q], -1);
-                push_rec(rec, ct, -1, O[q]);
+                const int q = -2 - ownv;
+                set_fwd(fwd, Fs[lo + q], Fi[lo + q], -1);
+                push_rec(rec, ct, -1, O[lo + q]);
             } else {
                 set_link(tn, ownv, -1);
             }
         }
         for (int k = 0; k < top; k++) {
             int c = atomicAdd(&ct->nlist2, 1);
-            cand[c] = S[k];
+            cand[c] = U[S[k]];
         }
-        for (int k = used; k < d; k++) free_slot(tv, freelist, ct, Fs[k]);
+        for (int k = used; k < d; k++) free_slot(tv, freelist, ct, Fs[lo + k]);
         vtri[f] = -1;
         vstate[f] = VS_GONE;
     }
@@ -1267,15 +1294,24 @@ int stage_boundary(Ctx &c)
     const int order[4] = {0, 2, 1, 3};
     const long long recn = 4LL * c.cap_tris;
     int removed = 0;
+    // stored fans of the selected fakes: (offset, length) per list entry and
+    // the entries; the incidence array of the links stage is free by now
+    int *fanoff = c.anchor, *fanlen = c.vround;  // per list entry (F <= V)
+    int2 *fan = (int2 *)c.inc;                    // 3 cap ints: 1.5 cap entries
+    // first pass: the four ring classes in turn (independent by construction);
+    // then rounds of priority-minimal fakes among all that remain
     for (int pass = 0; removed < c.F; pass++) {
         if (pass > kMaxRounds / 4) return GPUDT_ERR_NOCONVERGE;
-        for (int q = 0; q < 4; q++) {
+        const int nsub = pass == 0 ? 4 : 1;
+        for (int q = 0; q < nsub; q++) {
             int round = next_round(c);
             launch_n(c, ZeroInts{&c.ctr->nlist, &c.ctr->nrec}, 1);
-            launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, &c.ctr->nlist, c.N, c.F, order[q], c.ctr},
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->cand, 0, sizeof(int), c.stream));  // fan entries
+            launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
+                                   &c.ctr->cand, c.N, pass == 0 ? order[q] : -1, c.ctr},
                      c.F);
-            launch_dev(c, FakeRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, c.pos, c.vstate, c.rec,
-                                     cand, round, c.ctr},
+            launch_dev(c, FakeRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, fanoff, fanlen, fan, c.pos,
+                                     c.vstate, c.rec, cand, round, c.ctr},
                        &c.ctr->nlist, c.F);
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
         }

@@ -151,10 +151,11 @@ long long radix_scratch_ints(long long n)
     return 8 + 256 * ((n + kRsTile - 1) / kRsTile + 1);
 }
 
-// Sorts (keys, vals)[0..n) ascending (stable); result in keys/vals.  Uses
-// keys2/vals2 and `scratch` (radix_scratch_ints(n) ints).
+// Sorts (keys, vals)[0..n) ascending (stable) on the key bits from min_shift
+// up; result in keys/vals.  Uses keys2/vals2 and `scratch`
+// (radix_scratch_ints(n) ints).
 template <typename K>
-static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int n, int *scratch)
+static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int n, int *scratch, int min_shift = 0)
 {
     if (n <= 1) return GPUDT_OK;
     static_assert(sizeof(K) == 4 || sizeof(K) == 8, "32- or 64-bit keys");
@@ -180,7 +181,7 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
     int *hist = scratch + 8;
     K *ki = keys, *ko = keys2;
     int *vi = vals, *vo = vals2;
-    for (int shift = 0; shift < (int)(8 * sizeof(K)); shift += 8) {
+    for (int shift = min_shift; shift < (int)(8 * sizeof(K)); shift += 8) {
         if (((varying >> shift) & 255ull) == 0) continue;
         k_rs_hist<K><<<nblocks, kRsThreads, 0, c.stream>>>(ki, n, shift, hist, nblocks);
         count_launch();
@@ -199,9 +200,96 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
     return GPUDT_OK;
 }
 
+// ---------------------------------------------------------- 64-bit keys
+// The radix passes run on the top 40 bits only (5 digits instead of 8).
+// Entries whose top 40 bits agree are then put in full-key order: each such
+// group that is out of order is insertion-sorted (stable) by one thread.  A
+// group longer than kMaxFixGroup sends the whole array through the 3 low
+// digits as well (an LSD sort of the partly sorted array keeps equal keys in
+// their current, i.e. input, order), so the result is always the stable
+// sort of the full keys.
+constexpr int kLowBits = 24;
+constexpr int kMaxFixGroup = 64;
+
+struct FixFind {
+    const unsigned long long *keys;
+    int *starts, *flag;
+    int n;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        const int i = (int)ii;
+        const unsigned long long k = keys[i], kp = keys[i - 1];
+        if ((k >> kLowBits) != (kp >> kLowBits) || k >= kp) return;
+        int s = i - 1, len = 2;
+        while (s > 0 && (keys[s - 1] >> kLowBits) == (k >> kLowBits)) {
+            s--;
+            if (++len > kMaxFixGroup) {
+                ct->changed = 1;  // too long: full sort
+                return;
+            }
+        }
+        for (int e = i + 1; e < n && (keys[e] >> kLowBits) == (k >> kLowBits); e++)
+            if (++len > kMaxFixGroup) {
+                ct->changed = 1;
+                return;
+            }
+        if (atomicExch(&flag[s], 1) == 0) starts[atomicAdd(&ct->nlist2, 1)] = s;
+    }
+};
+
+struct FixFindOffset {
+    const unsigned long long *keys;
+    int *starts, *flag;
+    int n;
+    Counters *ct;
+    __device__ void operator()(long long i) const { FixFind{keys, starts, flag, n, ct}(i + 1); }
+};
+
+struct FixGroups {
+    unsigned long long *keys;
+    int *vals;
+    const int *starts;
+    int *flag;
+    int n;
+    __device__ void operator()(long long ii) const
+    {
+        const int s = starts[ii];
+        flag[s] = 0;
+        const unsigned long long hi = keys[s] >> kLowBits;
+        int e = s + 1;
+        while (e < n && (keys[e] >> kLowBits) == hi) e++;
+        for (int a = s + 1; a < e; a++) {
+            unsigned long long kc = keys[a];
+            int vc = vals[a];
+            int b = a - 1;
+            for (; b >= s && keys[b] > kc; b--) {
+                keys[b + 1] = keys[b];
+                vals[b + 1] = vals[b];
+            }
+            keys[b + 1] = kc;
+            vals[b + 1] = vc;
+        }
+    }
+};
+
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
 {
-    return radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist);
+    int r = radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist, kLowBits);
+    if (r || n <= 1) return r;
+    // group fix-up (starts / flags reuse the second key buffer, free now)
+    int *starts = (int *)keys2, *flag = starts + ((n + 63) & ~63);
+    GALPHA_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)n, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+    launch_n(c, FixFindOffset{keys, starts, flag, n, c.ctr}, n - 1);
+    r = read_counters(c);
+    if (r) return r;
+    if (c.hctr->changed)
+        return radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist, 0);
+    if (c.hctr->nlist2 > 0) launch_n(c, FixGroups{keys, vals, starts, flag, n}, c.hctr->nlist2);
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
 }
 
 int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch)
