@@ -1097,14 +1097,18 @@ struct FakeRemove {
         }
         for (int k = 0; k <= d; k++) P[k] = pos[U[k]];
         for (int k = 0; k < d; k++) epoch[Fs[lo + k]] = round;
-        // stack rule over the chain U[0..d]
+        // stack rule over the chain U[0..d].  Every one of the d chain edges
+        // ends with exactly one relink record (linked to a new triangle, or
+        // left as a hull edge), so the records are reserved with one atomic.
         int S[M + 1], SO[M + 1];  // SO[k]: owner of chain edge S[k-1] -> S[k]
         int top = 0, used = 0;
+        const int rbase = d > 0 ? atomicAdd(&ct->nrec, d) : 0;
+        int rn = 0;
         auto owner_link = [&](int ownv, int loc) {
             if (ownv <= -2) {
                 int k = -2 - ownv;
                 set_fwd(fwd, Fs[lo + k], Fi[lo + k], loc);
-                push_rec(rec, ct, loc, O[lo + k]);
+                rec[rbase + rn++] = Relink{loc, O[lo + k]};
             } else {
                 set_link(tn, loc, ownv);
                 set_link(tn, ownv, loc);
@@ -1138,16 +1142,23 @@ struct FakeRemove {
             if (ownv <= -2) {
                 const int q = -2 - ownv;
                 set_fwd(fwd, Fs[lo + q], Fi[lo + q], -1);
-                push_rec(rec, ct, -1, O[lo + q]);
+                rec[rbase + rn++] = Relink{-1, O[lo + q]};
             } else {
                 set_link(tn, ownv, -1);
             }
         }
-        for (int k = 0; k < top; k++) {
-            int c = atomicAdd(&ct->nlist2, 1);
-            cand[c] = U[S[k]];
+        if (rn != d) set_err(ct, GPUDT_ERR_TOPOLOGY, 74);
+        {
+            const int cb = atomicAdd(&ct->nlist2, top);
+            for (int k = 0; k < top; k++) cand[cb + k] = U[S[k]];
         }
-        for (int k = used; k < d; k++) free_slot(tv, freelist, ct, Fs[lo + k]);
+        if (used < d) {
+            const int fb = atomicAdd(&ct->nfree, d - used);
+            for (int k = used; k < d; k++) {
+                tv[Fs[lo + k]] = make_int4(-1, -1, -1, 0);
+                freelist[fb + k - used] = Fs[lo + k];
+            }
+        }
         vtri[f] = -1;
         vstate[f] = VS_GONE;
     }
