@@ -1057,6 +1057,150 @@ struct ZeroInts {
 };
 
 
+// Removal of the selected fake sites, one warp per fake: the lanes load the
+// stored fan, the chain U[0..d] and its positions into shared memory; lane 0
+// runs the stack rule (the ccw > 0 rule of cudaBoundary.cu:278) on that copy;
+// the lanes then write the remaining hull edges, the boundary candidates and
+// the released slots.
+struct FakeRemoveArgs {
+    int4 *tv, *tn, *fwd;
+    int *epoch, *freelist, *vtri;
+    const int *list, *fanoff, *fanlen;
+    const int2 *fan;
+    const double2 *pos;
+    int8_t *vstate;
+    Relink *rec;
+    int *cand;  // boundary-candidate vertices
+    int round;
+    Counters *ct;
+};
+
+#ifdef __CUDACC__
+__global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int *n_dev)
+{
+    constexpr int M = kMaxChain;
+    __shared__ int Fs[M], Fi[M], O[M], U[M + 1], S[M + 1], SO[M + 1];
+    __shared__ double2 P[M + 1];
+    __shared__ int s_top, s_used, s_rbase, s_rn;
+    const int lane = threadIdx.x;
+    const int n = *n_dev;
+    for (int item = blockIdx.x; item < n; item += gridDim.x) {
+        const int f = a.list[item], d = a.fanlen[item], base = a.fanoff[item];
+        if (d > M) {  // cannot happen: FakeSelect bounds the fan
+            if (lane == 0) set_err(a.ct, GPUDT_ERR_TOPOLOGY, 73);
+            continue;
+        }
+        for (int k = lane; k < d; k += 32) {
+            const int2 q = a.fan[base + k];
+            const int t = dtri(q.x), i = dori(q.x);
+            Fs[k] = t;
+            Fi[k] = i;
+            O[k] = q.y;
+            const int4 w = a.tv[t];
+            U[k] = geti(w, p1(i));
+            if (k == d - 1) U[d] = geti(w, m1(i));
+            a.epoch[t] = a.round;
+        }
+        __syncwarp();
+        for (int k = lane; k <= d; k += 32) P[k] = a.pos[U[k]];
+        __syncwarp();
+        if (lane == 0) {
+            // every one of the d chain edges ends with exactly one relink
+            // record (linked to a new triangle, or left as a hull edge)
+            const int rbase = d > 0 ? atomicAdd(&a.ct->nrec, d) : 0;
+            int rn = 0, top = 0, used = 0;
+            auto owner_link = [&](int ownv, int loc) {
+                if (ownv <= -2) {
+                    const int k = -2 - ownv;
+                    set_fwd(a.fwd, Fs[k], Fi[k], loc);
+                    a.rec[rbase + rn++] = Relink{loc, O[k]};
+                } else {
+                    set_link(a.tn, loc, ownv);
+                    set_link(a.tn, ownv, loc);
+                }
+            };
+            for (int k = 0; k <= d; k++) {
+                const int wv = U[k];
+                int wown = k > 0 ? -2 - (k - 1) : -1;  // chain edge U[k-1] -> U[k]: fan triangle k-1
+                while (top >= 2 && orientp(P[S[top - 2]], P[S[top - 1]], P[k], a.ct) > 0) {
+                    const int s = Fs[used++];
+                    const int A = U[S[top - 2]], B = U[S[top - 1]];
+                    a.tv[s] = make_int4(A, B, wv, 0);
+                    a.tn[s] = make_int4(-1, -1, -1, 0);
+                    // opp wv (2): A->B owned by SO[top-1]; opp A (0): B->wv owned by wown;
+                    // opp B (1): wv->A, the new chain edge A->wv
+                    owner_link(SO[top - 1], enc(s, 2));
+                    owner_link(wown, enc(s, 0));
+                    wown = enc(s, 1);
+                    a.vtri[A] = enc(s, 0);
+                    a.vtri[B] = enc(s, 1);
+                    a.vtri[wv] = enc(s, 2);
+                    top--;
+                }
+                S[top] = k;  // stack of chain positions
+                SO[top] = wown;
+                top++;
+            }
+            s_top = top;
+            s_used = used;
+            s_rbase = rbase;
+            s_rn = rn;
+        }
+        __syncwarp();
+        const int top = s_top, used = s_used, rbase = s_rbase;
+        // remaining chain edges are hull edges now (records after the rn
+        // written by the stack rule, in stack order)
+        {
+            int before = 0;  // chain-owned stack edges before this lane's
+            for (int k = 1 + lane; k < top; k += 32) {
+                const int ownv = SO[k];
+                if (ownv > -2) set_link(a.tn, ownv, -1);
+            }
+            int rn = s_rn;
+            for (int k0 = 1; k0 < top; k0 += 32) {
+                const int k = k0 + lane;
+                const bool own = k < top && SO[k] <= -2;
+                const unsigned m = __ballot_sync(0xffffffffu, own);
+                if (own) {
+                    const int q = -2 - SO[k];
+                    set_fwd(a.fwd, Fs[q], Fi[q], -1);
+                    a.rec[rbase + rn + __popc(m & ((1u << lane) - 1u))] = Relink{-1, O[q]};
+                }
+                rn += __popc(m);
+            }
+            (void)before;
+            if (lane == 0 && rn != d) set_err(a.ct, GPUDT_ERR_TOPOLOGY, 74);
+        }
+        {
+            int cb = 0, fb = 0;
+            if (lane == 0) {
+                cb = atomicAdd(&a.ct->nlist2, top);
+                fb = used < d ? atomicAdd(&a.ct->nfree, d - used) : 0;
+            }
+            cb = __shfl_sync(0xffffffffu, cb, 0);
+            fb = __shfl_sync(0xffffffffu, fb, 0);
+            for (int k = lane; k < top; k += 32) a.cand[cb + k] = U[S[k]];
+            for (int k = used + lane; k < d; k += 32) {
+                a.tv[Fs[k]] = make_int4(-1, -1, -1, 0);
+                a.freelist[fb + k - used] = Fs[k];
+            }
+        }
+        if (lane == 0) {
+            a.vtri[f] = -1;
+            a.vstate[f] = VS_GONE;
+        }
+        __syncwarp();
+    }
+}
+
+static void launch_fake_remove(Ctx &c, const FakeRemoveArgs &a, const int *n_dev, int max_n)
+{
+    const int blocks = std::max(1, std::min(max_n, c.sm_count * 16));
+    k_fake_remove<<<blocks, 32, 0, c.stream>>>(a, n_dev);
+    count_launch();
+}
+#else
+// Host emulation builds (no kernel launches): the same removal, one thread per fake.
 struct FakeRemove {
     int4 *tv, *tn, *fwd;
     int *epoch, *freelist, *vtri;
@@ -1163,6 +1307,14 @@ struct FakeRemove {
         vstate[f] = VS_GONE;
     }
 };
+
+static void launch_fake_remove(Ctx &c, const FakeRemoveArgs &a, const int *n_dev, int max_n)
+{
+    launch_dev(c, FakeRemove{a.tv, a.tn, a.fwd, a.epoch, a.freelist, a.vtri, a.list, a.fanoff, a.fanlen, a.fan, a.pos,
+                             a.vstate, a.rec, a.cand, a.round, a.ct},
+               n_dev, max_n);
+}
+#endif
 
 // Convexity check of a boundary candidate: finds its hull edges (u->v, v->w)
 // and reports reflex vertices (orient(u,v,w) < 0).
@@ -1321,9 +1473,10 @@ int stage_boundary(Ctx &c)
             launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
                                    &c.ctr->cand, c.N, pass == 0 ? order[q] : -1, c.ctr},
                      c.F);
-            launch_dev(c, FakeRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, fanoff, fanlen, fan, c.pos,
-                                     c.vstate, c.rec, cand, round, c.ctr},
-                       &c.ctr->nlist, c.F);
+            launch_fake_remove(c,
+                               FakeRemoveArgs{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, fanoff, fanlen, fan,
+                                              c.pos, c.vstate, c.rec, cand, round, c.ctr},
+                               &c.ctr->nlist, c.F);
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
         }
         GALPHA_CUDA(cudaGetLastError());
