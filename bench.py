@@ -330,6 +330,7 @@ def main():
             ev[k][1].record(stream)
         stages.append(list(st.ms))
         kernels.append(list(st.kernelMs))
+        stats_sort = (int(st.sortKeys), int(st.sortPasses))
         stats = {k: getattr(st, k) for k in ("nVerts", "nFake", "nDuplicates", "nMissing", "nBadShift", "nIslandPixels",
                                              "nRepairTiles", "nEscalated",
                                              "nFlips", "flipRounds", "shiftRounds", "missingRounds", "exactOrient",
@@ -347,7 +348,10 @@ def main():
     nt, ne, ns = eng.counts()
     value = world * n / (max_ms / 1e3) / 1e6
 
-    # roofline of the dominant texture kernel (row pass: envelope + colouring)
+    # rooflines.  The sort of the spectrum keys is the largest HBM-bound kernel
+    # of the step (k_rs_hist + k_rs_scatter, ~11 % of device time; the larger
+    # FlipCheck share is gather/latency-bound in-circle work): algorithmic
+    # bytes = passes x keys x (8 B key + 4 B value, read and written once).
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -356,9 +360,20 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     T = fbo
-    row_ms = sum(k[0] for k in kernels) / len(kernels)
+    sort_ms = sum(k[3] for k in kernels) / len(kernels)
+    sort_bytes = 24.0 * stats_sort[0] * stats_sort[1]
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "spectrum_sort_traffic.txt")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                per = {l.split(":")[0].strip(): float(l.split(":")[1]) for l in f if ":" in l}
+            traffic = per["dram_bytes_per_key_pass"] * stats_sort[0] * stats_sort[1]
+        except Exception:
+            traffic = None
     # k_vd_tri per launch: read the int16 column-candidate texture once (2 B/pixel)
     # and write the dual triangles (16 B each)
+    row_ms = sum(k[0] for k in kernels) / len(kernels)
     row_bytes = 2.0 * T * T + 16.0 * nt
     col_ms = sum(k[1] for k in kernels) / len(kernels)
     stage_mean = [sum(s[i] for s in stages) / len(stages) for i in range(12)]
@@ -366,11 +381,16 @@ def main():
     n_spec = ns
     b_alg = 28.0 * T * T + 16.0 * n + 36.0 * nt + 8.0 * n_spec + 24.0 * n_spec + 12.0 * ne + 4.0 * nt + 8.0 * n
     roof = {
-        "bound": "hbm", "kernel": "k_vd_tri (fused colouring + island test + dual triangles)",
-        "achieved": row_bytes / (row_ms / 1e3) / 1e9 if row_ms > 0 else None, "peak": peak, "unit": "GB/s",
-        "frac": (row_bytes / (row_ms / 1e3) / 1e9) / peak if row_ms > 0 else None,
-        "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650",
-        "algorithmic_bytes_per_launch": row_bytes, "launch_ms": row_ms,
+        "bound": "hbm",
+        "kernel": "spectrum key sort (k_rs_hist + scan + k_rs_scatter, %d passes of 8-bit digits)" % stats_sort[1],
+        "achieved": sort_bytes / (sort_ms / 1e3) / 1e9 if sort_ms > 0 else None, "peak": peak, "unit": "GB/s",
+        "frac": (sort_bytes / (sort_ms / 1e3) / 1e9) / peak if sort_ms > 0 else None,
+        "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650",
+        "algorithmic_bytes_per_launch": sort_bytes, "launch_ms": sort_ms, "keys": stats_sort[0],
+        "others": [{"kernel": "k_vd_tri (fused colouring + island test + dual triangles)",
+                    "achieved": row_bytes / (row_ms / 1e3) / 1e9 if row_ms > 0 else None,
+                    "frac": (row_bytes / (row_ms / 1e3) / 1e9) / peak if row_ms > 0 else None,
+                    "algorithmic_bytes_per_launch": row_bytes, "launch_ms": row_ms}],
         "pipeline": {"algorithmic_bytes": b_alg, "achieved_gbs": b_alg / (max_ms / 1e3) / 1e9,
                      "frac": b_alg / (max_ms / 1e3) / 1e9 / peak},
     }
@@ -426,7 +446,7 @@ def main():
                 ["upload", "voronoi", "triangles", "shift", "missing", "boundary", "flip", "compact", "alpha",
                  "download", "total"]) if i < 11},
             "kernels_ms": {"vd_tri": row_ms, "column_pass": col_ms,
-                           "emit": sum(k[2] for k in kernels) / len(kernels)},
+                           "emit": sum(k[2] for k in kernels) / len(kernels), "spectrum_sort": sort_ms},
             "counts": {"triangles": nt, "edges": ne, "spectrum": ns},
             "pipeline_stats": stats,
             "batched": batched,

@@ -534,8 +534,19 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     if (r) return r;
     const int nIn = 1 + nT + c.hctr->nlist;
     c.nSpecIn = nIn;
+    c.sort_passes = 0;
+    if (c.events) {
+        cudaEventRecord(c.kev[8], c.stream);
+        c.kev_rec[8] = true;
+    }
     r = radix_sort(c, c.keys + 1, c.vals + 1, c.keys2, c.vals2, nIn - 1);
     if (r) return r;
+    if (c.events) {
+        cudaEventRecord(c.kev[9], c.stream);
+        c.kev_rec[9] = true;
+    }
+    c.st.sortKeys = nIn - 1;
+    c.st.sortPasses = c.sort_passes;
     if (segs) {
         // stable sort by set: entries end up ordered by (set, value)
         const int m = nIn - 1;

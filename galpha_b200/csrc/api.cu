@@ -204,7 +204,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     r = ensure(H, V, T, 0);
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
-    for (int k = 0; k < 8; k++) c.kev_rec[k] = false;
+    for (int k = 0; k < 10; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
     int nonempty = has_triangles(c, d_xy, n);
@@ -291,7 +291,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     r = batch_buffers(c, H.bd, K, bh.N, (int)z.V, c.cap_tris, 3 * c.cap_tris + 8, bh.ntiles);
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
-    for (int k = 0; k < 8; k++) c.kev_rec[k] = false;
+    for (int k = 0; k < 10; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
     const char *stage = "setup";
@@ -368,6 +368,7 @@ static void fill_times(Ctx &c, int last)
     c.st.kernelMs[0] = kms(0);
     c.st.kernelMs[1] = kms(1);
     c.st.kernelMs[2] = kms(2) + kms(3);
+    c.st.kernelMs[3] = kms(4);
     cudaGetLastError();  // a timing query never leaves an error behind
 }
 
@@ -433,7 +434,7 @@ static int handle_init(galpha_ctx *h, int device, long long budget)
     GALPHA_CUDA(cudaMallocHost(&c.hctr, sizeof(Counters)));
     memset(c.hctr, 0, sizeof(Counters));
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2; k++) GALPHA_CUDA(cudaEventCreate(&c.ev[k]));
-    for (int k = 0; k < 8; k++) GALPHA_CUDA(cudaEventCreate(&c.kev[k]));
+    for (int k = 0; k < 10; k++) GALPHA_CUDA(cudaEventCreate(&c.kev[k]));
     c.events = true;
     // exact fall-back paths keep expansion arrays on the per-thread stack
     GALPHA_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 18432));  // largest kernel frame is ~16 KB
@@ -475,7 +476,7 @@ int galphaDestroy(galphaHandle h)
     if (h->H.bd.buf) cudaFree(h->H.bd.buf);
     if (c.hctr) cudaFreeHost(c.hctr);
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2 && c.events; k++) cudaEventDestroy(c.ev[k]);
-    for (int k = 0; k < 8 && c.events; k++) cudaEventDestroy(c.kev[k]);
+    for (int k = 0; k < 10 && c.events; k++) cudaEventDestroy(c.kev[k]);
     if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
     delete h;
     return GPUDT_OK;

@@ -154,11 +154,12 @@ struct Ctx {
 
     // events for stage timing
     cudaEvent_t ev[GALPHA_STAGE_TOTAL + 2];
-    cudaEvent_t kev[8];  // [2k, 2k+1] bracket single kernel k (see gpudtStatus.kernelMs)
-    bool kev_rec[8];     // recorded during the current call
+    cudaEvent_t kev[10];  // [2k, 2k+1] bracket single kernel k (see gpudtStatus.kernelMs)
+    bool kev_rec[10];     // recorded during the current call
     bool events = false;
     gpudtStatus st;
     bool have_mesh = false, have_alpha = false;
+    int sort_passes = 0;  // radix passes of the last radix_sort call
     bool fused_done = false;  // triangles came from the fused colour + dual kernel
 };
 

@@ -183,6 +183,7 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
     int *vi = vals, *vo = vals2;
     for (int shift = min_shift; shift < (int)(8 * sizeof(K)); shift += 8) {
         if (((varying >> shift) & 255ull) == 0) continue;
+        c.sort_passes++;
         k_rs_hist<K><<<nblocks, kRsThreads, 0, c.stream>>>(ki, n, shift, hist, nblocks);
         count_launch();
         int r = exclusive_scan_int(c, hist, hist, 256 * nblocks, nullptr);

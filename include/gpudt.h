@@ -90,7 +90,11 @@ typedef struct {
     float kernelMs[4];       /* single-kernel times (CUDA events on the launch stream):
                                 [0] colour + dual-triangle kernel (k_vd_tri; k_row_pass on
                                 the envelope path), [1] column pass,
-                                [2] triangle emission (count + write), [3] unused */
+                                [2] triangle emission (count + write),
+                                [3] spectrum key sort (all radix passes, alpha stage) */
+    long long sortKeys;      /* keys of the spectrum sort */
+    int sortPasses;          /* radix passes it took (8-bit digits) */
+    int pad0;
 } gpudtStatus;
 
 #ifdef __cplusplus
