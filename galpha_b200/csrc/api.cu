@@ -100,7 +100,7 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(inc, int, 3 * cap);
     TAKE(tilecount, int, z.ntiles + 1);
     TAKE(hist, int, 65536);
-    TAKE(rhist, int, 256 * (3 * cap / 4096 + 2) + 16);
+    TAKE(rhist, int, radix_scratch_ints((long long)(3 * cap)) + 16);
     TAKE(e_off, int, cap + 1);
     TAKE(edges, int4, 2 * cap);
     TAKE(edge_ro, int, 2 * cap);

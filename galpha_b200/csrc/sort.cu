@@ -15,8 +15,8 @@
 namespace galpha {
 
 constexpr int kRsThreads = 256;
-constexpr int kRsItems = 16;
-constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys per block
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 2048 keys per block (several blocks per SM)
 constexpr int kRsWarps = kRsThreads / 32;
 
 template <typename K>
@@ -44,8 +44,8 @@ struct RsSmem {
     int gbase[256];           // global start of this tile's run of each digit
 };
 
-// Stable scatter of one tile: warp w owns tile elements [w*512, (w+1)*512) in
-// 16 rounds of 32; an element's tile-local rank is (digit run start) + (keys
+// Stable scatter of one tile: warp w owns tile elements [w*256, (w+1)*256) in
+// 8 rounds of 32; an element's tile-local rank is (digit run start) + (keys
 // of the same digit in earlier warps) + (earlier rounds of its warp) + (lower
 // lanes of its round).
 template <typename K>
@@ -163,6 +163,8 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
     static bool attr_set[64];  // per key type and device: the opt-in above 48 KB, once
     if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
         GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxShared));
         if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
     }
     K *acc = reinterpret_cast<K *>(scratch);
