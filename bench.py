@@ -367,7 +367,8 @@ def main():
     if os.path.exists(tfile):
         try:
             with open(tfile) as f:
-                per = {l.split(":")[0].strip(): float(l.split(":")[1]) for l in f if ":" in l}
+                per = {l.split(":")[0].strip(): float(l.split(":")[1]) for l in f
+                       if ":" in l and not l.lstrip().startswith("#")}
             traffic = per["dram_bytes_per_key_pass"] * stats_sort[0] * stats_sort[1]
         except Exception:
             traffic = None

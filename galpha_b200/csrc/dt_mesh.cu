@@ -974,6 +974,8 @@ constexpr int kMaxChain = 256;
 // and index of f, packed, and the outer neighbour across the chain edge) so
 // that the removal reads it with independent loads instead of walking again;
 // fans of selected fakes are disjoint, so they stay valid until the removal.
+constexpr int kMaxFanLong = 4096;  // longest fan a fake may have (error beyond)
+
 struct FakeSelect {
     const int4 *tv, *tn;
     const int8_t *vstate;
@@ -991,13 +993,14 @@ struct FakeSelect {
     {
         const int f = N + (int)ii;
         constexpr int M = kMaxChain;
-        int2 E[2 * M];  // (packed f-corner, outer neighbour) per fan triangle
-        int lo = M, hi = M;
+        int2 E[2 * M];  // (packed f-corner, outer neighbour) per fan triangle, fans of up to M
+        int lo = M, hi = M, nccw = 0, ncw = 0, ecw = -1;
         bool pick = (cls < 0 || ((int)ii & 3) == cls) && vstate[f] == VS_FAKE;
         if (pick) {
             const uint32_t pf = prio((uint32_t)f);
             const int e0 = vtri[f];
             int e = e0;
+            ecw = e0;
             for (;;) {  // counterclockwise from e0
                 const int t = dtri(e), i = dori(e);
                 const int4 w = tv[t], n = tn[t];
@@ -1005,11 +1008,12 @@ struct FakeSelect {
                     pick = false;
                     break;
                 }
-                E[hi++] = make_int2(e, geti(n, i));
+                if (hi < 2 * M) E[hi++] = make_int2(e, geti(n, i));
+                nccw++;
                 const int nx = geti(n, p1(i));  // across (b, f)
                 if (nx < 0) break;
                 e = enc(dtri(nx), p1(dori(nx)));
-                if (e == e0 || hi >= 2 * M) {
+                if (e == e0 || nccw > kMaxFanLong) {
                     set_err(ct, GPUDT_ERR_TOPOLOGY, 70);
                     pick = false;
                     break;
@@ -1026,22 +1030,37 @@ struct FakeSelect {
                     pick = false;
                     break;
                 }
-                if (lo <= 0 || hi - lo >= M) {
+                if (nccw + ncw >= kMaxFanLong) {
                     set_err(ct, GPUDT_ERR_TOPOLOGY, 71);
                     pick = false;
                     break;
                 }
-                E[--lo] = make_int2(e, geti(tn[t], i));
+                if (lo > 0) E[--lo] = make_int2(e, geti(tn[t], i));
+                ncw++;
+                ecw = e;
             }
         }
-        const int d = pick ? hi - lo : 0;
+        const int d = pick ? nccw + ncw : 0;
         const int k = warp_reserve(count, pick ? 1 : 0);
         const int base = warp_reserve(fan_n, d);
         if (pick) {
             list[k] = f;
             fanoff[k] = base;
             fanlen[k] = d;
-            for (int q = 0; q < d; q++) fan[base + q] = E[lo + q];
+            if (d <= M) {
+                for (int q = 0; q < d; q++) fan[base + q] = E[lo + q];
+            } else {
+                // a long fan: walk it again from its clockwise end, into the store
+                int e = ecw;
+                for (int q = 0; q < d; q++) {
+                    const int t = dtri(e), i = dori(e);
+                    const int4 n = tn[t];
+                    fan[base + q] = make_int2(e, geti(n, i));
+                    const int nx = geti(n, p1(i));
+                    if (nx < 0) break;
+                    e = enc(dtri(nx), p1(dori(nx)));
+                }
+            }
         }
         warp_reserve(&ct->changed, pick ? 1 : 0);
     }
@@ -1075,21 +1094,24 @@ struct FakeRemoveArgs {
     Counters *ct;
 };
 
-#ifdef __CUDACC__
-__global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int *n_dev)
+// Dynamic shared memory for fans of up to M triangles.
+__host__ __device__ constexpr size_t fake_remove_smem(int M)
 {
-    constexpr int M = kMaxChain;
-    __shared__ int Fs[M], Fi[M], O[M], U[M + 1], S[M + 1], SO[M + 1];
-    __shared__ double2 P[M + 1];
+    return ((size_t)(3 * M + 3 * (M + 1)) * sizeof(int) + 15) / 16 * 16 + (size_t)(M + 1) * sizeof(double2);
+}
+
+// Items whose fan has dmin..M triangles (the short and the long launch).
+__global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int *n_dev, int M, int dmin)
+{
+    extern __shared__ __align__(16) unsigned char fr_smem[];
+    int *Fs = (int *)fr_smem, *Fi = Fs + M, *O = Fi + M, *U = O + M, *S = U + M + 1, *SO = S + M + 1;
+    double2 *P = (double2 *)(fr_smem + ((size_t)(3 * M + 3 * (M + 1)) * sizeof(int) + 15) / 16 * 16);
     __shared__ int s_top, s_used, s_rbase, s_rn;
     const int lane = threadIdx.x;
     const int n = *n_dev;
     for (int item = blockIdx.x; item < n; item += gridDim.x) {
         const int f = a.list[item], d = a.fanlen[item], base = a.fanoff[item];
-        if (d > M) {  // cannot happen: FakeSelect bounds the fan
-            if (lane == 0) set_err(a.ct, GPUDT_ERR_TOPOLOGY, 73);
-            continue;
-        }
+        if (d < dmin || d > M) continue;  // the other launch's item
         for (int k = lane; k < d; k += 32) {
             const int2 q = a.fan[base + k];
             const int t = dtri(q.x), i = dori(q.x);
@@ -1193,128 +1215,25 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
     }
 }
 
-static void launch_fake_remove(Ctx &c, const FakeRemoveArgs &a, const int *n_dev, int max_n)
+static int launch_fake_remove(Ctx &c, const FakeRemoveArgs &a, const int *n_dev, int max_n)
 {
-    const int blocks = std::max(1, std::min(max_n, c.sm_count * 16));
-    k_fake_remove<<<blocks, 32, 0, c.stream>>>(a, n_dev);
-    count_launch();
-}
-#else
-// Host emulation builds (no kernel launches): the same removal, one thread per fake.
-struct FakeRemove {
-    int4 *tv, *tn, *fwd;
-    int *epoch, *freelist, *vtri;
-    const int *list, *fanoff, *fanlen;
-    const int2 *fan;
-    const double2 *pos;
-    int8_t *vstate;
-    Relink *rec;
-    int *cand;  // boundary-candidate vertices
-    int round;
-    Counters *ct;
-    __device__ void operator()(long long ii) const
-    {
-        const int f = list[ii];
-        // f's fan as stored by FakeSelect: triangle k (slot Fs, f's index Fi,
-        // outer neighbour O across the chain edge U[k] -> U[k+1])
-        constexpr int M = kMaxChain;
-        int Fs[M], Fi[M], O[M];
-        const int lo = 0, hi = fanlen[ii], base = fanoff[ii];
-        for (int k = 0; k < hi; k++) {
-            const int2 q = fan[base + k];
-            Fs[k] = dtri(q.x);
-            Fi[k] = dori(q.x);
-            O[k] = q.y;
-        }
-        const int d = hi - lo;
-        if (d > M) {
-            set_err(ct, GPUDT_ERR_TOPOLOGY, 73);
-            return;
-        }
-        // chain U[0..d] and its positions (independent loads, issued together)
-        int U[M + 1];
-        double2 P[M + 1];
-        for (int k = 0; k < d; k++) {
-            const int4 w = tv[Fs[lo + k]];
-            U[k] = geti(w, p1(Fi[lo + k]));
-            if (k == d - 1) U[d] = geti(w, m1(Fi[lo + k]));
-        }
-        for (int k = 0; k <= d; k++) P[k] = pos[U[k]];
-        for (int k = 0; k < d; k++) epoch[Fs[lo + k]] = round;
-        // stack rule over the chain U[0..d].  Every one of the d chain edges
-        // ends with exactly one relink record (linked to a new triangle, or
-        // left as a hull edge), so the records are reserved with one atomic.
-        int S[M + 1], SO[M + 1];  // SO[k]: owner of chain edge S[k-1] -> S[k]
-        int top = 0, used = 0;
-        const int rbase = d > 0 ? atomicAdd(&ct->nrec, d) : 0;
-        int rn = 0;
-        auto owner_link = [&](int ownv, int loc) {
-            if (ownv <= -2) {
-                int k = -2 - ownv;
-                set_fwd(fwd, Fs[lo + k], Fi[lo + k], loc);
-                rec[rbase + rn++] = Relink{loc, O[lo + k]};
-            } else {
-                set_link(tn, loc, ownv);
-                set_link(tn, ownv, loc);
-            }
-        };
-        for (int k = 0; k <= d; k++) {
-            const int wv = U[k];
-            int wown = k > 0 ? -2 - (k - 1) : -1;
-            while (top >= 2 && orientp(P[S[top - 2]], P[S[top - 1]], P[k], ct) > 0) {
-                const int s = Fs[lo + used++];
-                const int A = U[S[top - 2]], B = U[S[top - 1]];
-                tv[s] = make_int4(A, B, wv, 0);
-                tn[s] = make_int4(-1, -1, -1, 0);
-                // opp wv (2): A->B owned by SO[top-1]; opp A (0): B->wv owned by wown;
-                // opp B (1): wv->A, the new chain edge A->wv
-                owner_link(SO[top - 1], enc(s, 2));
-                owner_link(wown, enc(s, 0));
-                wown = enc(s, 1);
-                vtri[A] = enc(s, 0);
-                vtri[B] = enc(s, 1);
-                vtri[wv] = enc(s, 2);
-                top--;
-            }
-            S[top] = k;  // stack of chain positions
-            SO[top] = wown;
-            top++;
-        }
-        // remaining chain edges are hull edges now
-        for (int k = 1; k < top; k++) {
-            const int ownv = SO[k];
-            if (ownv <= -2) {
-                const int q = -2 - ownv;
-                set_fwd(fwd, Fs[lo + q], Fi[lo + q], -1);
-                rec[rbase + rn++] = Relink{-1, O[lo + q]};
-            } else {
-                set_link(tn, ownv, -1);
-            }
-        }
-        if (rn != d) set_err(ct, GPUDT_ERR_TOPOLOGY, 74);
-        {
-            const int cb = atomicAdd(&ct->nlist2, top);
-            for (int k = 0; k < top; k++) cand[cb + k] = U[S[k]];
-        }
-        if (used < d) {
-            const int fb = atomicAdd(&ct->nfree, d - used);
-            for (int k = used; k < d; k++) {
-                tv[Fs[lo + k]] = make_int4(-1, -1, -1, 0);
-                freelist[fb + k - used] = Fs[lo + k];
-            }
-        }
-        vtri[f] = -1;
-        vstate[f] = VS_GONE;
+    static bool attr_set[64];
+    const int dv = c.device >= 0 && c.device < 64 ? c.device : 0;
+    if (!attr_set[dv]) {
+        GALPHA_CUDA(cudaFuncSetAttribute(k_fake_remove, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fake_remove_smem(kMaxFanLong)));
+        attr_set[dv] = true;
     }
-};
-
-static void launch_fake_remove(Ctx &c, const FakeRemoveArgs &a, const int *n_dev, int max_n)
-{
-    launch_dev(c, FakeRemove{a.tv, a.tn, a.fwd, a.epoch, a.freelist, a.vtri, a.list, a.fanoff, a.fanlen, a.fan, a.pos,
-                             a.vstate, a.rec, a.cand, a.round, a.ct},
-               n_dev, max_n);
+    const int blocks = std::max(1, std::min(max_n, c.sm_count * 16));
+    k_fake_remove<<<blocks, 32, fake_remove_smem(kMaxChain), c.stream>>>(a, n_dev, kMaxChain, 0);
+    count_launch();
+    // fans longer than kMaxChain (sparse input: chords across empty regions)
+    k_fake_remove<<<std::max(1, std::min(max_n, c.sm_count)), 32, fake_remove_smem(kMaxFanLong), c.stream>>>(
+        a, n_dev, kMaxFanLong, kMaxChain + 1);
+    count_launch();
+    GALPHA_CUDA(cudaGetLastError());
+    return GPUDT_OK;
 }
-#endif
 
 // Convexity check of a boundary candidate: finds its hull edges (u->v, v->w)
 // and reports reflex vertices (orient(u,v,w) < 0).
@@ -1473,10 +1392,11 @@ int stage_boundary(Ctx &c)
             launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
                                    &c.ctr->cand, c.N, pass == 0 ? order[q] : -1, c.ctr},
                      c.F);
-            launch_fake_remove(c,
+            r = launch_fake_remove(c,
                                FakeRemoveArgs{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, fanoff, fanlen, fan,
                                               c.pos, c.vstate, c.rec, cand, round, c.ctr},
                                &c.ctr->nlist, c.F);
+            if (r) return r;
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
         }
         GALPHA_CUDA(cudaGetLastError());
