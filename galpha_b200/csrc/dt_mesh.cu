@@ -1493,8 +1493,12 @@ struct FlipCheck {
         if (has) {
             prop[t] = ci;
             target[t] = cu;
-            atomicMin(&vote[t], t);
-            atomicMin(&vote[cu], t);
+            // votes carry a hashed priority (prio is a bijection on 32 bits):
+            // chains of competing flips then resolve in about log rounds
+            // instead of one step per round along increasing slot ids
+            const unsigned pt = prio((uint32_t)t);
+            atomicMin((unsigned *)&vote[t], pt);
+            atomicMin((unsigned *)&vote[cu], pt);
         }
         const int slot = warp_reserve(cand_n, has ? 1 : 0);
         if (has) cands[slot] = t;
@@ -1514,7 +1518,8 @@ struct FlipApply {
     {
         const int t = cands[ii];
         const int u = target[t];
-        const bool win = vote[t] == t && vote[u] == t;
+        const unsigned pt = prio((uint32_t)t);
+        const bool win = (unsigned)vote[t] == pt && (unsigned)vote[u] == pt;
         int nx[6], nn = 0;
         Relink r4[4];
         if (!win) {
@@ -1574,8 +1579,8 @@ struct FlipReset {
     __device__ void operator()(long long ii) const
     {
         int t = cands[ii];
-        vote[t] = 0x7fffffff;
-        vote[target[t]] = 0x7fffffff;
+        vote[t] = -1;  // 0xffffffff: no unsigned vote yet
+        vote[target[t]] = -1;
     }
 };
 
@@ -1618,6 +1623,7 @@ int stage_flip(Ctx &c)
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->flips_total, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nflips, 0, sizeof(int), c.stream));
     launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
+    GALPHA_CUDA(cudaMemsetAsync(c.vote, 0xff, sizeof(int) * (size_t)nt, c.stream));  // unsigned votes start at max
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
     const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
     int rounds = 0, done = 0, prev_round = -1;
