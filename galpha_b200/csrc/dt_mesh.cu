@@ -271,10 +271,16 @@ static int run_relink(Ctx &c, int round, int nrec)
 }
 
 // Host-side epoch counter: every operation round gets a fresh id.
-static int next_round(Ctx &c)
+static thread_local int g_round_counter = 1;
+static int next_round(Ctx &)
 {
-    static thread_local int counter = 1;
-    return ++counter;
+    return ++g_round_counter;
+}
+// Marks the k ids after `first` (first + 1 .. first + k) as used by rounds
+// that device code numbered itself.
+static void skip_rounds(int first, int k)
+{
+    if (first + k > g_round_counter) g_round_counter = first + k;
 }
 
 // ------------------------------------------------------------------- shift
@@ -1599,6 +1605,50 @@ struct FlipRoundStart {
     }
 };
 
+// The tail of the stage: once the active list is short, whole rounds run
+// inside ONE block, with __syncthreads between their phases instead of a launch
+// per phase (long flip chains -- a retriangulated hull pocket, a dense cluster
+// -- otherwise cost five launches per round for a handful of flips).  The same
+// functors run in the same phase order with consecutive round ids, so the mesh
+// is the one the launched rounds produce.  The block stops when the list
+// empties, when a round's list exceeds `leave` (the host goes back to launched
+// rounds) or after max_rounds; no thread ever waits on another block.
+constexpr int kTailThreads = 1024;
+constexpr int kTailEnter = 4096;    // the host hands over at or below this many active triangles
+constexpr int kTailLeave = 32768;   // the block hands back above this many
+
+__global__ void __launch_bounds__(kTailThreads) k_flip_tail(FlipCheck ck, FlipApply ap, Relinker rl, FlipReset rs,
+                                                             int *l0, int *l1, int p0, int round0, int prev0,
+                                                             int max_rounds, int leave)
+{
+    Counters *ct = ck.ct;
+    int k = 0;
+    for (; k < max_rounds; k++) {
+        const int p = (p0 + k) & 1;
+        const int n = *(volatile int *)&ct->act[p];
+        if (n == 0 || n > leave) break;
+        if (threadIdx.x == 0) FlipRoundStart{p, ct}(0);
+        __syncthreads();
+        const int round = round0 + k;
+        ck.act = p ? l1 : l0;
+        ck.prev_round = k ? round - 1 : prev0;
+        for (int i = threadIdx.x; i < n; i += kTailThreads) ck(i);
+        __syncthreads();
+        const int nc = *(volatile int *)&ct->cand;
+        ap.next = p ? l0 : l1;
+        ap.next_n = &ct->act[1 - p];
+        ap.round = round;
+        for (int i = threadIdx.x; i < nc; i += kTailThreads) ap(i);
+        __syncthreads();
+        const int nr = *(volatile int *)&ct->nrec;
+        rl.round = round;
+        for (int i = threadIdx.x; i < nr; i += kTailThreads) rl(i);
+        for (int i = threadIdx.x; i < nc; i += kTailThreads) rs(i);  // independent of the relinks
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) ct->tail_rounds = k;
+}
+
 struct AllAlive {
     const int4 *tv;
     int *list;
@@ -1626,8 +1676,32 @@ int stage_flip(Ctx &c)
     GALPHA_CUDA(cudaMemsetAsync(c.vote, 0xff, sizeof(int) * (size_t)nt, c.stream));  // unsigned votes start at max
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
     const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
-    int rounds = 0, done = 0, prev_round = -1;
-    while (!done) {
+    int rounds = 0, prev_round = -1;
+    long long known = nt;  // active-list length at `rounds`, as last read (nt bounds the first)
+    while (known > 0) {
+        if (known <= kTailEnter) {
+            const int p = rounds & 1;
+            const int round0 = next_round(c);
+            k_flip_tail<<<1, kTailThreads, 0, c.stream>>>(
+                FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr, stamp, -1},
+                FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nullptr, nullptr, prop, target, cands,
+                          c.rec, 0, c.ctr},
+                Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, 0, c.ctr}, FlipReset{c.vote, target, cands},
+                lists[0], lists[1], p, round0, prev_round, kMaxRounds + 1 - rounds, kTailLeave);
+            count_launch();
+            GALPHA_CUDA(cudaGetLastError());
+            r = read_counters(c);
+            if (r) return r;
+            if (c.hctr->err) return c.hctr->err;
+            const int k = c.hctr->tail_rounds;
+            skip_rounds(round0, k - 1);
+            if (k > 0) prev_round = round0 + k - 1;
+            rounds += k;
+            known = c.hctr->act[rounds & 1];
+            if (known == 0) break;
+            if (rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+            if (known <= kTailLeave) return set_last_error("flip: in-block rounds stopped early"), GPUDT_ERR_TOPOLOGY;
+        }
         for (int k = 0; k < kFlipSync; k++) {
             int p = rounds & 1;
             int round = next_round(c);
@@ -1647,7 +1721,7 @@ int stage_flip(Ctx &c)
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        done = c.hctr->act[rounds & 1] == 0;
+        known = c.hctr->act[rounds & 1];
         if (rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
     }
     c.st.nFlips = c.hctr->flips_total + c.hctr->nflips;

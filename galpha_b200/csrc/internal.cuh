@@ -62,6 +62,8 @@ struct Counters {
     int qrank;       // alpha query: largest spectrum rank <= alpha (-1 if alpha < 0)
     int qpad;
     double qalpha;   // alpha query: the alpha value classified
+    int tail_rounds; // flip: rounds run by the last in-block tail launch
+    int tail_pad;
 };
 
 // Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
