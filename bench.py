@@ -18,8 +18,9 @@ Two more legs share the JSON line (rank 0, N = 1):
   batched  c4: 4096 independent sets in one batched pipeline run
            (galphaRunBatch), against plain per-set galphaRunDevice calls on
            a sample, plus end to end through galphaRunBatchHost.
-  serving  c5: a Poisson request stream served by micro-batches with
-           quantile alpha queries on the resident meshes; p50 / p99 latency.
+  serving  c5: a Poisson request stream served by continuous batching on
+           two handles (streams) with quantile alpha queries on the
+           resident meshes; p50 / p99 latency.
 
 Multi-GPU: a single DT does not shard (the flip, insertion and sort stages are
 global), so N GPUs run N independent replicas of the workload ("replicas
@@ -240,11 +241,12 @@ def batched_leg(G, D, torch, stream, reps=3):
     }
 
 
-def serving_leg(G, D, seconds, rate=2000.0):
+def serving_leg(G, D, seconds, rate=2000.0, nslots=2):
     """c5: Poisson requests (rate per s) over `seconds`, sizes log-uniform in
     [1000, 1048576], half uniform and half Gaussian clusters (the c3 blob
     recipe), each followed by alpha queries at spectrum quantiles 0.1 / 0.5 /
-    0.9 on its resident mesh; micro-batches admitted under a 120 GB budget."""
+    0.9 on its resident mesh; continuous batching on `nslots` handles that
+    share a 120 GB budget."""
     import numpy as np
     from galpha_b200 import serving as S
 
@@ -256,17 +258,19 @@ def serving_leg(G, D, seconds, rate=2000.0):
     bounds = G.Engine.batch_bounds(pool)  # the clients' GPUDTPARAMS bounds
     arrivals = S.poisson_arrivals(rate, seconds, 77)
     pick = rng.integers(0, len(pool), len(arrivals))
-    eng = G.Engine()
+    slots = [G.Engine() for _ in range(nslots)]
     warm = [S.Request(i, 0.0, pool[i], bounds=bounds[i]) for i in range(len(pool))]
-    S.Server(eng).run(warm)
+    S.Server(slots, hbm_budget=120e9).run(warm)
     reqs = [S.Request(i, t, pool[pick[i]], bounds=bounds[pick[i]]) for i, t in enumerate(arrivals)]
-    srv = S.Server(eng, hbm_budget=120e9)
+    srv = S.Server(slots, hbm_budget=120e9)
     srv.run(reqs)
-    eng.close()
+    for e in slots:
+        e.close()
     out = S.summary(reqs, srv.batches)
     out["config"] = {"workload": "c5: Poisson %.0f req/s for %.1f s (of the 60 s stream), sizes log-uniform in "
                                  "[1000, 1048576], 50/50 uniform / Gaussian clusters, 3 quantile queries per request, "
-                                 "120 GB admission budget" % (rate, seconds), "pool_sets": len(pool)}
+                                 "120 GB admission budget" % (rate, seconds), "pool_sets": len(pool),
+                     "slots": nslots}
     out["offered_mpoints_per_s"] = float(sum(len(r.points) for r in reqs) / seconds / 1e6)
     return out
 

@@ -166,6 +166,9 @@ static int ensure_sizes(HandleState &H, const Sizes &z)
     plan(z, &c, &H.arena);
     c.cap_tris = (int)z.cap;
     // per-call initialisation of the slot state
+    // round ids restart well before the int range ends; every stage that
+    // compares stamps with round ids initialises its stamps first
+    if (c.round_counter > (1 << 30)) c.round_counter = 1;
     GALPHA_CUDA(cudaMemsetAsync(c.epoch, 0, sizeof(int) * z.cap, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vote, 0x7f, sizeof(int) * z.cap, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.ctr, 0, sizeof(Counters), c.stream));

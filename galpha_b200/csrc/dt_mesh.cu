@@ -35,6 +35,7 @@
 // a triangle owned by another operation of the same round.
 #include <cstdio>
 #include <algorithm>
+#include <mutex>
 #include "internal.cuh"
 #include "exact.cuh"
 
@@ -270,17 +271,18 @@ static int run_relink(Ctx &c, int round, int nrec)
     return GPUDT_OK;
 }
 
-// Host-side epoch counter: every operation round gets a fresh id.
-static thread_local int g_round_counter = 1;
-static int next_round(Ctx &)
+// Every operation round gets a fresh id from the handle's counter (the
+// round-stamped arrays belong to the handle's arena, so ids must not repeat
+// on a handle, whichever thread drives it).
+static int next_round(Ctx &c)
 {
-    return ++g_round_counter;
+    return ++c.round_counter;
 }
 // Marks the k ids after `first` (first + 1 .. first + k) as used by rounds
 // that device code numbered itself.
-static void skip_rounds(int first, int k)
+static void skip_rounds(Ctx &c, int first, int k)
 {
-    if (first + k > g_round_counter) g_round_counter = first + k;
+    if (first + k > c.round_counter) c.round_counter = first + k;
 }
 
 // ------------------------------------------------------------------- shift
@@ -1223,12 +1225,16 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
 
 static int launch_fake_remove(Ctx &c, const FakeRemoveArgs &a, const int *n_dev, int max_n)
 {
-    static bool attr_set[64];
-    const int dv = c.device >= 0 && c.device < 64 ? c.device : 0;
-    if (!attr_set[dv]) {
-        GALPHA_CUDA(cudaFuncSetAttribute(k_fake_remove, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fake_remove_smem(kMaxFanLong)));
-        attr_set[dv] = true;
+    {
+        static std::mutex mu;
+        static bool attr_set[64];
+        const int dv = c.device >= 0 && c.device < 64 ? c.device : 0;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!attr_set[dv]) {
+            GALPHA_CUDA(cudaFuncSetAttribute(k_fake_remove, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)fake_remove_smem(kMaxFanLong)));
+            attr_set[dv] = true;
+        }
     }
     const int blocks = std::max(1, std::min(max_n, c.sm_count * 16));
     k_fake_remove<<<blocks, 32, fake_remove_smem(kMaxChain), c.stream>>>(a, n_dev, kMaxChain, 0);
@@ -1416,6 +1422,9 @@ int stage_boundary(Ctx &c)
     if (r) return r;
     int ncand = c.hctr->nlist2;
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+    // per-vertex stamps of the convexify rounds: this arena region may hold
+    // another stage's data (or a differently planned call's)
+    GALPHA_CUDA(cudaMemsetAsync(c.stamp, 0xff, sizeof(int) * (size_t)c.V, c.stream));
     launch_n(c, ReflexCheck{c.tv, c.tn, c.pos, c.vtri, cand, c.vstate, c.list, c.stamp, next_round(c), c.ctr}, ncand);
     r = read_counters(c);
     if (r) return r;
@@ -1694,7 +1703,7 @@ int stage_flip(Ctx &c)
             if (r) return r;
             if (c.hctr->err) return c.hctr->err;
             const int k = c.hctr->tail_rounds;
-            skip_rounds(round0, k - 1);
+            skip_rounds(c, round0, k - 1);
             if (k > 0) prev_round = round0 + k - 1;
             rounds += k;
             known = c.hctr->act[rounds & 1];

@@ -163,6 +163,7 @@ struct Ctx {
     bool have_mesh = false, have_alpha = false;
     int sort_passes = 0;  // radix passes of the last radix_sort call
     bool fused_done = false;  // triangles came from the fused colour + dual kernel
+    int round_counter = 1;    // ids of operation rounds (per handle: stamps live in its arena)
 };
 
 // ------------------------------------------------------------- error helpers

@@ -10,6 +10,7 @@
 // from __match_any_sync, stable) and then writes each digit's run to its
 // global offset, so consecutive threads store consecutive addresses.
 #include <algorithm>
+#include <mutex>
 #include "internal.cuh"
 
 namespace galpha {
@@ -160,12 +161,16 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
     if (n <= 1) return GPUDT_OK;
     static_assert(sizeof(K) == 4 || sizeof(K) == 8, "32- or 64-bit keys");
     const int smem = (int)sizeof(RsSmem<K>);
-    static bool attr_set[64];  // per key type and device: the opt-in above 48 KB, once
-    if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
-        GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         cudaSharedmemCarveoutMaxShared));
-        if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+    {
+        static std::mutex mu;
+        static bool attr_set[64];  // per key type and device: the opt-in above 48 KB, once
+        std::lock_guard<std::mutex> lk(mu);
+        if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
+            GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             cudaSharedmemCarveoutMaxShared));
+            if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+        }
     }
     K *acc = reinterpret_cast<K *>(scratch);
     GALPHA_CUDA(cudaMemcpyAsync(acc, keys, sizeof(K), cudaMemcpyDeviceToDevice, c.stream));

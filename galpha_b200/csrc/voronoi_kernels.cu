@@ -1,6 +1,7 @@
 // voronoi_kernels.cu -- block-level kernels of the discrete Voronoi stage:
 // the column pass, the per-row lower envelope + colouring, and the 2x2-window
 // triangle emission.  Launchers are called from dt_grid.cu.
+#include <mutex>
 #include "internal.cuh"
 
 namespace galpha {
@@ -832,11 +833,18 @@ int launch_row_pass_cells(Ctx &c, int cells, const int *cellmap)
 {
     const int T = c.T;
     size_t sm = sizeof(int16_t) * (3 * (size_t)T + (T & 1)) + sizeof(int) * (size_t)T;
-    static int configured[64];
-    const int dv = c.device >= 0 && c.device < 64 ? c.device : 0;
-    if (configured[dv] < (int)sm) {
-        GALPHA_CUDA(cudaFuncSetAttribute(k_row_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        configured[dv] = (int)sm;
+    {
+        // once per device, for the largest texture (16384): a per-size setting
+        // would race between handles driven from different threads
+        static std::mutex mu;
+        static bool configured[64];
+        const size_t smax = sizeof(int16_t) * 3 * 16384 + sizeof(int) * 16384;
+        const int dv = c.device >= 0 && c.device < 64 ? c.device : 0;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!configured[dv]) {
+            GALPHA_CUDA(cudaFuncSetAttribute(k_row_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+            configured[dv] = true;
+        }
     }
     kev_record(c, 0);
     k_row_pass<<<dim3(T, cells), kRowThreads, sm, c.stream>>>(c.ycol, c.idmap, c.colour, T, c.logT, cellmap);

@@ -83,3 +83,87 @@ def test_fifo_and_latency_accounting():
     assert len(order) == 5
     for r in reqs:
         assert abs(r.latency - (r.done - r.arrival)) < 1e-12 and r.latency > 0
+
+
+class SleepEngine:
+    """A slot that takes real time (5 ms + 0.1 us per point) per batch; records
+    how many slots were busy at once."""
+
+    busy = 0
+    peak = 0
+    lock = None
+
+    def __init__(self, fail=False):
+        self.batches = []
+        self.fail = fail
+
+    def run_batch(self, sets, bounds=None):
+        import time
+
+        assert bounds is not None and len(bounds) == len(sets)
+        with SleepEngine.lock:
+            SleepEngine.busy += 1
+            SleepEngine.peak = max(SleepEngine.peak, SleepEngine.busy)
+        try:
+            if self.fail:
+                raise RuntimeError("slot failed")
+            time.sleep(5e-3 + 1e-7 * sum(len(p) for p in sets))
+            self.batches.append([len(p) for p in sets])
+            self._last = [len(p) for p in sets]
+        finally:
+            with SleepEngine.lock:
+                SleepEngine.busy -= 1
+
+    def batch_query(self, values, by_quantile=False):
+        return [(n, v) for n, v in zip(self._last, values)]
+
+
+def _reset_sleep_engines():
+    import threading
+
+    SleepEngine.busy = SleepEngine.peak = 0
+    SleepEngine.lock = threading.Lock()
+
+
+def test_slots_overlap_and_serve_every_request_once():
+    _reset_sleep_engines()
+    slots = [SleepEngine(), SleepEngine(), SleepEngine()]
+    rng = np.random.default_rng(3)
+    reqs = [S.Request(i, 0.0 if i < 12 else 0.002 * i, np.zeros((int(rng.integers(100, 3000)), 2)))
+            for i in range(40)]
+    srv = S.Server(slots, max_batch_points=4000)
+    srv.run(reqs)
+    # every request answered exactly once, by the batch that held it
+    assert all(r.done is not None and r.done >= r.start >= r.arrival - 1e-9 for r in reqs)
+    assert all([x for x in r.results] == [(len(r.points), q) for q in (0.1, 0.5, 0.9)] for r in reqs)
+    served = sorted(n for e in slots for b in e.batches for n in b)
+    assert served == sorted(len(r.points) for r in reqs)
+    assert all(sum(b) <= 4000 or len(b) == 1 for e in slots for b in e.batches)
+    # the burst at t = 0 kept several slots busy at once, and batch intervals overlap
+    assert SleepEngine.peak >= 2
+    iv = sorted((b[0], b[1], b[4]) for b in srv.batches)
+    assert any(a[2] != b[2] and b[0] < a[1] for a, b in zip(iv, iv[1:]))
+    assert len({b[4] for b in srv.batches}) >= 2
+
+
+def test_slot_budget_share():
+    _reset_sleep_engines()
+    slots = [SleepEngine(), SleepEngine()]
+    reqs = [S.Request(i, 0.0, np.zeros((3000, 2))) for i in range(8)]
+    srv = S.Server(slots, hbm_budget=2 * 7000 * S.BYTES_PER_POINT, max_batch_points=10**9)
+    assert srv.max_points == 7000
+    srv.run(reqs)
+    assert all(sum(b) <= 7000 for e in slots for b in e.batches)
+    assert sum(len(b) for e in slots for b in e.batches) == 8
+
+
+def test_failing_slot_raises_after_the_others_finish():
+    import pytest
+
+    _reset_sleep_engines()
+    slots = [SleepEngine(), SleepEngine(fail=True)]
+    reqs = [S.Request(i, 0.0, np.zeros((2000, 2))) for i in range(6)]
+    srv = S.Server(slots, max_batch_points=2000)
+    with pytest.raises(RuntimeError, match="slot failed"):
+        srv.run(reqs)
+    assert SleepEngine.busy == 0
