@@ -153,6 +153,8 @@ def load(path=None):
     L.galphaTriangulate.argtypes = [vp, ctypes.POINTER(_Params), ctypes.POINTER(_Output), ctypes.POINTER(Status)]
     L.galphaComputeResident.argtypes = [vp, ctypes.POINTER(_AlphaOut)]
     L.galphaCompute.argtypes = [vp, ctypes.POINTER(_Params), ctypes.POINTER(_Output), ctypes.POINTER(_AlphaOut)]
+    L.galphaComputeAll.argtypes = [vp, ctypes.POINTER(_Params), ctypes.POINTER(_Output), ctypes.POINTER(_AlphaOut),
+                                   ctypes.POINTER(Status)]
     L.galphaRunDevice.argtypes = [vp, vp, ip, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_double, ip, ip, ctypes.POINTER(Status)]
     L.galphaGetCounts.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
@@ -334,6 +336,26 @@ class Engine:
         out, bufs = self._alpha_bufs(self._npoints, nt)
         _check(self._L.galphaComputeResident(self._h, ctypes.byref(out)), "galphaComputeResident")
         return self._alpha_result(out, bufs, copy)
+
+    def compute_all(self, params, copy=True):
+        """DT + alpha spectrum of params in one call (galphaComputeAll): returns
+        (DTOutput, alpha result dict).  The triangles are downloaded while the
+        alpha stage runs.  With copy=False the arrays are views of reused pinned
+        buffers, valid until the next call on this engine."""
+        self._batch_active = False
+        cp = params._c()
+        n = params.nPoints
+        buf = self._pool.get("tri", 2 * n + 64, TRIANGLE_DTYPE)
+        o = _Output()
+        o.triangles = buf.ctypes.data
+        o.nTris = len(buf)
+        out, bufs = self._alpha_bufs(n, len(buf))
+        st = Status()
+        _check(self._L.galphaComputeAll(self._h, ctypes.byref(cp), ctypes.byref(o), ctypes.byref(out),
+                                        ctypes.byref(st)), "galphaComputeAll")
+        self._npoints = n
+        arr = buf[: o.nTris]
+        return DTOutput(arr.copy() if copy else arr, st), self._alpha_result(out, bufs, copy)
 
     def alpha_of(self, params, dt, copy=True):
         """Alpha spectrum + intervals of a given triangulation (Alpha_Shapes_2D(pInput, pDT))."""

@@ -556,10 +556,8 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
         if (r) return r;
         unsigned long long *tk = (unsigned long long *)c.spectrum;
         launch_n(c, GatherEntries{c.keys + 1, c.vals + 1, c.vals2, ka, tk, c.rank, segs->seg}, m);
-        GALPHA_CUDA(cudaMemcpyAsync(c.keys + 1, tk, sizeof(unsigned long long) * (size_t)m,
-                                    cudaMemcpyDeviceToDevice, c.stream));
-        GALPHA_CUDA(cudaMemcpyAsync(c.vals + 1, c.rank, sizeof(int) * (size_t)m, cudaMemcpyDeviceToDevice,
-                                    c.stream));
+        launch_n(c, CopyElems<unsigned long long>{c.keys + 1, tk}, m);
+        launch_n(c, CopyElems<int>{c.vals + 1, c.rank}, m);
     }
     // ranks
     int *nr = c.aux, *unc = c.list, *slow = c.list2, *slowflag = c.stamp;

@@ -28,10 +28,40 @@ int cuda_fail(cudaError_t e, const char *what)
 const char *last_error_text() { return g_err.c_str(); }
 void set_last_error(const char *text) { g_err = text; }
 
+// Device words to mapped host memory.  The stores travel as PCIe writes of
+// the SMs, not through a copy engine, so a pipeline's counter reads do not
+// wait for result downloads queued by this or another handle.
+__global__ void k_read_words(const unsigned *__restrict__ src, unsigned *dst, int nwords)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += gridDim.x * blockDim.x) dst[i] = src[i];
+    __threadfence_system();
+}
+
 int read_counters(Ctx &c)
 {
-    GALPHA_CUDA(cudaMemcpyAsync(c.hctr, c.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, c.stream));
+    static_assert(sizeof(Counters) % 4 == 0, "counter block is read as 32-bit words");
+    const int nw = (int)(sizeof(Counters) / 4);
+    k_read_words<<<1, 256, 0, c.stream>>>((const unsigned *)c.ctr, (unsigned *)c.hctr_dev, nw);
+    count_launch();
+    GALPHA_CUDA(cudaGetLastError());
     GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    return GPUDT_OK;
+}
+
+int read_small(Ctx &c, void *host_dst, const void *dev_src, size_t bytes)
+{
+    if (bytes == 0) return GPUDT_OK;
+    if (bytes > kMailBytes || (bytes & 3) || ((uintptr_t)dev_src & 3)) {
+        GALPHA_CUDA(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, c.stream));
+        GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+        return GPUDT_OK;
+    }
+    const int nw = (int)(bytes / 4);
+    k_read_words<<<(nw + 255) / 256, 256, 0, c.stream>>>((const unsigned *)dev_src, (unsigned *)c.hmail_dev, nw);
+    count_launch();
+    GALPHA_CUDA(cudaGetLastError());
+    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    memcpy(host_dst, c.hmail, bytes);
     return GPUDT_OK;
 }
 
@@ -128,6 +158,8 @@ struct HandleState {
     BatchDev bd;
     double *d_xy = nullptr;
     size_t d_xy_cap = 0;
+    cudaStream_t side = nullptr;  // downloads that overlap later stages (galphaComputeAll)
+    cudaEvent_t side_ev = nullptr;
 };
 
 static int ensure_sizes(HandleState &H, const Sizes &z);
@@ -434,8 +466,18 @@ static int handle_init(galpha_ctx *h, int device, long long budget)
     c.budget = budget;
     GALPHA_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.own_stream = true;
-    GALPHA_CUDA(cudaMallocHost(&c.hctr, sizeof(Counters)));
-    memset(c.hctr, 0, sizeof(Counters));
+    {
+        // counter mirror + mailbox: pinned, mapped into the device's address space
+        const size_t ctr_bytes = (sizeof(Counters) + 255) & ~(size_t)255;
+        void *hp = nullptr, *dp = nullptr;
+        GALPHA_CUDA(cudaHostAlloc(&hp, ctr_bytes + kMailBytes, cudaHostAllocMapped));
+        memset(hp, 0, ctr_bytes + kMailBytes);
+        GALPHA_CUDA(cudaHostGetDevicePointer(&dp, hp, 0));
+        c.hctr = (Counters *)hp;
+        c.hctr_dev = (Counters *)dp;
+        c.hmail = (char *)hp + ctr_bytes;
+        c.hmail_dev = (char *)dp + ctr_bytes;
+    }
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2; k++) GALPHA_CUDA(cudaEventCreate(&c.ev[k]));
     for (int k = 0; k < 10; k++) GALPHA_CUDA(cudaEventCreate(&c.kev[k]));
     c.events = true;
@@ -481,6 +523,11 @@ int galphaDestroy(galphaHandle h)
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2 && c.events; k++) cudaEventDestroy(c.ev[k]);
     for (int k = 0; k < 10 && c.events; k++) cudaEventDestroy(c.kev[k]);
     if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+    if (h->H.side) {
+        cudaStreamSynchronize(h->H.side);
+        cudaStreamDestroy(h->H.side);
+    }
+    if (h->H.side_ev) cudaEventDestroy(h->H.side_ev);
     delete h;
     return GPUDT_OK;
 }
@@ -776,6 +823,80 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
     if (r) return r;
     c.have_alpha = true;
     return download_alpha(c, out);
+}
+
+// gpudtComputeDT + Alpha_Shapes_2D in one call with host outputs: the
+// triangles are copied back on a second stream while the alpha stage runs on
+// the handle's stream, so their transfer overlaps the alpha computation.
+int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt, GAlphaOutput *out, gpudtStatus *st)
+{
+    if (!h || !dt || !out) return GPUDT_ERR_ARG;
+    int r = check_params(params);
+    if (r) return r;
+    std::lock_guard<std::mutex> lk(h->mu);
+    HandleState &H = h->H;
+    Ctx &c = H.c;
+    cudaSetDevice(c.device);
+    cudaGetLastError();  // clear an error left by unrelated runtime calls
+    if (!H.side) {
+        GALPHA_CUDA(cudaStreamCreateWithFlags(&H.side, cudaStreamNonBlocking));
+        GALPHA_CUDA(cudaEventCreateWithFlags(&H.side_ev, cudaEventDisableTiming));
+    }
+    ev_record(c, 0);
+    r = upload_points(H, params->points, params->nPoints);
+    if (!r)
+        r = run_dt(H, H.d_xy, params->nPoints, params->minX, params->minY, params->maxX, params->maxY,
+                   params->fboSize);
+    gpudtTriangle *tris = nullptr;
+    bool owned = false, copying = false;
+    if (!r) {
+        const int n = params->nPoints;
+        if (dt->triangles) {
+            if (dt->nTris < c.nT_out) {
+                g_err = "galphaComputeAll: triangle buffer too small";
+                r = GPUDT_ERR_NOMEM;
+            } else {
+                tris = dt->triangles;
+            }
+        } else {
+            int nv = n + std::max(4, (int)(std::sqrt((double)n) / 10));
+            int capacity = std::max(2 * nv, c.nT_out);
+            tris = new (std::nothrow) gpudtTriangle[capacity > 0 ? capacity : 1];
+            owned = true;
+            if (!tris) r = GPUDT_ERR_NOMEM;
+        }
+    }
+    if (!r && c.nT_out > 0) {
+        cudaError_t e = cudaEventRecord(H.side_ev, c.stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(H.side, H.side_ev, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(tris, c.outtri, sizeof(gpudtTriangle) * (size_t)c.nT_out, cudaMemcpyDeviceToHost,
+                                H.side);
+        if (e != cudaSuccess) r = cuda_fail(e, "galphaComputeAll: download triangles");
+        else copying = true;
+    }
+    if (!r) {
+        ev_record(c, 8);
+        r = stage_alpha(c);
+        if (!r) c.have_alpha = true;
+        ev_record(c, 9);
+    }
+    if (!r) r = download_alpha(c, out);
+    if (copying) {
+        // the side copy reads c.outtri: wait for it whatever happened above
+        cudaError_t e = cudaStreamSynchronize(H.side);
+        if (!r && e != cudaSuccess) r = cuda_fail(e, "galphaComputeAll: download triangles");
+    }
+    if (!r) {
+        dt->triangles = tris;
+        dt->nTris = c.nT_out;
+        fill_times(c, 9);
+    } else if (owned) {
+        delete[] tris;
+    }
+    c.st.status = r;
+    if (st) *st = c.st;
+    return r;
 }
 
 int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double *d_xy, const double *bounds,

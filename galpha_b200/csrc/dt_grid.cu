@@ -299,14 +299,14 @@ int has_triangles(Ctx &c, const double *d_xy, int n)
 {
     if (n < 3) return 0;
     int *first = c.aux;
-    int big = 0x7fffffff;
-    GALPHA_CUDA(cudaMemcpyAsync(first, &big, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    const int big = 0x7f7f7f7f;  // above every point index
+    GALPHA_CUDA(cudaMemsetAsync(first, 0x7f, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
     launch_n(c, FirstDistinct{d_xy, first}, n);
     int hfirst = 0;
-    GALPHA_CUDA(cudaMemcpyAsync(&hfirst, first, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
-    if (hfirst == 0x7fffffff) return 0;
+    int rr = read_small(c, &hfirst, first, sizeof(int));
+    if (rr) return rr;
+    if (hfirst == big) return 0;
     launch_n(c, CountOffLine{d_xy, first, c.ctr}, n);
     int r = read_counters(c);
     if (r) return r;
@@ -341,9 +341,7 @@ int cell_occupancy(Ctx &c, const uint32_t *bandocc, int T, int W2, int cells, in
     if (nb <= 2) return GPUDT_OK;
     GALPHA_CUDA(cudaMemsetAsync(dev, 0, sizeof(int) * (size_t)cells, c.stream));
     launch_n(c, CellOccupancy{bandocc, T, W2, nb, dev}, (long long)cells * (nb - 2) * (nb - 2));
-    GALPHA_CUDA(cudaMemcpyAsync(host, dev, sizeof(int) * (size_t)cells, cudaMemcpyDeviceToHost, c.stream));
-    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
-    return GPUDT_OK;
+    return read_small(c, host, dev, sizeof(int) * (size_t)cells);
 }
 
 // The fused path pays a window scan as long as the distance to the nearest
@@ -513,9 +511,8 @@ int emit_global(Ctx &c, int base, int cells, const int *cellmap)
     if ((long long)base + total > c.cap_tris) return GPUDT_ERR_NOMEM;
     r = launch_emit_cells(c, ntiles, nwin, true, c.tv + base, cells, cellmap);
     if (r) return r;
-    const int nt = base + total;
-    GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->ntris, &nt, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-    GALPHA_CUDA(cudaStreamSynchronize(c.stream));  // nt lives on this stack frame
+    launch_n(c, SetInt{&c.ctr->ntris, base + total}, 1);
+    GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
 }
 

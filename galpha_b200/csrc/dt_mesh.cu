@@ -940,10 +940,7 @@ int stage_missing(Ctx &c)
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        if (c.hctr->nfree < 0) {
-            int z = 0;
-            GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->nfree, &z, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-        }
+        if (c.hctr->nfree < 0) GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nfree, 0, sizeof(int), c.stream));
         if (c.hctr->ntris > c.cap_tris) return GPUDT_ERR_NOMEM;
         r = run_relink(c, round, c.hctr->nrec);
         if (r) return r;
@@ -1447,10 +1444,7 @@ int stage_boundary(Ctx &c)
         n = c.hctr->nlist2;
         std::swap(lin, lout);
     }
-    if (c.hctr->nfree < 0) {
-        int z = 0;
-        GALPHA_CUDA(cudaMemcpyAsync(&c.ctr->nfree, &z, sizeof(int), cudaMemcpyHostToDevice, c.stream));
-    }
+    if (c.hctr->nfree < 0) GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nfree, 0, sizeof(int), c.stream));
     return GPUDT_OK;
 }
 

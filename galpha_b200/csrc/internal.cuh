@@ -124,7 +124,9 @@ struct Ctx {
     int *inc = nullptr;        // [3*cap]
     int *tilecount = nullptr;  // [ntiles + 1]
     Counters *ctr = nullptr;   // device counters
-    Counters *hctr = nullptr;  // pinned host mirror
+    Counters *hctr = nullptr;  // pinned, device-mapped host mirror of ctr (written by a kernel)
+    Counters *hctr_dev = nullptr;  // the device address of hctr
+    char *hmail = nullptr, *hmail_dev = nullptr;  // mapped mailbox for other small reads
 
     // alpha arrays
     int nT_out = 0, nE = 0, nSpecIn = 0, nSpec = 0;
@@ -180,6 +182,11 @@ void set_last_error(const char *text);
 // Reserve device buffers for V vertices, T texture, cap triangles.
 int reserve(Ctx &c, int V, int T, int cap_tris, bool alpha);
 int read_counters(Ctx &c);
+// Small device -> host read (bytes a multiple of 4, src 4-byte aligned): a
+// kernel writes into mapped pinned memory, so the read never queues behind
+// large copies on the copy engines; synchronises the handle's stream.
+int read_small(Ctx &c, void *host_dst, const void *dev_src, size_t bytes);
+constexpr size_t kMailBytes = 65536;
 
 // Kernel launches issued by this library (all handles, all threads).
 extern unsigned long long g_launches;
@@ -228,6 +235,21 @@ inline void launch_n(const Ctx &c, F f, long long n)
     count_launch();
 }
 #endif
+
+// Element copies and single-word stores as kernels: on the handle's stream
+// they never wait behind downloads that the copy engines are busy with.
+template <typename T>
+struct CopyElems {
+    T *dst;
+    const T *src;
+    __device__ void operator()(long long i) const { dst[i] = src[i]; }
+};
+
+struct SetInt {
+    int *p;
+    int v;
+    __device__ void operator()(long long) const { *p = v; }
+};
 
 // Report the first error from device code.
 __device__ __forceinline__ void set_err(Counters *ct, int code, int info)

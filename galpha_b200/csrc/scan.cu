@@ -123,7 +123,7 @@ int exclusive_scan_int(Ctx &c, const int *in, int *out, int n, int *total_dev)
     int *scratch = c.hist;  // scan scratch lives at the start of the histogram buffer
     if (total_dev) {
         // keep the last input before an in-place scan overwrites it
-        GALPHA_CUDA(cudaMemcpyAsync(scratch, in + n - 1, sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+        launch_n(c, CopyElems<int>{scratch, in + n - 1}, 1);
     }
     int r = scan_rec(c, in, out, n, scratch + 16);
     if (r) return r;

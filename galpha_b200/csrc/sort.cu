@@ -173,7 +173,7 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
         }
     }
     K *acc = reinterpret_cast<K *>(scratch);
-    GALPHA_CUDA(cudaMemcpyAsync(acc, keys, sizeof(K), cudaMemcpyDeviceToDevice, c.stream));
+    launch_n(c, CopyElems<K>{acc, keys}, 1);
     GALPHA_CUDA(cudaMemsetAsync(acc + 1, 0, sizeof(K), c.stream));
     {
         long long blocks = std::min<long long>((n + 255) / 256, (long long)c.sm_count * 4);
@@ -181,8 +181,8 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
         count_launch();
     }
     K hv[2];
-    GALPHA_CUDA(cudaMemcpyAsync(hv, acc, sizeof(hv), cudaMemcpyDeviceToHost, c.stream));
-    GALPHA_CUDA(cudaStreamSynchronize(c.stream));
+    int rr = read_small(c, hv, acc, sizeof(hv));
+    if (rr) return rr;
     const unsigned long long varying = (unsigned long long)hv[1];
     const int nblocks = (n + kRsTile - 1) / kRsTile;
     int *hist = scratch + 8;
@@ -202,8 +202,8 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
         std::swap(vi, vo);
     }
     if (ki != keys) {
-        GALPHA_CUDA(cudaMemcpyAsync(keys, ki, sizeof(K) * (size_t)n, cudaMemcpyDeviceToDevice, c.stream));
-        GALPHA_CUDA(cudaMemcpyAsync(vals, vi, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, c.stream));
+        launch_n(c, CopyElems<K>{keys, ki}, n);
+        launch_n(c, CopyElems<int>{vals, vi}, n);
     }
     return GPUDT_OK;
 }

@@ -90,6 +90,14 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
  * galphaReleaseOutput. */
 int galphaComputeResident(galphaHandle h, GAlphaOutput *out);
 
+/* gpudtComputeDT followed by Alpha_Shapes_2D + computeAlphaShapes
+ * (main.cu:392-395) in one call: dt receives the triangles (same rules as
+ * galphaTriangulate's out), out the alpha arrays (same rules as
+ * galphaComputeResident).  The triangles travel to the host while the alpha
+ * stage runs. */
+int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt, GAlphaOutput *out,
+                     gpudtStatus *st);
+
 /* Alpha spectrum + intervals of a host triangulation (Alpha_Shapes_2D(pInput, pDT)). */
 int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *dt, GAlphaOutput *out);
 

@@ -82,3 +82,34 @@ def test_large_alpha_properties(engine):
     assert ro.min() >= 1 and ro.max() < len(s)
     e = a["edge_list"]
     assert e["ro_rank"].max() < len(s) and (e["nu_min_rank"] <= np.where(e["nu_max_rank"] == 0, 1 << 30, e["nu_max_rank"])).all()
+
+
+@pytest.mark.parametrize("n,seed", [(20000, 21), (300000, 22)])
+def test_compute_all_matches_two_calls(engine, n, seed):
+    """galphaComputeAll (triangles downloaded while the alpha stage runs) gives
+    the mesh of galphaTriangulate and, for its own triangle order, exactly the
+    alpha arrays of galphaCompute on that mesh.  (Triangle slots are handed
+    out by atomics, so the order of the triangles, and with it the edge
+    numbering, may differ between runs; the triangle set may not.)"""
+    from alphacheck import canonical_alpha
+    from dtcheck import canon_set
+
+    pts = np.random.default_rng(seed).random((n, 2)) if seed % 2 else D.gaussian_blobs(n, seed)
+    p = G.GPUDTParams(pts, fboSize=2048)
+    dt1 = engine.triangulate(p)
+    a1 = engine.alpha_resident()
+    dt2, a2 = engine.compute_all(p)
+    assert dt2.nTris == dt1.nTris and canon_set(dt2.vtx) == canon_set(dt1.vtx)
+    b = engine.alpha_of(p, dt2)
+    for k in ("spectrum", "point_list", "edge_list", "tri_list"):
+        assert np.array_equal(a2[k], b[k]), k
+    c1, c2 = canonical_alpha(dt1.vtx, a1), canonical_alpha(dt2.vtx, a2)
+    assert np.array_equal(c1[0], c2[0]) and np.array_equal(c1[3], c2[3])
+    assert c1[1] == c2[1] and c1[2] == c2[2]
+    if n <= 20000:
+        ok, rep = compare_alpha(pts, dt2.vtx, dt2.tri, a2, ULP_TOL)
+        assert ok, rep
+    # pinned views (copy=False) hold a complete result until the next call
+    dt3, a3 = engine.compute_all(p, copy=False)
+    assert canon_set(dt3.vtx) == canon_set(dt1.vtx)
+    assert np.array_equal(a3["spectrum"], a1["spectrum"])
