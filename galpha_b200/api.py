@@ -440,21 +440,27 @@ class Engine:
         _check(self._L.galphaBatchSets(self._h, arr), "galphaBatchSets")
         return arr
 
-    def batch_results(self):
+    def batch_results(self, copy=True):
         """Per-set results of the last batch: list of dicts with ``triangles``
         (TRIANGLE_DTYPE, set-local indices) and, with alpha, ``spectrum``,
-        ``point_list``, ``edge_list``, ``tri_list``."""
+        ``point_list``, ``edge_list``, ``tri_list``.  With copy=False the arrays
+        are views of reused pinned buffers (one DMA copy each), valid until the
+        next batch_results call on this engine."""
         k, alpha = self._batch
         sets = self.batch_sets()
         nt = sum(s.nTris for s in sets)
         npt = sum(s.nPoints for s in sets)
         ne = sum(s.nEdges for s in sets)
         nsp = sum(s.nSpectrum for s in sets)
-        tri = np.empty(nt, TRIANGLE_DTYPE)
-        pt = np.empty(npt, POINT_INTERVAL_DTYPE) if alpha else None
-        ed = np.empty(ne, EDGE_INTERVAL_DTYPE) if alpha else None
-        tr = np.empty(nt, TRIANGLE_INTERVAL_DTYPE) if alpha else None
-        sp = np.empty(nsp, np.float64) if alpha else None
+        if copy:
+            new = lambda name, m, dt: np.empty(m, dt)
+        else:
+            new = lambda name, m, dt: self._pool.get(name, m, dt)[:m]
+        tri = new("b_tri", nt, TRIANGLE_DTYPE)
+        pt = new("b_pt", npt, POINT_INTERVAL_DTYPE) if alpha else None
+        ed = new("b_edge", ne, EDGE_INTERVAL_DTYPE) if alpha else None
+        tr = new("b_trilist", nt, TRIANGLE_INTERVAL_DTYPE) if alpha else None
+        sp = new("b_spec", nsp, np.float64) if alpha else None
         ptr = lambda a: a.ctypes.data if a is not None and len(a) else None
         _check(self._L.galphaBatchCopy(self._h, ptr(tri), ptr(pt), ptr(ed), ptr(tr), ptr(sp)), "galphaBatchCopy")
         out = []
