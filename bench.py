@@ -180,6 +180,11 @@ def batched_leg(G, D, torch, stream, reps=3):
     eng = G.Engine()
     eng.set_stream(stream.cuda_stream)
     L = G.load()
+    # texture density tuned on another draw of the c4 distribution (a quarter of its sets)
+    from galpha_b200 import autotune
+
+    tune_sets = D.c4_sets(seed=14)[:1024]
+    density, table = autotune.tune_batch_density(eng, tune_sets, bounds=G.Engine.batch_bounds(tune_sets))
     st = eng.run_batch_device(d_xy.data_ptr(), sizes, bounds)  # warm-up (arena growth)
     torch.cuda.synchronize()
     ts = []
@@ -232,6 +237,8 @@ def batched_leg(G, D, torch, stream, reps=3):
         "value": value, "unit": UNIT, "ms_per_batch": ms, "gpu_launches": int(launches),
         "plain_per_set": {"value": plain, "unit": UNIT, "sets": len(sample), "points": npts, "ms": plain_ms},
         "speedup_vs_plain": value / plain,
+        "tuning": {"batch_density": density, "table_ms": table,
+                   "sample": "1024 sets of c4_sets(seed=14) (not the measured draw)"},
         "e2e": {"value": n / (min(te) / 1e3) / 1e6, "unit": UNIT, "ms": min(te), "h2d_bytes": int(xy.nbytes),
                 "d2h_bytes": int(d2h)},
         "stages_ms": {nm: float(st.ms[i]) for i, nm in enumerate(
@@ -259,6 +266,12 @@ def serving_leg(G, D, seconds, rate=2000.0, nslots=2):
     arrivals = S.poisson_arrivals(rate, seconds, 77)
     pick = rng.integers(0, len(pool), len(arrivals))
     slots = [G.Engine() for _ in range(nslots)]
+    from galpha_b200 import autotune
+
+    # texture density tuned on a batch of every 4th pool set, then set on every slot
+    density, _ = autotune.tune_batch_density(slots[0], pool[::4], bounds=bounds[::4], reps=1)
+    for e in slots[1:]:
+        e.set_batch_density(density)
     warm = [S.Request(i, 0.0, pool[i], bounds=bounds[i]) for i in range(len(pool))]
     S.Server(slots, hbm_budget=120e9).run(warm)
     reqs = [S.Request(i, t, pool[pick[i]], bounds=bounds[pick[i]]) for i, t in enumerate(arrivals)]
@@ -270,7 +283,7 @@ def serving_leg(G, D, seconds, rate=2000.0, nslots=2):
     out["config"] = {"workload": "c5: Poisson %.0f req/s for %.1f s (of the 60 s stream), sizes log-uniform in "
                                  "[1000, 1048576], 50/50 uniform / Gaussian clusters, 3 quantile queries per request, "
                                  "120 GB admission budget" % (rate, seconds), "pool_sets": len(pool),
-                     "slots": nslots}
+                     "slots": nslots, "batch_density": density}
     out["offered_mpoints_per_s"] = float(sum(len(r.points) for r in reqs) / seconds / 1e6)
     return out
 

@@ -166,6 +166,7 @@ def load(path=None):
     L.galphaRunBatch.argtypes = [vp, ip, vp, vp, vp, ip, ctypes.POINTER(Status)]
     L.galphaRunBatchHost.argtypes = [vp, ip, vp, vp, vp, ip, ctypes.POINTER(Status)]
     L.galphaBatchSets.argtypes = [vp, vp]
+    L.galphaSetBatchDensity.argtypes = [vp, ctypes.c_double]
     L.galphaBatchCopy.argtypes = [vp, vp, vp, vp, vp, vp]
     L.galphaBatchQuery.argtypes = [vp, vp, ip, vp]
     L.galphaMasterList.argtypes = [vp, ctypes.POINTER(_MasterOut)]
@@ -433,6 +434,12 @@ class Engine:
         self._batch = (len(sizes), bool(with_alpha))
         self._batch_active = True
         return st
+
+    def set_batch_density(self, pixels_per_point):
+        """Texture pixels per point of every set in later batches
+        (galphaSetBatchDensity; default 10, tuned by galpha_b200.autotune)."""
+        _check(self._L.galphaSetBatchDensity(self._h, float(pixels_per_point)), "galphaSetBatchDensity")
+        self._density = float(pixels_per_point)
 
     def batch_sets(self):
         k = self._batch[0]

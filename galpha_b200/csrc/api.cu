@@ -933,6 +933,14 @@ int galphaRunBatchHost(galphaHandle h, int nSets, const int *setSizes, const dou
     return galphaRunBatch(h, nSets, setSizes, h->H.d_xy, bounds, withAlpha, st);
 }
 
+int galphaSetBatchDensity(galphaHandle h, double pixelsPerPoint)
+{
+    if (!h || !(pixelsPerPoint >= 1.0 && pixelsPerPoint <= 64.0)) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->H.bh.density = pixelsPerPoint;
+    return GPUDT_OK;
+}
+
 int galphaBatchSets(galphaHandle h, galphaBatchSet *sets)
 {
     if (!h || !sets) return GPUDT_ERR_ARG;

@@ -31,12 +31,15 @@ namespace galpha {
 
 namespace {
 
-// power-of-two texture cell for n points: about 10 pixels per point, at least
-// 128 (the fused tile width), so the dense (fused) colouring path applies
-int cell_size(int n)
+// power-of-two texture cell for n points: at least `density` pixels per point
+// inside the ring margin (10 by default; a tuned value from the autotuner),
+// at least 128 (the fused tile width), so the dense (fused) colouring path
+// applies.  Fewer pixels per point mean fewer pixels to colour and more
+// points sharing a pixel (missing sites, inserted later).
+int cell_size(int n, double density)
 {
     int T = 128;
-    while (T < 16384 && (double)(T - 2 * kMargin) * (T - 2 * kMargin) < 10.0 * n) T *= 2;
+    while (T < 16384 && (double)(T - 2 * kMargin) * (T - 2 * kMargin) < density * n) T *= 2;
     return T;
 }
 
@@ -382,7 +385,9 @@ int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, 
 // which sets are degenerate.
 int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds)
 {
+    const double density = bh.density;  // a handle setting, kept across batches
     bh = BatchHost();
+    bh.density = density;
     bh.K = K;
     bh.sets.resize(K);
     long long N = 0, F = 0;
@@ -398,7 +403,7 @@ int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds)
         S.maxX = bounds[4 * s + 2];
         S.maxY = bounds[4 * s + 3];
         if (!(S.minX <= S.maxX && S.minY <= S.maxY)) return GPUDT_ERR_ARG;
-        S.T = cell_size(S.n);
+        S.T = cell_size(S.n, bh.density);
         S.logT = 0;
         while ((1 << S.logT) < S.T) S.logT++;
         S.W2 = ((S.T >> 6) + 31) / 32;

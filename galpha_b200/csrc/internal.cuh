@@ -357,6 +357,7 @@ struct BatchHost {
     long long T2 = 0, occw = 0, band = 0;
     int ntiles = 0;
     bool alpha = false, valid = false;
+    double density = 10.0;  // texture pixels per point of a set (galphaSetBatchDensity)
 };
 
 struct BatchDev {

@@ -138,6 +138,12 @@ int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double 
 /* The same from host memory (copied to the device inside the call). */
 int galphaRunBatchHost(galphaHandle h, int nSets, const int *setSizes, const double *xy, const double *bounds,
                        int withAlpha, gpudtStatus *st);
+/* Texture pixels per point of each set's cell in later batches (1 to 64;
+ * default 10).  The cell is the smallest power of two, at least 128, whose
+ * area inside the fake-site margin holds that many pixels per point; the
+ * result of a set does not depend on it, the speed does (see
+ * galpha_b200/autotune.py). */
+int galphaSetBatchDensity(galphaHandle h, double pixelsPerPoint);
 /* Per-set counts and bases of the last batch (host array of nSets). */
 int galphaBatchSets(galphaHandle h, galphaBatchSet *sets);
 /* Copy the last batch's results to host buffers sized by galphaBatchSets

@@ -130,3 +130,20 @@ def test_batch_query_matches_interval_rule(engine):
                 assert list(qr[k].nPoints) == np.bincount(wp, minlength=4).tolist()
     finally:
         beng.close()
+
+
+@pytest.mark.parametrize("density", [3.0, 24.0])
+def test_batch_density_keeps_results(engine, density):
+    """The texture density (pixels per point of a set's cell) changes how
+    many sites share a pixel, not the result."""
+    sets = _mixed_sets(4)[:12]
+    beng = G.Engine()
+    try:
+        beng.set_batch_density(density)
+        beng.run_batch(sets)
+        res = beng.batch_results()
+        with pytest.raises(G.GpudtError):
+            beng.set_batch_density(0.5)
+    finally:
+        beng.close()
+    _compare(engine, sets, res)
