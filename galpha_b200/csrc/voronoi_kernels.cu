@@ -372,33 +372,34 @@ constexpr int KT_W = 128, KT_H = 8;
 constexpr int KT_CW = KT_W + 3, KT_CH = KT_H + 3;  // coloured pixels incl. halo
 constexpr int kFusedThreads = 256;
 
+// 32-bit arithmetic throughout: T <= 16384, so k^2 + dy^2 < 2^30.  Scanning
+// outwards, a left candidate at distance k has a smaller column than every
+// earlier best (all lie within k - 1 of x), so it wins ties; a right one never
+// does -- the (d, column) order without a column compare.
 __device__ __forceinline__ unsigned owner_scan(const int16_t *__restrict__ row, int x, int y, int T)
 {
-    long long bestd = 0x7fffffffffffffffLL;
-    int bx = -1;
-    int yc = row[x];
+    int bestd = 0x7fffffff, bx = -1;
+    const int yc = row[x];
     if (yc >= 0) {
-        bestd = (long long)(y - yc) * (y - yc);
+        bestd = (y - yc) * (y - yc);
         bx = x;
     }
-    for (int k = 1; (long long)k * k <= bestd || bx < 0; k++) {
-        if (k >= T) break;
-        long long kk = (long long)k * k;
-        int xl = x - k, xr = x + k;
+    for (int k = 1; k < T && k * k <= bestd; k++) {
+        const int kk = k * k, xl = x - k, xr = x + k;
         if (xl >= 0) {
-            int c = row[xl];
+            const int c = row[xl];
             if (c >= 0) {
-                long long d = kk + (long long)(y - c) * (y - c);
-                if (d < bestd || (d == bestd && xl < bx)) {
+                const int d = kk + (y - c) * (y - c);
+                if (d <= bestd) {
                     bestd = d;
                     bx = xl;
                 }
             }
         }
         if (xr < T) {
-            int c = row[xr];
+            const int c = row[xr];
             if (c >= 0) {
-                long long d = kk + (long long)(y - c) * (y - c);
+                const int d = kk + (y - c) * (y - c);
                 if (d < bestd) {
                     bestd = d;
                     bx = xr;
@@ -406,7 +407,7 @@ __device__ __forceinline__ unsigned owner_scan(const int16_t *__restrict__ row, 
             }
         }
     }
-    int sy = row[bx];
+    const int sy = row[bx];
     return ((unsigned)sy << 16) | (unsigned)bx;
 }
 
