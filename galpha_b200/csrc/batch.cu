@@ -448,7 +448,7 @@ int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds)
         C.cells = (int)C.sets.size();
         // island pixel lists index a class's cells with 32-bit integers
         if ((long long)C.cells * T * T > 0x7fffffffLL) return GPUDT_ERR_NOMEM;
-        tiles += C.cells * (((T - 1 + 127) / 128) * ((T - 1 + 7) / 8));
+        tiles += C.cells * fused_tiles(T);
         bh.classes.push_back(C);
     }
     bh.T2 = tex;

@@ -377,6 +377,7 @@ struct BatchDev {
 void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale, double &sx, double &sy);
 void launch_compact_write(Ctx &c, const int *newidx, int nslots);
 int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds);
+int fused_tiles(int T);  // tiles of the fused colouring kernel per T x T cell
 int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, int ntiles);
 int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy);
 int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh);

@@ -368,9 +368,9 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit_write(const int *__restri
 // the column pass already kept the upper site).  Columns are visited at
 // growing distance k from x; the scan stops once k^2 exceeds the best d, which
 // no further column can beat.  This is the same assignment k_row_pass makes.
-constexpr int KT_W = 128, KT_H = 8;
+constexpr int KT_W = 128, KT_H = 16;  // 16 rows: the one-pixel halo adds 21 % to the coloured pixels, not 41 %
 constexpr int KT_CW = KT_W + 3, KT_CH = KT_H + 3;  // coloured pixels incl. halo
-constexpr int kFusedThreads = 256;
+constexpr int kFusedThreads = 512;
 
 // 32-bit arithmetic throughout: T <= 16384, so k^2 + dy^2 < 2^30.  Scanning
 // outwards, a left candidate at distance k has a smaller column than every
@@ -803,6 +803,12 @@ int launch_vd_tri_cells(Ctx &c, int T, int logT, int cells, const int16_t *ycol,
     kev_record(c, 1);
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
+}
+
+// Tiles of the fused kernel per T x T cell.
+int fused_tiles(int T)
+{
+    return ((T - 1 + KT_W - 1) / KT_W) * ((T - 1 + KT_H - 1) / KT_H);
 }
 
 // ---------------------------------------------------------------- launchers
