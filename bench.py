@@ -19,7 +19,7 @@ Two more legs share the JSON line (rank 0, N = 1):
            (galphaRunBatch), against plain per-set galphaRunDevice calls on
            a sample, plus end to end through galphaRunBatchHost.
   serving  c5: a Poisson request stream served by continuous batching on
-           two handles (streams) with quantile alpha queries on the
+           six handles (streams) with quantile alpha queries on the
            resident meshes; p50 / p99 latency.
 
 Multi-GPU: a single DT does not shard (the flip, insertion and sort stages are
@@ -248,7 +248,7 @@ def batched_leg(G, D, torch, stream, reps=3):
     }
 
 
-def serving_leg(G, D, seconds, rate=2000.0, nslots=2):
+def serving_leg(G, D, seconds, rate=2000.0, nslots=6):
     """c5: Poisson requests (rate per s) over `seconds`, sizes log-uniform in
     [1000, 1048576], half uniform and half Gaussian clusters (the c3 blob
     recipe), each followed by alpha queries at spectrum quantiles 0.1 / 0.5 /
@@ -272,10 +272,11 @@ def serving_leg(G, D, seconds, rate=2000.0, nslots=2):
     density, _ = autotune.tune_batch_density(slots[0], pool[::4], bounds=bounds[::4], reps=1)
     for e in slots[1:]:
         e.set_batch_density(density)
-    warm = [S.Request(i, 0.0, pool[i], bounds=bounds[i]) for i in range(len(pool))]
-    S.Server(slots, hbm_budget=120e9).run(warm)
     reqs = [S.Request(i, t, pool[pick[i]], bounds=bounds[pick[i]]) for i, t in enumerate(arrivals)]
     srv = S.Server(slots, hbm_budget=120e9)
+    # every slot grows its device arena and pinned staging buffers before the stream
+    srv.warm(pool, bounds=bounds)
+    S.Server(slots, hbm_budget=120e9).run([S.Request(i, 0.0, pool[i], bounds=bounds[i]) for i in range(len(pool))])
     srv.run(reqs)
     for e in slots:
         e.close()

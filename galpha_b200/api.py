@@ -255,6 +255,8 @@ class _HostPool:
         dtype = np.dtype(dtype)
         a = self._bufs.get(name)
         if a is None or len(a) < n or a.dtype != dtype:
+            if a is not None and a.dtype == dtype:
+                n = max(int(n), int(1.5 * len(a)))  # grow geometrically: pinning is slow
             nbytes = max(1, int(n) * dtype.itemsize)
             if self._torch is not None:
                 t = self._torch.empty(nbytes, dtype=self._torch.uint8, pin_memory=True)
@@ -264,6 +266,30 @@ class _HostPool:
                 a = np.empty(max(1, int(n)), dtype=dtype)
             self._bufs[name] = a
         return a
+
+
+_stage_pool = None
+
+
+def _stage(out, arrays, sizes):
+    """Concatenates point arrays into `out` (a pinned staging buffer); large
+    batches are copied by several threads (NumPy releases the GIL for the
+    copies)."""
+    global _stage_pool
+    n = int(sizes.sum())
+    if n < (1 << 20) or len(arrays) < 2:
+        np.concatenate(arrays, out=out)
+        return
+    if _stage_pool is None:
+        from concurrent.futures import ThreadPoolExecutor
+
+        _stage_pool = ThreadPoolExecutor(max(2, min(8, os.cpu_count() or 2)))
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+
+    def copy(k):
+        out[offs[k]:offs[k + 1]] = arrays[k]
+
+    list(_stage_pool.map(copy, range(len(arrays))))
 
 
 class Engine:
@@ -414,7 +440,7 @@ class Engine:
         # staged in a reused pinned buffer: one DMA copy to the device
         xy = self._pool.get("batch_xy", 2 * n, np.float64)[: 2 * n].reshape(-1, 2)
         if n:
-            np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 2) for p in sets], out=xy)
+            _stage(xy, [np.asarray(p, dtype=np.float64).reshape(-1, 2) for p in sets], sizes)
         b = np.ascontiguousarray(self.batch_bounds(sets) if bounds is None else bounds, dtype=np.float64)
         st = Status()
         _check(self._L.galphaRunBatchHost(self._h, len(sets), sizes.ctypes.data, xy.ctypes.data if len(xy) else None,

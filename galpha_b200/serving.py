@@ -84,6 +84,14 @@ class Server:
         self.max_points = int(min(max_batch_points, share))
         self.batches = []  # (start, done, requests, points, slot)
 
+    def warm(self, sets, bounds=None):
+        """Runs a representative batch (the largest expected) on every slot, so
+        that device arenas and pinned staging buffers are grown before the
+        first request rather than inside its latency."""
+        for e in self.slots:
+            e.run_batch(sets, bounds=bounds)
+            e.batch_query([0.5] * len(sets), by_quantile=True)
+
     def _admit(self, queue):
         batch, pts = [], 0
         while queue:

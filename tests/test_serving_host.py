@@ -167,3 +167,12 @@ def test_failing_slot_raises_after_the_others_finish():
     with pytest.raises(RuntimeError, match="slot failed"):
         srv.run(reqs)
     assert SleepEngine.busy == 0
+
+
+def test_warm_runs_every_slot():
+    _reset_sleep_engines()
+    slots = [SleepEngine(), SleepEngine()]
+    sets = [np.zeros((100, 2)), np.zeros((50, 2))]
+    slots[0]._last = slots[1]._last = [0, 0]
+    S.Server(slots).warm(sets, bounds=np.zeros((2, 4)))
+    assert all(e.batches == [[100, 50]] for e in slots)
