@@ -289,8 +289,8 @@ def serving_leg(G, D, seconds, rate=2000.0, nslots=6):
     return out
 
 
-def e2e_pipelined(G, params, n, steps, device, dist, world, nslots=2):
-    """The same host-API call stream with two handles in flight (one host
+def e2e_pipelined(G, params, n, steps, device, dist, world, nslots=6):
+    """The same host-API call stream with several handles in flight (one host
     thread each): one call's uploads and downloads overlap the other's
     kernels.  Every call still uploads its points and downloads all of its
     results.  Wall-clock time over nslots x steps calls after one warm-up
