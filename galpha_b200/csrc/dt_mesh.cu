@@ -1467,20 +1467,23 @@ struct FlipCheck {
     int prev_round;  // -1: every triangle is listed
     __device__ void operator()(long long ii) const
     {
-        const int t = act[ii];
+        const int t = act ? act[ii] : (int)ii;  // no list: every slot (the first round)
         const int4 v = tv[t];
         int ci = -1, cu = -1, nfilt = 0;
         bool err = false;
         if (v.x >= 0) {
             const int4 n = tn[t];
-            const int x[3] = {v.x, v.y, v.z}, nb[3] = {n.x, n.y, n.z};
-            for (int i = 0; i < 3 && ci < 0 && !err; i++) {
+            const int nb[3] = {n.x, n.y, n.z};
+            const double2 P[3] = {pos[v.x], pos[v.y], pos[v.z]};  // once per triangle, not per edge
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                if (ci >= 0 || err) break;
                 const int e = nb[i];
                 if (e < 0) continue;
                 const int u = dtri(e);
                 if (u < t && (prev_round < 0 || stamp[u] == prev_round)) continue;  // u tests this edge
                 const int d = geti(tv[u], dori(e));
-                const double2 A = pos[x[p1(i)]], B = pos[x[m1(i)]], C = pos[x[i]], D = pos[d];
+                const double2 A = P[p1(i)], B = P[m1(i)], C = P[i], D = pos[d];
                 double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
                 int s = incircle_filter(pa, pb, pc, pd);
                 if (s == 2) {
@@ -1675,7 +1678,9 @@ int stage_flip(Ctx &c)
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->act[0], 0, 2 * sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->flips_total, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nflips, 0, sizeof(int), c.stream));
-    launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
+    // the first launched round tests every slot directly; the in-block tail
+    // (small meshes) starts from a list of the live slots
+    if (nt <= kTailEnter) launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
     GALPHA_CUDA(cudaMemsetAsync(c.vote, 0xff, sizeof(int) * (size_t)nt, c.stream));  // unsigned votes start at max
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
     const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
@@ -1709,9 +1714,14 @@ int stage_flip(Ctx &c)
             int p = rounds & 1;
             int round = next_round(c);
             launch_n(c, FlipRoundStart{p, c.ctr}, 1);
-            launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand, c.ctr,
-                                    stamp, prev_round},
-                       &c.ctr->act[p], capn);
+            if (rounds == 0)
+                launch_n(c, FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr,
+                                      stamp, -1},
+                         nt);
+            else
+                launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand,
+                                        c.ctr, stamp, prev_round},
+                           &c.ctr->act[p], capn);
             launch_dev(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, lists[1 - p],
                                     &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr},
                        &c.ctr->cand, capn);
