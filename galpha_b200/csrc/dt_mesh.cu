@@ -1071,6 +1071,140 @@ struct FakeSelect {
     }
 };
 
+// Runs of fake sites removed as one unit.  Removing one ring class after
+// another leaves the last class as a chain: collinear fakes on a side of the
+// texture become hull neighbours through the chords their removed neighbours
+// leave, so every fake of the last class touches the next one and the
+// priority rounds take out only about a third of the chain per round.  A run
+// -- selected fakes that follow each other along the hull -- has as outer
+// boundary the concatenation of its members' fan chains without the one
+// triangle each consecutive pair shares; the stack rule patches that chain
+// exactly as it patches one fake's.  Selection by separator levels over the
+// class's chain (j = ring position / 4): level l takes the fakes with j a
+// multiple of 16^l but not of 16^(l+1), so the kept multiples separate the
+// runs of one level (level 0: runs of 15 between every 16th fake).  The
+// leader (the member whose clockwise hull neighbour is not selected) stores
+// the kept fan entries followed by the shared triangles (outer link -1);
+// fanlen holds kept | shared << 16.  A run whose fans touch a selected fake
+// of another run, or that closes on itself, is left to the priority rounds.
+constexpr int kMaxRunMembers = 64;
+
+struct FakeSelectRuns {
+    const int4 *tv, *tn;
+    const int8_t *vstate;
+    const int *vtri;
+    int *list, *fanoff, *fanlen;
+    int2 *fan;
+    int *count, *fan_n;
+    int N, cls, level;
+    Counters *ct;
+    __device__ bool selected(int g) const
+    {
+        if (g < N || vstate[g] != VS_FAKE || ((g - N) & 3) != cls) return false;
+        const int j = (g - N) >> 2, sh = 4 * level;
+        return (j & ((1 << sh) - 1)) == 0 && ((j >> sh) & 15) != 0;
+    }
+    // Walks the run led by f from its clockwise fan end ecw; calls
+    // put(k, entry, outer) for the kept entries (k = 0..) and
+    // shared(j, entry) for the triangles consecutive members share.  Returns
+    // the number of members, 0 if the run is invalid (another selected fake
+    // in its fans, a fan too long), with *kept and *nshared set.
+    template <class Put, class Shared>
+    __device__ int walk(int f, int ecw, int *kept, int *nshared, Put put, Shared shared) const
+    {
+        int prev = -1, e = ecw, nk = 0, ns = 0;
+        for (int mi = 0; mi < kMaxRunMembers; mi++) {
+            // member fan: first pass to its counterclockwise end
+            int d = 0, nother = 0, bend = -1, tlast = -1, ilast = -1;
+            int ee = e;
+            for (;;) {
+                const int t = dtri(ee), i = dori(ee);
+                const int4 w = tv[t];
+                const int av = geti(w, p1(i)), bv = geti(w, m1(i));
+                if (d == 0 && av != prev && selected(av)) nother++;
+                if (bv != prev && selected(bv)) nother++;
+                bend = bv;
+                tlast = t;
+                ilast = i;
+                d++;
+                if (d > kMaxFanLong) return 0;
+                const int nx = geti(tn[t], p1(i));
+                if (nx < 0) break;
+                ee = enc(dtri(nx), p1(dori(nx)));
+            }
+            const bool next = selected(bend) && bend != f;
+            if (nother != (next ? 1 : 0)) return 0;  // touches another selected fake
+            if (mi > 0 && d < 2) return 0;            // one triangle shared with both neighbours
+            // second pass over the member's entries: kept / shared
+            ee = e;
+            for (int k = 0; k < d; k++) {
+                const int t = dtri(ee), i = dori(ee);
+                const int4 n = tn[t];
+                if (k == d - 1 && next) {
+                    shared(ns++, ee);
+                } else if (!(k == 0 && mi > 0)) {
+                    if (nk >= kMaxFanLong) return 0;
+                    put(nk++, ee, geti(n, i));
+                }
+                const int nx = geti(n, p1(i));
+                if (nx < 0) break;
+                ee = enc(dtri(nx), p1(dori(nx)));
+            }
+            if (!next) {
+                *kept = nk;
+                *nshared = ns;
+                return mi + 1;
+            }
+            prev = geti(tv[tlast], ilast);  // this member
+            e = enc(tlast, m1(ilast));       // the next member's clockwise end: the shared triangle
+        }
+        return 0;  // a closed ring of members (a small ring) or too many
+    }
+    __device__ void operator()(long long ii) const
+    {
+        const int f = N + (int)ii;
+        bool pick = selected(f);
+        int ecw = -1;
+        if (pick) {
+            // clockwise end of f's fan; f leads its run if that neighbour is no member
+            const int e0 = vtri[f];
+            int e = e0;
+            for (int g = 0;; g++) {
+                const int nx = geti(tn[dtri(e)], m1(dori(e)));  // across (f, a)
+                if (nx < 0) break;
+                e = enc(dtri(nx), m1(dori(nx)));
+                if (e == e0 || g > kMaxFanLong) {
+                    e = -1;
+                    break;
+                }
+            }
+            ecw = e;
+            if (ecw < 0) {
+                pick = false;
+            } else {
+                const int a0 = geti(tv[dtri(ecw)], p1(dori(ecw)));
+                if (selected(a0)) pick = false;
+            }
+        }
+        int kept = 0, nsh = 0, nmem = 0;
+        if (pick) {
+            nmem = walk(f, ecw, &kept, &nsh, [](int, int, int) {}, [](int, int) {});
+            pick = nmem > 0 && kept > 0;
+        }
+        const int k = warp_reserve(count, pick ? 1 : 0);
+        const int base = warp_reserve(fan_n, pick ? kept + nsh : 0);
+        if (pick) {
+            list[k] = f;
+            fanoff[k] = base;
+            fanlen[k] = kept | (nsh << 16);
+            int kk = 0, ss = 0;
+            walk(f, ecw, &kk, &ss, [&](int q, int e, int o) { fan[base + q] = make_int2(e, o); },
+                 [&](int j, int e) { fan[base + kept + j] = make_int2(e, -1); });
+        }
+        warp_reserve(&ct->changed, pick ? nmem : 0);
+    }
+};
+
 struct ZeroInts {
     int *a, *b;
     __device__ void operator()(long long) const
@@ -1115,7 +1249,8 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
     const int lane = threadIdx.x;
     const int n = *n_dev;
     for (int item = blockIdx.x; item < n; item += gridDim.x) {
-        const int f = a.list[item], d = a.fanlen[item], base = a.fanoff[item];
+        const int f = a.list[item], d = a.fanlen[item] & 0xffff, nsh = a.fanlen[item] >> 16,
+                  base = a.fanoff[item];
         if (d < dmin || d > M) continue;  // the other launch's item
         for (int k = lane; k < d; k += 32) {
             const int2 q = a.fan[base + k];
@@ -1127,6 +1262,11 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
             U[k] = geti(w, p1(i));
             if (k == d - 1) U[d] = geti(w, m1(i));
             a.epoch[t] = a.round;
+            const int fk = geti(w, i);  // the fake of this fan triangle (a run has several)
+            if (fk != f) {
+                a.vtri[fk] = -1;
+                a.vstate[fk] = VS_GONE;
+            }
         }
         __syncwarp();
         for (int k = lane; k <= d; k += 32) P[k] = a.pos[U[k]];
@@ -1202,7 +1342,7 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
             int cb = 0, fb = 0;
             if (lane == 0) {
                 cb = atomicAdd(&a.ct->nlist2, top);
-                fb = used < d ? atomicAdd(&a.ct->nfree, d - used) : 0;
+                fb = used < d || nsh ? atomicAdd(&a.ct->nfree, d - used + nsh) : 0;
             }
             cb = __shfl_sync(0xffffffffu, cb, 0);
             fb = __shfl_sync(0xffffffffu, fb, 0);
@@ -1210,6 +1350,20 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
             for (int k = used + lane; k < d; k += 32) {
                 a.tv[Fs[k]] = make_int4(-1, -1, -1, 0);
                 a.freelist[fb + k - used] = Fs[k];
+            }
+            // triangles shared by consecutive members of a run: inside the removed
+            // region.  Both members are marked here: a middle member whose fan is
+            // just its two shared triangles has no kept entry to be marked by.
+            for (int k = lane; k < nsh; k += 32) {
+                const int e = a.fan[base + d + k].x, t = dtri(e), i = dori(e);
+                const int4 w = a.tv[t];
+                const int m0 = geti(w, i), m2 = geti(w, m1(i));  // this member, the next one
+                a.vtri[m0] = -1;
+                a.vstate[m0] = VS_GONE;
+                a.vtri[m2] = -1;
+                a.vstate[m2] = VS_GONE;
+                a.tv[t] = make_int4(-1, -1, -1, 0);
+                a.freelist[fb + d - used + k] = t;
             }
         }
         if (lane == 0) {
@@ -1389,18 +1543,28 @@ int stage_boundary(Ctx &c)
     // the entries; the incidence array of the links stage is free by now
     int *fanoff = c.anchor, *fanlen = c.vround;  // per list entry (F <= V)
     int2 *fan = (int2 *)c.inc;                    // 3 cap ints: 1.5 cap entries
+    int run_levels = 1;  // separator levels covering the last class's chain of F / 4 fakes
+    while (run_levels < 6 && (1LL << (4 * run_levels)) < (c.F + 3) / 4) run_levels++;
     // first pass: the four ring classes in turn (independent by construction);
     // then rounds of priority-minimal fakes among all that remain
     for (int pass = 0; removed < c.F; pass++) {
         if (pass > kMaxRounds / 4) return GPUDT_ERR_NOCONVERGE;
-        const int nsub = pass == 0 ? 4 : 1;
+        // pass 0: three ring classes one fake at a time, then the last class
+        // (a chain by then) as runs, one separator level after another; later
+        // passes: priority rounds among the fakes left
+        const int nsub = pass == 0 ? 3 + run_levels : 1;
         for (int q = 0; q < nsub; q++) {
             int round = next_round(c);
             launch_n(c, ZeroInts{&c.ctr->nlist, &c.ctr->nrec}, 1);
             GALPHA_CUDA(cudaMemsetAsync(&c.ctr->cand, 0, sizeof(int), c.stream));  // fan entries
-            launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
-                                   &c.ctr->cand, c.N, pass == 0 ? order[q] : -1, c.ctr},
-                     c.F);
+            if (pass == 0 && q >= 3)
+                launch_n(c, FakeSelectRuns{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
+                                           &c.ctr->cand, c.N, order[3], q - 3, c.ctr},
+                         c.F);
+            else
+                launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
+                                       &c.ctr->cand, c.N, pass == 0 ? order[q] : -1, c.ctr},
+                         c.F);
             r = launch_fake_remove(c,
                                FakeRemoveArgs{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.list, fanoff, fanlen, fan,
                                               c.pos, c.vstate, c.rec, cand, round, c.ctr},
