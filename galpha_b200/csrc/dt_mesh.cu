@@ -1089,88 +1089,39 @@ struct FakeSelect {
 // of another run, or that closes on itself, is left to the priority rounds.
 constexpr int kMaxRunMembers = 64;
 
-struct FakeSelectRuns {
+// Separator-level selection of the fakes of one ring class (see above).
+__device__ __forceinline__ bool run_selected(const int8_t *vstate, int N, int cls, int level, int g)
+{
+    if (g < N || vstate[g] != VS_FAKE || ((g - N) & 3) != cls) return false;
+    const int j = (g - N) >> 2, sh = 4 * level;
+    return (j & ((1 << sh) - 1)) == 0 && ((j >> sh) & 15) != 0;
+}
+
+// Per selected fake, its own fan: the entries (clockwise end first) in the
+// staging array, and a record {offset, length, clockwise end vertex U[0],
+// counterclockwise end vertex U[d], valid}.  A fan holding a selected fake
+// strictly inside its chain is not valid (it touches another run).  Each
+// thread walks one fan, so the latency is that of one fan, not of a run.
+struct FakeRunStage {
     const int4 *tv, *tn;
     const int8_t *vstate;
     const int *vtri;
-    int *list, *fanoff, *fanlen;
-    int2 *fan;
-    int *count, *fan_n;
     int N, cls, level;
+    int2 *stage;
+    int *stage_n;
+    int *rec;  // 5 ints per ring position
     Counters *ct;
-    __device__ bool selected(int g) const
-    {
-        if (g < N || vstate[g] != VS_FAKE || ((g - N) & 3) != cls) return false;
-        const int j = (g - N) >> 2, sh = 4 * level;
-        return (j & ((1 << sh) - 1)) == 0 && ((j >> sh) & 15) != 0;
-    }
-    // Walks the run led by f from its clockwise fan end ecw; calls
-    // put(k, entry, outer) for the kept entries (k = 0..) and
-    // shared(j, entry) for the triangles consecutive members share.  Returns
-    // the number of members, 0 if the run is invalid (another selected fake
-    // in its fans, a fan too long), with *kept and *nshared set.
-    template <class Put, class Shared>
-    __device__ int walk(int f, int ecw, int *kept, int *nshared, Put put, Shared shared) const
-    {
-        int prev = -1, e = ecw, nk = 0, ns = 0;
-        for (int mi = 0; mi < kMaxRunMembers; mi++) {
-            // member fan: first pass to its counterclockwise end
-            int d = 0, nother = 0, bend = -1, tlast = -1, ilast = -1;
-            int ee = e;
-            for (;;) {
-                const int t = dtri(ee), i = dori(ee);
-                const int4 w = tv[t];
-                const int av = geti(w, p1(i)), bv = geti(w, m1(i));
-                if (d == 0 && av != prev && selected(av)) nother++;
-                if (bv != prev && selected(bv)) nother++;
-                bend = bv;
-                tlast = t;
-                ilast = i;
-                d++;
-                if (d > kMaxFanLong) return 0;
-                const int nx = geti(tn[t], p1(i));
-                if (nx < 0) break;
-                ee = enc(dtri(nx), p1(dori(nx)));
-            }
-            const bool next = selected(bend) && bend != f;
-            if (nother != (next ? 1 : 0)) return 0;  // touches another selected fake
-            if (mi > 0 && d < 2) return 0;            // one triangle shared with both neighbours
-            // second pass over the member's entries: kept / shared
-            ee = e;
-            for (int k = 0; k < d; k++) {
-                const int t = dtri(ee), i = dori(ee);
-                const int4 n = tn[t];
-                if (k == d - 1 && next) {
-                    shared(ns++, ee);
-                } else if (!(k == 0 && mi > 0)) {
-                    if (nk >= kMaxFanLong) return 0;
-                    put(nk++, ee, geti(n, i));
-                }
-                const int nx = geti(n, p1(i));
-                if (nx < 0) break;
-                ee = enc(dtri(nx), p1(dori(nx)));
-            }
-            if (!next) {
-                *kept = nk;
-                *nshared = ns;
-                return mi + 1;
-            }
-            prev = geti(tv[tlast], ilast);  // this member
-            e = enc(tlast, m1(ilast));       // the next member's clockwise end: the shared triangle
-        }
-        return 0;  // a closed ring of members (a small ring) or too many
-    }
     __device__ void operator()(long long ii) const
     {
         const int f = N + (int)ii;
-        bool pick = selected(f);
-        int ecw = -1;
-        if (pick) {
-            // clockwise end of f's fan; f leads its run if that neighbour is no member
+        const bool sel = run_selected(vstate, N, cls, level, f);
+        int ecw = -1, d = 0, a0 = -1, bend = -1;
+        bool ok = sel;
+        if (ok) {
             const int e0 = vtri[f];
             int e = e0;
-            for (int g = 0;; g++) {
-                const int nx = geti(tn[dtri(e)], m1(dori(e)));  // across (f, a)
+            for (int g = 0;; g++) {  // clockwise to the hull edge (f, U[0])
+                const int nx = geti(tn[dtri(e)], m1(dori(e)));
                 if (nx < 0) break;
                 e = enc(dtri(nx), m1(dori(nx)));
                 if (e == e0 || g > kMaxFanLong) {
@@ -1179,17 +1130,94 @@ struct FakeSelectRuns {
                 }
             }
             ecw = e;
-            if (ecw < 0) {
-                pick = false;
-            } else {
-                const int a0 = geti(tv[dtri(ecw)], p1(dori(ecw)));
-                if (selected(a0)) pick = false;
+            ok = ecw >= 0;
+        }
+        if (ok) {
+            int ee = ecw;
+            for (;;) {  // counterclockwise: count, ends, foreign selected fakes
+                const int t = dtri(ee), i = dori(ee);
+                const int4 w = tv[t];
+                if (d == 0) a0 = geti(w, p1(i));
+                const int bv = geti(w, m1(i));
+                bend = bv;
+                d++;
+                const int nx = geti(tn[t], p1(i));
+                if (nx < 0) break;
+                if (run_selected(vstate, N, cls, level, bv) || d > kMaxFanLong) {  // U[k] inside the chain
+                    ok = false;
+                    break;
+                }
+                ee = enc(dtri(nx), p1(dori(nx)));
             }
         }
+        const int off = warp_reserve(stage_n, ok ? d : 0);
+        if (ok) {
+            int ee = ecw;
+            for (int k = 0; k < d; k++) {
+                const int t = dtri(ee), i = dori(ee);
+                const int4 n = tn[t];
+                stage[off + k] = make_int2(ee, geti(n, i));
+                const int nx = geti(n, p1(i));
+                if (nx < 0) break;
+                ee = enc(dtri(nx), p1(dori(nx)));
+            }
+        }
+        if (sel) {
+            int *r = rec + 5 * ii;
+            r[0] = off;
+            r[1] = d;
+            r[2] = a0;
+            r[3] = bend;
+            r[4] = ok ? 1 : 0;
+        }
+    }
+};
+
+// Per run leader (a selected fake whose clockwise hull neighbour is not
+// selected): follows the members through their records, checks that each
+// next member's clockwise end is the current one, and copies the kept
+// entries followed by the shared triangles (outer link -1) into the fan
+// store; fanlen = kept | shared << 16.
+struct FakeRunJoin {
+    const int8_t *vstate;
+    int N, cls, level;
+    const int2 *stage;
+    const int *rec;
+    int *list, *fanoff, *fanlen;
+    int2 *fan;
+    int *count, *fan_n;
+    Counters *ct;
+    // members and counts of the run led by ring position ii; 0 if invalid
+    __device__ int scan(int ii, int *kept, int *nsh) const
+    {
+        const int f = N + ii;
+        int m = ii, nk = 0, ns = 0;
+        for (int mi = 0; mi < kMaxRunMembers; mi++) {
+            const int *r = rec + 5 * m;
+            if (!r[4] || (mi > 0 && r[1] < 2)) return 0;
+            const int nxt = r[3];
+            const bool next = nxt != f && run_selected(vstate, N, cls, level, nxt);
+            if (next && rec[5 * (nxt - N) + 2] != N + m) return 0;  // not hull neighbours
+            nk += r[1] - (mi > 0 ? 1 : 0) - (next ? 1 : 0);
+            ns += next ? 1 : 0;
+            if (!next) {
+                *kept = nk;
+                *nsh = ns;
+                return nk > 0 && nk <= kMaxFanLong ? mi + 1 : 0;
+            }
+            m = nxt - N;
+        }
+        return 0;
+    }
+    __device__ void operator()(long long ii) const
+    {
+        const int f = N + (int)ii;
+        bool pick = run_selected(vstate, N, cls, level, f) && rec[5 * ii + 4] &&
+                    !run_selected(vstate, N, cls, level, rec[5 * ii + 2]);
         int kept = 0, nsh = 0, nmem = 0;
         if (pick) {
-            nmem = walk(f, ecw, &kept, &nsh, [](int, int, int) {}, [](int, int) {});
-            pick = nmem > 0 && kept > 0;
+            nmem = scan((int)ii, &kept, &nsh);
+            pick = nmem > 0;
         }
         const int k = warp_reserve(count, pick ? 1 : 0);
         const int base = warp_reserve(fan_n, pick ? kept + nsh : 0);
@@ -1197,9 +1225,17 @@ struct FakeSelectRuns {
             list[k] = f;
             fanoff[k] = base;
             fanlen[k] = kept | (nsh << 16);
-            int kk = 0, ss = 0;
-            walk(f, ecw, &kk, &ss, [&](int q, int e, int o) { fan[base + q] = make_int2(e, o); },
-                 [&](int j, int e) { fan[base + kept + j] = make_int2(e, -1); });
+            int m = (int)ii, q = 0;
+            for (int mi = 0; mi < nmem; mi++) {
+                const int *r = rec + 5 * m;
+                const bool next = mi + 1 < nmem;
+                const int s0 = mi > 0 ? 1 : 0, s1 = r[1] - (next ? 1 : 0);
+                for (int j = s0; j < s1; j++) fan[base + q++] = stage[r[0] + j];
+                if (next) {
+                    fan[base + kept + mi] = make_int2(stage[r[0] + r[1] - 1].x, -1);
+                    m = r[3] - N;
+                }
+            }
         }
         warp_reserve(&ct->changed, pick ? nmem : 0);
     }
@@ -1557,11 +1593,18 @@ int stage_boundary(Ctx &c)
             int round = next_round(c);
             launch_n(c, ZeroInts{&c.ctr->nlist, &c.ctr->nrec}, 1);
             GALPHA_CUDA(cudaMemsetAsync(&c.ctr->cand, 0, sizeof(int), c.stream));  // fan entries
-            if (pass == 0 && q >= 3)
-                launch_n(c, FakeSelectRuns{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
-                                           &c.ctr->cand, c.N, order[3], q - 3, c.ctr},
+            if (pass == 0 && q >= 3) {
+                // staging in alpha-stage buffers, idle until the mesh is final
+                int2 *stage = (int2 *)c.keys2;
+                int *rec5 = (int *)c.spectrum;
+                GALPHA_CUDA(cudaMemsetAsync(&c.ctr->runstage, 0, sizeof(int), c.stream));
+                launch_n(c, FakeRunStage{c.tv, c.tn, c.vstate, c.vtri, c.N, order[3], q - 3, stage, &c.ctr->runstage,
+                                         rec5, c.ctr},
                          c.F);
-            else
+                launch_n(c, FakeRunJoin{c.vstate, c.N, order[3], q - 3, stage, rec5, c.list, fanoff, fanlen, fan,
+                                        &c.ctr->nlist, &c.ctr->cand, c.ctr},
+                         c.F);
+            } else
                 launch_n(c, FakeSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, fanoff, fanlen, fan, &c.ctr->nlist,
                                        &c.ctr->cand, c.N, pass == 0 ? order[q] : -1, c.ctr},
                          c.F);

@@ -63,7 +63,7 @@ struct Counters {
     int qpad;
     double qalpha;   // alpha query: the alpha value classified
     int tail_rounds; // flip: rounds run by the last in-block tail launch
-    int tail_pad;
+    int runstage;    // fake runs: staged fan entries
 };
 
 // Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
