@@ -360,40 +360,84 @@ struct ShiftCandidates {
     __device__ void operator()(long long i) const { cand[i] = vstate[i] == VS_UNDECIDED ? 1 : 0; }
 };
 
+// Drops candidate v (once per iteration) and lists it.
+__device__ __forceinline__ void shift_drop(int v, const int8_t *cand, int *drop, int *list, int *n)
+{
+    if (cand[v] && atomicExch(&drop[v], 1) == 0) list[atomicAdd(n, 1)] = v;
+}
+
+// A triangle with candidate vertices that would not stay counterclockwise with
+// them moved drops them.
+__device__ __forceinline__ void shift_check(int4 v, const double2 *pos, const double2 *opos, const int8_t *cand,
+                                            int *drop, int *list, int *n, Counters *ct)
+{
+    const int8_t c0 = cand[v.x], c1 = cand[v.y], c2 = cand[v.z];
+    if (!(c0 | c1 | c2)) return;
+    const double2 a = c0 ? opos[v.x] : pos[v.x];
+    const double2 b = c1 ? opos[v.y] : pos[v.y];
+    const double2 c = c2 ? opos[v.z] : pos[v.z];
+    if (orientp(a, b, c, ct) > 0) return;
+    if (c0) shift_drop(v.x, cand, drop, list, n);
+    if (c1) shift_drop(v.y, cand, drop, list, n);
+    if (c2) shift_drop(v.z, cand, drop, list, n);
+}
+
+// First iteration: every triangle.
 struct ShiftCheckTris {
     const int4 *tv;
     const double2 *pos, *opos;
-    int8_t *cand, *drop;
+    const int8_t *cand;
+    int *drop, *list, *n;
     Counters *ct;
     __device__ void operator()(long long ii) const
     {
-        int4 v = tv[ii];
+        const int4 v = tv[ii];
         if (v.x < 0) return;
-        int8_t c0 = cand[v.x], c1 = cand[v.y], c2 = cand[v.z];
-        if (!(c0 | c1 | c2)) return;
-        double2 a = c0 ? opos[v.x] : pos[v.x];
-        double2 b = c1 ? opos[v.y] : pos[v.y];
-        double2 c = c2 ? opos[v.z] : pos[v.z];
-        if (orientp(a, b, c, ct) > 0) return;
-        if (c0) drop[v.x] = 1;
-        if (c1) drop[v.y] = 1;
-        if (c2) drop[v.z] = 1;
+        shift_check(v, pos, opos, cand, drop, list, n, ct);
     }
 };
 
-struct ShiftDrop {
-    int8_t *cand, *drop;
+// Later iterations: only a triangle with a vertex dropped in the previous
+// iteration can change its verdict, so the fans of those vertices are checked.
+struct ShiftCheckFans {
+    const int4 *tv, *tn;
+    const int *vtri;
+    const double2 *pos, *opos;
+    const int8_t *cand;
+    const int *prev;
+    int *drop, *list, *n;
     Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        const int v = prev[ii];
+        const bool fine = walk_fan(tv, tn, vtri[v], [&](int t, int, int, int) {
+            shift_check(tv[t], pos, opos, cand, drop, list, n, ct);
+            return true;
+        });
+        if (!fine) set_err(ct, GPUDT_ERR_TOPOLOGY, 41);
+    }
+};
+
+// Takes the listed vertices out of the candidate set and appends them to the
+// list of all dropped vertices.
+struct ShiftDropList {
+    const int *list;
+    int8_t *cand;
+    int *drop, *all;
     __device__ void operator()(long long i) const
     {
-        if (drop[i]) {
-            drop[i] = 0;
-            if (cand[i]) {
-                cand[i] = 0;
-                atomicAdd(&ct->changed, 1);
-            }
-        }
+        const int v = list[i];
+        drop[v] = 0;
+        cand[v] = 0;
+        all[i] = v;
     }
+};
+
+// The undecided sites for the priority rounds: ring position ii of a list.
+struct ShiftRoundList {
+    ShiftRound r;
+    const int *list;
+    __device__ void operator()(long long ii) const { r(list[ii]); }
 };
 
 struct ShiftCommit {
@@ -435,6 +479,13 @@ struct BadSelect {
         int k = atomicAdd(&ct->nlist, 1);
         list[k] = v;
     }
+};
+
+// BAD sites are among the dropped ones.
+struct BadSelectList {
+    BadSelect b;
+    const int *list;
+    __device__ void operator()(long long ii) const { b(list[ii]); }
 };
 
 // Remove vertex v (interior) and triangulate its star hole by ear clipping
@@ -586,21 +637,38 @@ int stage_shift(Ctx &c)
 {
     int r;
     int shiftRounds = 0, badCount = 0;
+    int *dropped = c.aux2;  // every site the optimistic phase dropped: the only undecided ones after it
+    int ndropped = 0;
     {
         r = read_counters(c);
         if (r) return r;
         int nt = c.hctr->ntris;
-        int8_t *cand = (int8_t *)c.list2, *drop = (int8_t *)c.list2 + ((c.V + 255) & ~255);
+        // candidate flags (bytes) and per-iteration drop flags (ints) share list2
+        int8_t *cand = (int8_t *)c.list2;
+        int *drop = c.list2 + ((c.V + 1023) >> 2) + 256;
+        int *lists[2] = {c.list, c.aux};  // vertices dropped in an iteration (ping-pong)
         launch_n(c, ShiftCandidates{c.vstate, cand}, c.V);
-        GALPHA_CUDA(cudaMemsetAsync(drop, 0, (size_t)c.V, c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(drop, 0, sizeof(int) * (size_t)c.V, c.stream));
+        int nprev = 0;
         for (int it = 0; it < kMaxRounds; it++) {
-            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-            launch_n(c, ShiftCheckTris{c.tv, c.pos, c.opos, cand, drop, c.ctr}, nt);
-            launch_n(c, ShiftDrop{cand, drop, c.ctr}, c.V);
+            int *cur = lists[it & 1], *prev = lists[(it + 1) & 1];
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+            if (it == 0)
+                launch_n(c, ShiftCheckTris{c.tv, c.pos, c.opos, cand, drop, cur, &c.ctr->nlist2, c.ctr}, nt);
+            else
+                launch_n(c, ShiftCheckFans{c.tv, c.tn, c.vtri, c.pos, c.opos, cand, prev, drop, cur, &c.ctr->nlist2,
+                                           c.ctr},
+                         nprev);
             r = read_counters(c);
             if (r) return r;
+            if (c.hctr->err) return c.hctr->err;
             shiftRounds++;
-            if (c.hctr->changed == 0) break;
+            const int nd = c.hctr->nlist2;
+            if (nd == 0) break;
+            if ((long long)ndropped + nd > c.N) return GPUDT_ERR_TOPOLOGY;
+            launch_n(c, ShiftDropList{cur, cand, drop, dropped + ndropped}, nd);
+            ndropped += nd;
+            nprev = nd;
         }
         launch_n(c, ShiftCommit{cand, c.pos, c.opos, c.vstate, c.vround}, c.V);
     }
@@ -609,7 +677,9 @@ int stage_shift(Ctx &c)
     for (int round = 2;; round++) {
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int) + 0, c.stream));
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-        launch_n(c, ShiftRound{c.tv, c.tn, c.pos, c.opos, c.vstate, c.vround, c.vtri, round, c.ctr}, c.N);
+        launch_n(c, ShiftRoundList{ShiftRound{c.tv, c.tn, c.pos, c.opos, c.vstate, c.vround, c.vtri, round, c.ctr},
+                                   dropped},
+                 ndropped);
         r = run_counts(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
@@ -624,7 +694,7 @@ int stage_shift(Ctx &c)
     int guard = 0;
     while (badCount > 0) {
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-        launch_n(c, BadSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.ctr}, c.N);
+        launch_n(c, BadSelectList{BadSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.ctr}, dropped}, ndropped);
         r = run_counts(c);
         if (r) return r;
         int nsel = c.hctr->nlist;
