@@ -522,14 +522,14 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.keys, 0, sizeof(unsigned long long), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vals, 0, sizeof(int), c.stream));
-    launch_n(c, TriKeys{c.cv, c.cn, c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
+    launch_n(c, TriKeys{c.cv, c.cn, alpha_positions(c), e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->err) return c.hctr->err;
-    if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{c.cv, c.opos, c.list, c.keys, c.ctr}, c.hctr->nlist2);
+    if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{c.cv, alpha_positions(c), c.list, c.keys, c.ctr}, c.hctr->nlist2);
     r = exclusive_scan_int(c, unatt, spos, nE, &c.ctr->nlist);
     if (r) return r;
-    launch_n(c, EdgeKeys{c.edges, c.opos, unatt, spos, c.keys, c.vals, 1 + nT, nT}, nE);
+    launch_n(c, EdgeKeys{c.edges, alpha_positions(c), unatt, spos, c.keys, c.vals, 1 + nT, nT}, nE);
     r = read_counters(c);
     if (r) return r;
     const int nIn = 1 + nT + c.hctr->nlist;
@@ -568,14 +568,14 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     int nunc = c.hctr->nlist;
     if (nunc > 0) {
         GALPHA_CUDA(cudaMemsetAsync(slowflag, 0, sizeof(int) * (size_t)nIn, c.stream));
-        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, c.cv, c.edges, c.opos, nT, c.ctr,
+        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, c.cv, c.edges, alpha_positions(c), nT, c.ctr,
                                   segs ? segs->seg : nullptr},
                  nunc);
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
         if (c.hctr->nlist2 > 0)
-            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, c.cv, c.edges, c.opos, nIn, nT, c.ctr,
+            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, c.cv, c.edges, alpha_positions(c), nIn, nT, c.ctr,
                                     segs ? segs->seg : nullptr},
                      c.hctr->nlist2);
     }

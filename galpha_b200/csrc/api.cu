@@ -126,6 +126,7 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(vstate, int8_t, V);
     TAKE(vround, int, V);
     TAKE(anchor, int, V);
+    TAKE(perm, int, V);
     TAKE(deg, int, V + 1);
     TAKE(inc, int, 3 * cap);
     TAKE(tilecount, int, z.ntiles + 1);
@@ -812,6 +813,7 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
     if (r) return r;
     c.N = n;
     c.V = n;
+    c.renumbered = false;  // a host mesh: input ids throughout
     GALPHA_CUDA(cudaMemcpyAsync(c.opos, h->H.d_xy, sizeof(double2) * (size_t)n, cudaMemcpyDeviceToDevice, c.stream));
     GALPHA_CUDA(cudaMemcpyAsync(c.outtri, dt->triangles, sizeof(gpudtTriangle) * (size_t)dt->nTris,
                                 cudaMemcpyHostToDevice, c.stream));

@@ -462,6 +462,7 @@ int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds)
 // fake ring and no triangles; then the sites of all other sets are set up.
 int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy)
 {
+    c.renumbered = false;  // sets keep their input vertex order
     const int K = bh.K, N = bh.N;
     std::vector<int> vb(K + 1), fb(K + 1);
     for (int s = 0; s < K; s++) vb[s] = bh.sets[s].vbase;

@@ -66,8 +66,48 @@ struct RingPix {
     }
 };
 
+// Pixel of input point v inside the margin (the snap SetupSites makes).
+__device__ __forceinline__ void snap_pixel(double x, double y, double sx, double sy, double scale, int D, int *ix,
+                                           int *iy)
+{
+    const double gx = floor((x - sx) / scale), gy = floor((y - sy) / scale);
+    *ix = (int)fmin(fmax(gx, 0.0), (double)(D - 1));
+    *iy = (int)fmin(fmax(gy, 0.0), (double)(D - 1));
+}
+
+__device__ __forceinline__ unsigned spread_bits14(unsigned v)
+{
+    v &= 0x3fffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// Morton code of each input point's pixel, with its input index as payload.
+// Sorted stably, it numbers the vertices so that neighbours in the plane
+// have nearby ids (their positions, states and incidence share cache lines),
+// and points that share a pixel keep their input order, so the lowest input
+// index still owns the pixel.
+struct SpatialKeys {
+    const double *xy;
+    unsigned *keys;
+    int *vals;
+    double scale, sx, sy;
+    int D;
+    __device__ void operator()(long long i) const
+    {
+        int ix, iy;
+        snap_pixel(xy[2 * i], xy[2 * i + 1], sx, sy, scale, D, &ix, &iy);
+        keys[i] = spread_bits14((unsigned)ix) | (spread_bits14((unsigned)iy) << 1);
+        vals[i] = (int)i;
+    }
+};
+
 struct SetupSites {
     const double *xy;
+    const int *perm;  // internal vertex -> input index (nullptr: identity)
     double2 *opos, *pos;
     short2 *gpix;
     int *idmap;
@@ -84,12 +124,12 @@ struct SetupSites {
         double2 o, p;
         int px, py;
         if (v < N) {
-            o = make_double2(xy[2 * v], xy[2 * v + 1]);
-            if (!(o.x >= minX && o.x <= maxX && o.y >= minY && o.y <= maxY)) set_err(ct, GPUDT_ERR_ARG, v);
+            const int src = perm ? perm[v] : v;
+            o = make_double2(xy[2 * src], xy[2 * src + 1]);
+            if (!(o.x >= minX && o.x <= maxX && o.y >= minY && o.y <= maxY)) set_err(ct, GPUDT_ERR_ARG, src);
             int D = T - 2 * kMargin;
-            double gx = floor((o.x - sx) / scale), gy = floor((o.y - sy) / scale);
-            int ix = (int)fmin(fmax(gx, 0.0), (double)(D - 1));
-            int iy = (int)fmin(fmax(gy, 0.0), (double)(D - 1));
+            int ix, iy;
+            snap_pixel(o.x, o.y, sx, sy, scale, D, &ix, &iy);
             p = make_double2(sx + ix * scale, sy + iy * scale);
             px = ix + kMargin;
             py = iy + kMargin;
@@ -368,8 +408,17 @@ int stage_setup(Ctx &c, const double *d_xy, int n, double minX, double minY, dou
     GALPHA_CUDA(cudaMemsetAsync(c.occ, 0, sizeof(uint32_t) * (size_t)T * (T >> 5), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.bandocc, 0, sizeof(uint32_t) * (size_t)T * W2, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.ctr, 0, sizeof(Counters), c.stream));
+    // spatial numbering of the input points (stable radix sort of pixel Morton codes)
+    c.renumbered = n > 1;
+    if (c.renumbered) {
+        unsigned *k1 = (unsigned *)c.keys, *k2 = (unsigned *)c.keys2;
+        launch_n(c, SpatialKeys{d_xy, k1, c.perm, c.scale, c.shiftX, c.shiftY, T - 2 * kMargin}, n);
+        int r = radix_sort32(c, k1, c.perm, k2, c.vals2, n, c.rhist);
+        if (r) return r;
+    }
     SetupSites s;
     s.xy = d_xy;
+    s.perm = c.renumbered ? c.perm : nullptr;
     s.opos = c.opos;
     s.pos = c.pos;
     s.gpix = c.gpix;

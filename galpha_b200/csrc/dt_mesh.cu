@@ -2031,11 +2031,13 @@ struct CompactWrite {
     const int *newidx;
     int4 *cv, *cn;
     gpudtTriangle *out;
+    const int *perm;  // internal -> input vertex index (nullptr: identity)
     __device__ void operator()(long long ii) const
     {
         int t = (int)ii;
         int4 v = tv[t];
         if (v.x < 0) return;
+        if (perm) v = make_int4(perm[v.x], perm[v.y], perm[v.z], 0);
         int4 n = tn[t];
         int k = newidx[t];
         int nn[3] = {n.x, n.y, n.z};
@@ -2055,9 +2057,16 @@ struct CompactWrite {
     }
 };
 
+struct PositionsByInput {
+    const double2 *opos;
+    const int *perm;
+    double2 *out;
+    __device__ void operator()(long long v) const { out[perm[v]] = opos[v]; }
+};
+
 void launch_compact_write(Ctx &c, const int *newidx, int nslots)
 {
-    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri}, nslots);
+    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, nullptr}, nslots);
 }
 
 int stage_compact(Ctx &c)
@@ -2068,7 +2077,10 @@ int stage_compact(Ctx &c)
     launch_n(c, MarkAlive{c.tv, c.aux}, nt);
     r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->nlist);
     if (r) return r;
-    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, c.outtri}, nt);
+    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr}, nt);
+    // the input positions in input order for the alpha stage (pos, the moved
+    // positions of the mesh stages, is not needed any more)
+    if (c.renumbered) launch_n(c, PositionsByInput{c.opos, c.perm, c.pos}, c.N);
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
     if (r) return r;

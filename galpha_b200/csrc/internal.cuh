@@ -117,6 +117,8 @@ struct Ctx {
     int *freelist = nullptr;   // [cap]
     Relink *rec = nullptr;     // [3*cap]
     int *vtri = nullptr;       // [V] one incident oriented triangle
+    int *perm = nullptr;       // [V] single-set path: internal (spatially sorted) vertex -> input index
+    bool renumbered = false;   // the mesh stages ran on spatially sorted ids (perm); outputs use input ids
     int8_t *vstate = nullptr;  // [V]
     int *vround = nullptr;     // [V]
     int *anchor = nullptr;     // [V]
@@ -424,6 +426,9 @@ int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *o
 // LSD radix sort of (keys, vals) ascending (sort.cu)
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n);
 int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);
+// Positions by input index for the alpha stage: input order after a renumbered
+// mesh (written at compaction), else the original positions.
+inline const double2 *alpha_positions(const Ctx &c) { return c.renumbered ? c.pos : c.opos; }
 long long radix_scratch_ints(long long n);
 
 // Prefix sums (scan.cu)
