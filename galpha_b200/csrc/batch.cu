@@ -98,8 +98,39 @@ struct VertexSets {
     __device__ void operator()(long long i) const { vset[i] = find_set(vbases, K, (int)i); }
 };
 
+// Morton code of each point's pixel in its set's cell (payload: the input
+// index), and the set of the point at a sorted position: two stable sorts,
+// by code then by set, number each set's vertices spatially inside the set's
+// own id range.
+struct BSpatialKeys {
+    const double *xy;
+    const SetDesc *sets;
+    const int *vset;
+    unsigned *keys;
+    int *vals;
+    __device__ void operator()(long long i) const
+    {
+        const SetDesc &S = sets[vset[i]];
+        const int D = S.T - 2 * kMargin;
+        const double gx = floor((xy[2 * i] - S.sx) / S.scale), gy = floor((xy[2 * i + 1] - S.sy) / S.scale);
+        const unsigned ix = (unsigned)fmin(fmax(gx, 0.0), (double)(D - 1));
+        const unsigned iy = (unsigned)fmin(fmax(gy, 0.0), (double)(D - 1));
+        unsigned m = 0;
+        for (int b = 0; b < 14; b++) m |= ((ix >> b) & 1u) << (2 * b) | ((iy >> b) & 1u) << (2 * b + 1);
+        keys[i] = m;
+        vals[i] = (int)i;
+    }
+};
+
+struct SetOfPerm {
+    const int *vset, *perm;
+    unsigned *keys;
+    __device__ void operator()(long long i) const { keys[i] = (unsigned)vset[perm[i]]; }
+};
+
 struct BSetupSites {
     const double *xy;
+    const int *perm;  // internal vertex -> input index (nullptr: identity)
     const SetDesc *sets;
     const int *vset;
     const int *fbases;  // [K] fake bases (relative to N)
@@ -123,7 +154,8 @@ struct BSetupSites {
         double2 o, p;
         int px, py;
         if (v < N) {
-            o = make_double2(xy[2 * v], xy[2 * v + 1]);
+            const int src = perm ? perm[v] : v;
+            o = make_double2(xy[2 * src], xy[2 * src + 1]);
             if (!S.live) {
                 opos[v] = o;
                 pos[v] = o;
@@ -131,7 +163,7 @@ struct BSetupSites {
                 vstate[v] = VS_GONE;  // a set without triangles stays out of the mesh
                 return;
             }
-            if (!(o.x >= S.minX && o.x <= S.maxX && o.y >= S.minY && o.y <= S.maxY)) set_err(ct, GPUDT_ERR_ARG, v);
+            if (!(o.x >= S.minX && o.x <= S.maxX && o.y >= S.minY && o.y <= S.maxY)) set_err(ct, GPUDT_ERR_ARG, src);
             int D = S.T - 2 * kMargin;
             double gx = floor((o.x - S.sx) / S.scale), gy = floor((o.y - S.sy) / S.scale);
             int ix = (int)fmin(fmax(gx, 0.0), (double)(D - 1));
@@ -462,7 +494,6 @@ int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds)
 // fake ring and no triangles; then the sites of all other sets are set up.
 int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy)
 {
-    c.renumbered = false;  // sets keep their input vertex order
     const int K = bh.K, N = bh.N;
     std::vector<int> vb(K + 1), fb(K + 1);
     for (int s = 0; s < K; s++) vb[s] = bh.sets[s].vbase;
@@ -499,8 +530,20 @@ int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy)
     GALPHA_CUDA(cudaMemcpyAsync(B.sets, bh.sets.data(), sizeof(SetDesc) * (size_t)K, cudaMemcpyHostToDevice, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.occ, 0, sizeof(uint32_t) * (size_t)bh.occw, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.bandocc, 0, sizeof(uint32_t) * (size_t)bh.band, c.stream));
+    // spatial numbering inside each set
+    c.renumbered = N > 1;
+    if (c.renumbered) {
+        unsigned *k1 = (unsigned *)c.keys, *k2 = (unsigned *)c.keys2;
+        launch_n(c, BSpatialKeys{d_xy, B.sets, B.vset, k1, c.perm}, N);
+        int r = radix_sort32(c, k1, c.perm, k2, c.vals2, N, c.rhist);
+        if (r) return r;
+        launch_n(c, SetOfPerm{B.vset, c.perm, k1}, N);
+        r = radix_sort32(c, k1, c.perm, k2, c.vals2, N, c.rhist);
+        if (r) return r;
+    }
     BSetupSites st;
     st.xy = d_xy;
+    st.perm = c.renumbered ? c.perm : nullptr;
     st.sets = B.sets;
     st.vset = B.vset;
     st.fbases = B.fbases;

@@ -2066,7 +2066,8 @@ struct PositionsByInput {
 
 void launch_compact_write(Ctx &c, const int *newidx, int nslots)
 {
-    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, nullptr}, nslots);
+    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr}, nslots);
+    if (c.renumbered) launch_n(c, PositionsByInput{c.opos, c.perm, c.pos}, c.N);
 }
 
 int stage_compact(Ctx &c)
