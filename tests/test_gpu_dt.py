@@ -160,6 +160,28 @@ def test_large_uniform_properties(engine):
     assert dt.nTris == 2 * n - 2 - chk["hull_edges"]
 
 
+def test_c3_degenerate_properties(engine):
+    """c3 size (16.7M points: Gaussian blobs, uniform, lattice-snapped
+    duplicates and cocircular quads; texture 8192, about 7.5M sites inserted
+    after the Voronoi stage): exact validity of the full mesh, exactly the
+    lowest input index of each group of exact duplicates as vertex, the Euler
+    count, and a spectrum that increases strictly with every rank in range."""
+    pts, fbo = D.make("c3")
+    dt = run(engine, pts, fbo)
+    chk = O.check_mesh(pts, dt.vtx, dt.tri)
+    assert chk["links"] == 0 and chk["ccw"] == 0 and chk["delaunay"] == 0 and chk["bad_index"] == 0, chk
+    verts = np.unique(dt.vtx)
+    _, first = np.unique(pts, axis=0, return_index=True)
+    assert np.array_equal(verts, np.sort(first))
+    assert dt.nTris == 2 * len(verts) - 2 - chk["hull_edges"]
+    a = engine.alpha_resident()
+    s = a["spectrum"]
+    assert s[0] == 0.0 and np.all(np.diff(s[1:]) > 0)
+    ro = a["tri_list"]["ro_rank"]
+    assert ro.min() >= 1 and ro.max() < len(s)
+    assert a["edge_list"]["ro_rank"].max() < len(s)
+
+
 def test_voronoi_paths(engine):
     """Each discrete-Voronoi path: fused (dense), fused + local island repair,
     escalation to the global island path (sparse Gaussian tails), and the
