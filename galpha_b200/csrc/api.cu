@@ -611,6 +611,7 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
             tris = new (std::nothrow) gpudtTriangle[capacity > 0 ? capacity : 1];
             if (!tris) r = GPUDT_ERR_NOMEM;
         }
+        if (!r) r = ensure_outtri(c);
         if (!r) {
             if (c.nT_out > 0) {
                 cudaError_t e = cudaMemcpyAsync(tris, c.outtri, sizeof(gpudtTriangle) * (size_t)c.nT_out,
@@ -696,6 +697,8 @@ int galphaCopyTriangles(galphaHandle h, gpudtTriangle *dst, int cap)
     Ctx &c = h->H.c;
     if (!c.have_mesh) return GPUDT_ERR_ARG;
     int n = std::min(cap, c.nT_out);
+    int r = ensure_outtri(c);
+    if (r) return r;
     if (n > 0) {
         GALPHA_CUDA(cudaMemcpyAsync(dst, c.outtri, sizeof(gpudtTriangle) * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
         GALPHA_CUDA(cudaStreamSynchronize(c.stream));
@@ -818,6 +821,7 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
     GALPHA_CUDA(cudaMemcpyAsync(c.outtri, dt->triangles, sizeof(gpudtTriangle) * (size_t)dt->nTris,
                                 cudaMemcpyHostToDevice, c.stream));
     launch_n(c, AosToSoa{c.outtri, c.cv, c.cn}, dt->nTris);
+    c.outtri_ready = true;
     c.nT_out = dt->nTris;
     c.have_mesh = true;
     c.have_alpha = c.have_master = false;
@@ -868,6 +872,7 @@ int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt,
             if (!tris) r = GPUDT_ERR_NOMEM;
         }
     }
+    if (!r) r = ensure_outtri(c);
     if (!r && c.nT_out > 0) {
         cudaError_t e = cudaEventRecord(H.side_ev, c.stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(H.side, H.side_ev, 0);

@@ -2045,6 +2045,7 @@ struct CompactWrite {
             if (nn[q] >= 0) nn[q] = enc(newidx[dtri(nn[q])], dori(nn[q]));
         cv[k] = make_int4(v.x, v.y, v.z, 0);
         cn[k] = make_int4(nn[0], nn[1], nn[2], 0);
+        if (!out) return;
         gpudtTriangle g;
         g.tri[0] = nn[0];
         g.tri[1] = nn[1];
@@ -2057,6 +2058,34 @@ struct CompactWrite {
     }
 };
 
+// gpudtTriangle records of the compacted mesh (tmp[] zero).
+struct SoaToAos {
+    const int4 *cv, *cn;
+    gpudtTriangle *out;
+    __device__ void operator()(long long k) const
+    {
+        const int4 v = cv[k], n = cn[k];
+        gpudtTriangle g;
+        g.tri[0] = n.x;
+        g.tri[1] = n.y;
+        g.tri[2] = n.z;
+        g.vtx[0] = v.x;
+        g.vtx[1] = v.y;
+        g.vtx[2] = v.z;
+        g.tmp[0] = g.tmp[1] = g.tmp[2] = 0;
+        out[k] = g;
+    }
+};
+
+int ensure_outtri(Ctx &c)
+{
+    if (c.outtri_ready) return GPUDT_OK;
+    if (c.nT_out > 0) launch_n(c, SoaToAos{c.cv, c.cn, c.outtri}, c.nT_out);
+    GALPHA_CUDA(cudaGetLastError());
+    c.outtri_ready = true;
+    return GPUDT_OK;
+}
+
 struct PositionsByInput {
     const double2 *opos;
     const int *perm;
@@ -2067,6 +2096,7 @@ struct PositionsByInput {
 void launch_compact_write(Ctx &c, const int *newidx, int nslots)
 {
     launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr}, nslots);
+    c.outtri_ready = true;
     if (c.renumbered) launch_n(c, PositionsByInput{c.opos, c.perm, c.pos}, c.N);
 }
 
@@ -2078,7 +2108,9 @@ int stage_compact(Ctx &c)
     launch_n(c, MarkAlive{c.tv, c.aux}, nt);
     r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->nlist);
     if (r) return r;
-    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr}, nt);
+    // cv / cn only: the gpudtTriangle records are built when a download asks for them
+    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, nullptr, c.renumbered ? c.perm : nullptr}, nt);
+    c.outtri_ready = false;
     // the input positions in input order for the alpha stage (pos, the moved
     // positions of the mesh stages, is not needed any more)
     if (c.renumbered) launch_n(c, PositionsByInput{c.opos, c.perm, c.pos}, c.N);

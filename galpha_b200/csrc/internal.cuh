@@ -153,6 +153,7 @@ struct Ctx {
     int *hist = nullptr;       // scan scratch
     int *rhist = nullptr;      // radix sort histograms
     gpudtTriangle *outtri = nullptr;  // [cap] AoS output staging
+    bool outtri_ready = false;          // outtri holds the current mesh (built on the first download)
     galphaEdgeInterval *edge_aos = nullptr;  // [2*cap] edge records for download
 
     DevBuf bufs[64];
@@ -380,6 +381,9 @@ void grid_scaling(double minX, double minY, double maxX, double maxY, int T, dou
 void launch_compact_write(Ctx &c, const int *newidx, int nslots);
 int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds);
 int fused_tiles(int T);  // tiles of the fused colouring kernel per T x T cell
+// The mesh in the gpudtTriangle layout (outtri), built from cv / cn when a
+// host download first needs it.
+int ensure_outtri(Ctx &c);
 int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, int ntiles);
 int batch_setup(Ctx &c, BatchDev &B, BatchHost &bh, const double *d_xy);
 int batch_voronoi(Ctx &c, BatchDev &B, BatchHost &bh);
