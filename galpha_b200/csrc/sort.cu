@@ -6,8 +6,8 @@
 // 8-bit digits; digits on which all keys agree are skipped (an OR of
 // key XOR first-key finds them).  Each pass: a per-block shared-memory
 // histogram, a scan of the digit-major histogram table, and a scatter that
-// first sorts the block's 4096-key tile by digit in shared memory (warp ranks
-// from __match_any_sync, stable) and then writes each digit's run to its
+// first sorts the block's 2048-key tile by digit in shared memory (warp ranks
+// from 8 ballots per round, stable) and then writes each digit's run to its
 // global offset, so consecutive threads store consecutive addresses.
 #include <algorithm>
 #include <mutex>
@@ -72,13 +72,24 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K *__restrict__
         bool ok = i < n;
         key[r] = ok ? kin[i] : (K)0;
         val[r] = ok ? vin[i] : 0;
-        const int dg = ok ? (int)((key[r] >> shift) & 255) : 256 + lane;  // unique dummy digits
-        unsigned peers = __match_any_sync(0xffffffffu, dg);
-        int before = ok ? S.wcnt[w][dg] : 0;
+    }
+    // lanes with the same digit: 8 ballots; the lowest such lane adds the
+    // group to the warp's digit count and hands the old count to the group
+#pragma unroll
+    for (int r = 0; r < kRsItems; r++) {
+        const bool ok = base + r * 32 + lane < n;
+        const int dg = (int)((key[r] >> shift) & 255);
+        unsigned peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const unsigned bb = __ballot_sync(0xffffffffu, (dg >> b) & 1);
+            peers &= ((dg >> b) & 1) ? bb : ~bb;
+        }
+        const int leader = ok ? __ffs(peers) - 1 : lane;
+        int before = 0;
+        if (ok && lane == leader) before = atomicAdd(&S.wcnt[w][dg], __popc(peers));
+        before = __shfl_sync(0xffffffffu, before, leader);
         rk[r] = before + __popc(peers & lanemask_lt);
-        __syncwarp();
-        if (ok && (peers & lanemask_lt) == 0) S.wcnt[w][dg] = before + __popc(peers);
-        __syncwarp();
     }
     __syncthreads();
     // per digit: totals over warps, then the digit-major exclusive scan
