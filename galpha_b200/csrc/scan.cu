@@ -113,11 +113,117 @@ static int scan_rec(Ctx &c, const int *in, int *out, long long n, int *scratch)
     return GPUDT_OK;
 }
 
+// ---------------------------------------------------------- single pass
+// One launch: tiles are taken in ticket order; each tile publishes its sum,
+// then warp 0 looks back over the published sums of up to 32 earlier tiles at
+// a time until it meets a tile that has published its inclusive prefix
+// (decoupled look-back), and publishes its own.  A tile only waits on tiles
+// with earlier tickets, whose blocks are running; the bounded wait guards a
+// broken invariant and reports it in the counter block.
+constexpr unsigned long long kScAgg = 1ull << 62;  // status: the tile's own sum
+constexpr unsigned long long kScPre = 2ull << 62;  // status: the sum of this and all earlier tiles
+constexpr unsigned long long kScVal = (1ull << 62) - 1;
+constexpr int kScanSpinLimit = 1 << 22;
+constexpr int kScanStatusOff = 64;  // ints before the status words in the scratch (ticket at [2])
+constexpr long long kScanMaxTiles = (65536 - kScanStatusOff) / 2;
+
+__device__ __forceinline__ void sc_st_release(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long sc_ld_acquire(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_1p(const int *__restrict__ in, int *__restrict__ out,
+                                                          long long n, unsigned long long *status, int *ticket,
+                                                          int *total, Counters *ct)
+{
+    __shared__ int s_tile;
+    __shared__ long long s_excl;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int tile = s_tile;
+    const long long base = (long long)tile * kScanTile + (long long)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const long long i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        sum += v[k];
+    }
+    int excl;
+    const int tot = block_scan(sum, excl);
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        long long acc = 0;
+        if (tile > 0) {
+            if (lane == 0) sc_st_release(&status[tile], kScAgg | (unsigned long long)(unsigned)tot);
+            bool bad = false;
+            for (int j = tile - 1;; j -= 32) {
+                const int idx = j - lane;
+                unsigned long long w = kScPre;  // before tile 0: nothing to add
+                if (idx >= 0) {
+                    int spins = 0;
+                    while (((w = sc_ld_acquire(&status[idx])) >> 62) == 0) {
+                        if (++spins > kScanSpinLimit) {
+                            bad = true;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                if (__any_sync(0xffffffffu, bad)) {
+                    bad = true;
+                    break;
+                }
+                const unsigned pre = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+                const int first = pre ? __ffs(pre) - 1 : 31;  // lanes up to the nearest prefix count
+                long long mine = (lane <= first && idx >= 0) ? (long long)(w & kScVal) : 0;
+                for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+                acc += mine;
+                if (pre) break;
+            }
+            if (bad && lane == 0) set_err(ct, GPUDT_ERR_NOCONVERGE, 97);
+        }
+        if (lane == 0) {
+            sc_st_release(&status[tile], kScPre | (unsigned long long)(acc + tot));
+            s_excl = acc;
+        }
+    }
+    __syncthreads();
+    const int off = (int)s_excl + excl;
+    int e = off;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const long long i = base + k;
+        if (i < n) out[i] = e;
+        e += v[k];
+    }
+    if (total && threadIdx.x == 0 && (long long)(tile + 1) * kScanTile >= n) *total = (int)(s_excl + tot);
+}
+
 // out may alias in.  total_dev (optional) receives sum(in).
 int exclusive_scan_int(Ctx &c, const int *in, int *out, int n, int *total_dev)
 {
     if (n <= 0) {
         if (total_dev) GALPHA_CUDA(cudaMemsetAsync(total_dev, 0, sizeof(int), c.stream));
+        return GPUDT_OK;
+    }
+    const long long tiles = ((long long)n + kScanTile - 1) / kScanTile;
+    if (tiles > 1 && tiles <= kScanMaxTiles) {
+        int *ticket = c.hist + 2;
+        unsigned long long *status = reinterpret_cast<unsigned long long *>(c.hist + kScanStatusOff);
+        GALPHA_CUDA(cudaMemsetAsync(ticket, 0, sizeof(int), c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (size_t)tiles, c.stream));
+        k_scan_1p<<<(unsigned)tiles, kScanThreads, 0, c.stream>>>(in, out, n, status, ticket, total_dev, c.ctr);
+        count_launch();
+        GALPHA_CUDA(cudaGetLastError());
         return GPUDT_OK;
     }
     int *scratch = c.hist;  // scan scratch lives at the start of the histogram buffer
