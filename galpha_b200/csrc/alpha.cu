@@ -539,8 +539,17 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
         cudaEventRecord(c.kev[8], c.stream);
         c.kev_rec[8] = true;
     }
-    r = radix_sort(c, c.keys + 1, c.vals + 1, c.keys2, c.vals2, nIn - 1);
+    bool second = false;
+    r = radix_sort(c, c.keys + 1, c.vals + 1, c.keys2 + 1, c.vals2 + 1, nIn - 1, &second);
     if (r) return r;
+    if (second) {
+        // the sorted entries are in the second buffers: they become keys / vals
+        // (sentinel entry 0 included) for the rest of this result's life
+        GALPHA_CUDA(cudaMemsetAsync(c.keys2, 0, sizeof(unsigned long long), c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(c.vals2, 0, sizeof(int), c.stream));
+        std::swap(c.keys, c.keys2);
+        std::swap(c.vals, c.vals2);
+    }
     if (c.events) {
         cudaEventRecord(c.kev[9], c.stream);
         c.kev_rec[9] = true;

@@ -428,7 +428,8 @@ int launch_emit_cells(Ctx &c, int ntiles, long long nwin, bool write, int4 *tv_o
 int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *occ, const uint32_t *bandocc,
                              int16_t *ycol);
 // LSD radix sort of (keys, vals) ascending (sort.cu)
-int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n);
+int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n,
+               bool *in_second);
 int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);
 // Positions by input index for the alpha stage: input order after a renumbered
 // mesh (written at compaction), else the original positions.

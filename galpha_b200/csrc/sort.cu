@@ -167,8 +167,10 @@ long long radix_scratch_ints(long long n)
 // up; result in keys/vals.  Uses keys2/vals2 and `scratch`
 // (radix_scratch_ints(n) ints).
 template <typename K>
-static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int n, int *scratch, int min_shift = 0)
+static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int n, int *scratch, int min_shift = 0,
+                           bool *in_second = nullptr)
 {
+    if (in_second) *in_second = false;
     if (n <= 1) return GPUDT_OK;
     static_assert(sizeof(K) == 4 || sizeof(K) == 8, "32- or 64-bit keys");
     const int smem = (int)sizeof(RsSmem<K>);
@@ -213,6 +215,10 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
         std::swap(vi, vo);
     }
     if (ki != keys) {
+        if (in_second) {  // the caller takes the result where the last pass left it
+            *in_second = true;
+            return GPUDT_OK;
+        }
         launch_n(c, CopyElems<K>{keys, ki}, n);
         launch_n(c, CopyElems<int>{vals, vi}, n);
     }
@@ -292,21 +298,33 @@ struct FixGroups {
     }
 };
 
-int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
+// The result is left in (keys, vals) or, when *in_second comes back true, in
+// (keys2, vals2): an odd number of passes ends there, and a copy back would
+// cost a full read and write of both arrays.
+int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n,
+               bool *in_second)
 {
-    int r = radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist, kLowBits);
+    bool sec = false;
+    int r = radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist, kLowBits, &sec);
+    *in_second = sec;
     if (r || n <= 1) return r;
-    // group fix-up (starts / flags reuse the second key buffer, free now)
-    int *starts = (int *)keys2, *flag = starts + ((n + 63) & ~63);
+    unsigned long long *rk = sec ? keys2 : keys, *fk = sec ? keys : keys2;
+    int *rv = sec ? vals2 : vals, *fv = sec ? vals : vals2;
+    // group fix-up (starts / flags in the other key buffer, free now)
+    int *starts = (int *)fk, *flag = starts + ((n + 63) & ~63);
     GALPHA_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)n, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-    launch_n(c, FixFindOffset{keys, starts, flag, n, c.ctr}, n - 1);
+    launch_n(c, FixFindOffset{rk, starts, flag, n, c.ctr}, n - 1);
     r = read_counters(c);
     if (r) return r;
-    if (c.hctr->changed)
-        return radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist, 0);
-    if (c.hctr->nlist2 > 0) launch_n(c, FixGroups{keys, vals, starts, flag, n}, c.hctr->nlist2);
+    if (c.hctr->changed) {
+        bool sec2 = false;
+        r = radix_sort_keys<unsigned long long>(c, rk, rv, fk, fv, n, c.rhist, 0, &sec2);
+        if (sec2) *in_second = !sec;
+        return r;
+    }
+    if (c.hctr->nlist2 > 0) launch_n(c, FixGroups{rk, rv, starts, flag, n}, c.hctr->nlist2);
     GALPHA_CUDA(cudaGetLastError());
     return GPUDT_OK;
 }
