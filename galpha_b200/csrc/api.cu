@@ -119,6 +119,7 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(cn, int4, cap);
     TAKE(epoch, int, cap);
     TAKE(vote, int, cap);
+    TAKE(eflag, int8_t, cap);
     TAKE(stamp, int, L);
     TAKE(freelist, int, cap);
     TAKE(rec, Relink, 3 * cap);

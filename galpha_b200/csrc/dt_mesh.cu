@@ -1730,9 +1730,12 @@ int stage_boundary(Ctx &c)
 // the host looks at the counters only every kFlipSync rounds.
 constexpr int kFlipSync = 4;
 
-// Each edge is tested from one side: when both triangles are in this round's
-// list (all of them in the first round; else stamp == prev_round), from the
-// lower index; the other side's proposal for the edge is made by that one.
+// The first round tests every edge once, from the triangle with the lower
+// slot.  A flip replaces edge (b, c) of the quad (a, b, d, c) by (a, d); only
+// the quad's four outer edges can then have stopped being locally Delaunay,
+// so the two new triangles are listed with their outer edges marked
+// (eflag), and later rounds test marked edges only.  A candidate that loses
+// its vote keeps its marks (all three after the one-sided first round).
 struct FlipCheck {
     const int4 *tv, *tn;
     const double2 *pos;
@@ -1740,15 +1743,17 @@ struct FlipCheck {
     int *vote, *prop, *target, *cands;
     int *cand_n;
     Counters *ct;
-    const int *stamp;
-    int prev_round;  // -1: every triangle is listed
+    int8_t *eflag;
     __device__ void operator()(long long ii) const
     {
         const int t = act ? act[ii] : (int)ii;  // no list: every slot (the first round)
         const int4 v = tv[t];
         int ci = -1, cu = -1, nfilt = 0;
         bool err = false;
-        if (v.x >= 0) {
+        // the first round tests every edge once (from the lower slot); later
+        // rounds test the edges a flip or a lost vote left marked
+        const int fl = act ? eflag[t] : 7;
+        if (v.x >= 0 && fl) {
             const int4 n = tn[t];
             const int nb[3] = {n.x, n.y, n.z};
             const double2 P[3] = {pos[v.x], pos[v.y], pos[v.z]};  // once per triangle, not per edge
@@ -1756,9 +1761,9 @@ struct FlipCheck {
             for (int i = 0; i < 3; i++) {
                 if (ci >= 0 || err) break;
                 const int e = nb[i];
-                if (e < 0) continue;
+                if (e < 0 || !((fl >> i) & 1)) continue;
                 const int u = dtri(e);
-                if (u < t && (prev_round < 0 || stamp[u] == prev_round)) continue;  // u tests this edge
+                if (!act && u < t) continue;  // first round: u tests this edge
                 const int d = geti(tv[u], dori(e));
                 const double2 A = P[p1(i)], B = P[m1(i)], C = P[i], D = pos[d];
                 double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
@@ -1779,6 +1784,7 @@ struct FlipCheck {
         if (err) set_err(ct, GPUDT_ERR_EXACT, 90);
         warp_add_spread(ct->filt_spread, nfilt);
         const bool has = ci >= 0;
+        if (act && !has && fl) eflag[t] = 0;  // every marked edge is locally Delaunay
         if (has) {
             prop[t] = ci;
             target[t] = cu;
@@ -1802,6 +1808,8 @@ struct FlipApply {
     Relink *rec;
     int round;
     Counters *ct;
+    int8_t *eflag;
+    bool first;  // first round: a losing candidate was tested one-sided, so all its edges stay marked
     __device__ bool fresh(int x) const { return x >= 0 && atomicExch(&stamp[x], round) != round; }
     __device__ void operator()(long long ii) const
     {
@@ -1812,6 +1820,7 @@ struct FlipApply {
         int nx[6], nn = 0;
         Relink r4[4];
         if (!win) {
+            if (first) eflag[t] = 7;
             if (fresh(t)) nx[nn++] = t;
         } else {
             const int i = prop[t];
@@ -1845,12 +1854,12 @@ struct FlipApply {
             vtri[b] = enc(t, 1);
             vtri[d] = enc(t, 2);
             vtri[cc] = enc(u, 1);
+            // only the four outer edges of the new pair can have stopped being
+            // locally Delaunay: edges 0 and 2 of t and of u
+            eflag[t] = 5;
+            eflag[u] = 5;
             if (fresh(t)) nx[nn++] = t;
             if (fresh(u)) nx[nn++] = u;
-            if (ou1 >= 0 && fresh(dtri(ou1))) nx[nn++] = dtri(ou1);
-            if (ot2 >= 0 && fresh(dtri(ot2))) nx[nn++] = dtri(ot2);
-            if (ot1 >= 0 && fresh(dtri(ot1))) nx[nn++] = dtri(ot1);
-            if (ou2 >= 0 && fresh(dtri(ou2))) nx[nn++] = dtri(ou2);
         }
         // one atomic per warp for each of the records, the flip count and the next list
         const int rb = warp_reserve(&ct->nrec, win ? 4 : 0);
@@ -1901,7 +1910,7 @@ constexpr int kTailEnter = 4096;    // the host hands over at or below this many
 constexpr int kTailLeave = 32768;   // the block hands back above this many
 
 __global__ void __launch_bounds__(kTailThreads) k_flip_tail(FlipCheck ck, FlipApply ap, Relinker rl, FlipReset rs,
-                                                             int *l0, int *l1, int p0, int round0, int prev0,
+                                                             int *l0, int *l1, int p0, int round0,
                                                              int max_rounds, int leave)
 {
     Counters *ct = ck.ct;
@@ -1914,7 +1923,6 @@ __global__ void __launch_bounds__(kTailThreads) k_flip_tail(FlipCheck ck, FlipAp
         __syncthreads();
         const int round = round0 + k;
         ck.act = p ? l1 : l0;
-        ck.prev_round = k ? round - 1 : prev0;
         for (int i = threadIdx.x; i < n; i += kTailThreads) ck(i);
         __syncthreads();
         const int nc = *(volatile int *)&ct->cand;
@@ -1958,21 +1966,24 @@ int stage_flip(Ctx &c)
     // the first launched round tests every slot directly; the in-block tail
     // (small meshes) starts from a list of the live slots
     if (nt <= kTailEnter) launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
+    // marked edges: none before the first launched round (it tests all), all
+    // when the in-block rounds start from the list of live slots
+    GALPHA_CUDA(cudaMemsetAsync(c.eflag, nt <= kTailEnter ? 7 : 0, (size_t)c.cap_tris, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vote, 0xff, sizeof(int) * (size_t)nt, c.stream));  // unsigned votes start at max
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
     const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
-    int rounds = 0, prev_round = -1;
+    int rounds = 0;
     long long known = nt;  // active-list length at `rounds`, as last read (nt bounds the first)
     while (known > 0) {
         if (known <= kTailEnter) {
             const int p = rounds & 1;
             const int round0 = next_round(c);
             k_flip_tail<<<1, kTailThreads, 0, c.stream>>>(
-                FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr, stamp, -1},
+                FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr, c.eflag},
                 FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nullptr, nullptr, prop, target, cands,
-                          c.rec, 0, c.ctr},
+                          c.rec, 0, c.ctr, c.eflag, false},
                 Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, 0, c.ctr}, FlipReset{c.vote, target, cands},
-                lists[0], lists[1], p, round0, prev_round, kMaxRounds + 1 - rounds, kTailLeave);
+                lists[0], lists[1], p, round0, kMaxRounds + 1 - rounds, kTailLeave);
             count_launch();
             GALPHA_CUDA(cudaGetLastError());
             r = read_counters(c);
@@ -1980,7 +1991,6 @@ int stage_flip(Ctx &c)
             if (c.hctr->err) return c.hctr->err;
             const int k = c.hctr->tail_rounds;
             skip_rounds(c, round0, k - 1);
-            if (k > 0) prev_round = round0 + k - 1;
             rounds += k;
             known = c.hctr->act[rounds & 1];
             if (known == 0) break;
@@ -1993,18 +2003,18 @@ int stage_flip(Ctx &c)
             launch_n(c, FlipRoundStart{p, c.ctr}, 1);
             if (rounds == 0)
                 launch_n(c, FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr,
-                                      stamp, -1},
+                                      c.eflag},
                          nt);
             else
                 launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand,
-                                        c.ctr, stamp, prev_round},
+                                        c.ctr, c.eflag},
                            &c.ctr->act[p], capn);
             launch_dev(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, lists[1 - p],
-                                    &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr},
+                                    &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr, c.eflag,
+                                    rounds == 0},
                        &c.ctr->cand, capn);
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
             launch_dev(c, FlipReset{c.vote, target, cands}, &c.ctr->cand, capn);
-            prev_round = round;
             rounds++;
         }
         GALPHA_CUDA(cudaGetLastError());

@@ -117,6 +117,7 @@ struct Ctx {
     int *freelist = nullptr;   // [cap]
     Relink *rec = nullptr;     // [3*cap]
     int *vtri = nullptr;       // [V] one incident oriented triangle
+    int8_t *eflag = nullptr;   // [cap] flip: edges of a triangle still to be tested (bit i: edge opposite vtx[i])
     int *perm = nullptr;       // [V] single-set path: internal (spatially sorted) vertex -> input index
     bool renumbered = false;   // the mesh stages ran on spatially sorted ids (perm); outputs use input ids
     int8_t *vstate = nullptr;  // [V]
