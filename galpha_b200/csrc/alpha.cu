@@ -124,6 +124,7 @@ struct EdgeCount {
 // Triangle keys + owned edges + attached test.
 struct TriKeys {
     const int4 *cv, *cn;
+    const int4 *gv;  // the triangles with the ids that index P
     const double2 *P;
     const int *e_off;
     unsigned long long *keys;
@@ -137,7 +138,9 @@ struct TriKeys {
     {
         int t = (int)ii;
         int4 v = cv[t], n = cn[t];
-        double2 A = P[v.x], B = P[v.y], C = P[v.z];
+        const int4 g = gv[t];
+        const double2 Q[3] = {P[g.x], P[g.y], P[g.z]};
+        const double2 A = Q[0], B = Q[1], C = Q[2];
         bool sl;
         double r = rho_tri(A, B, C, &sl);
         keys[1 + t] = (unsigned long long)__double_as_longlong(r);
@@ -147,12 +150,13 @@ struct TriKeys {
             slivers[k] = t;
         }
         int e = e_off[t];
+#pragma unroll
         for (int i = 0; i < 3; i++) {
             int a = geti(v, p1(i)), b = geti(v, m1(i));
             int nb = geti(n, i);
             if (!(a < b || nb == -1)) continue;
             edges[e] = make_int4(a, b, t, i);
-            double2 pa = P[a], pb = P[b], pk = P[geti(v, i)];
+            const double2 pa = Q[p1(i)], pb = Q[m1(i)], pk = Q[i];
             double qa[2] = {pa.x, pa.y}, qb[2] = {pb.x, pb.y}, qk[2] = {pk.x, pk.y};
             int att = attached_filter(qa, qb, qk);
             if (att == 2) {
@@ -160,7 +164,7 @@ struct TriKeys {
                 att = attached_exact(qa, qb, qk);
             }
             if (att == 0 && nb >= 0) {
-                double2 po = P[geti(cv[dtri(nb)], dori(nb))];
+                double2 po = P[geti(gv[dtri(nb)], dori(nb))];
                 double qo[2] = {po.x, po.y};
                 att = attached_filter(qa, qb, qo);
                 if (att == 2) {
@@ -177,7 +181,7 @@ struct TriKeys {
 };
 
 struct SliverKeys {
-    const int4 *cv;
+    const int4 *cv;  // the triangles with the ids that index P
     const double2 *P;
     const int *slivers;
     unsigned long long *keys;
@@ -195,6 +199,7 @@ struct SliverKeys {
 
 struct EdgeKeys {
     const int4 *edges;
+    const int4 *gv;  // the triangles with the ids that index P
     const double2 *P;
     const int *unatt, *spos;
     unsigned long long *keys;
@@ -206,7 +211,8 @@ struct EdgeKeys {
         if (!unatt[e]) return;
         int4 E = edges[e];
         int k = base + spos[e];
-        keys[k] = (unsigned long long)__double_as_longlong(rho_edge(P[E.x], P[E.y]));
+        const int4 g = gv[E.z];
+        keys[k] = (unsigned long long)__double_as_longlong(rho_edge(P[geti(g, p1(E.w))], P[geti(g, m1(E.w))]));
         vals[k] = nT + e;
     }
 };
@@ -256,7 +262,8 @@ __device__ __forceinline__ void entry_points(int val, int nT, const int4 *cv, co
         *kind = 3;
     } else {
         int4 E = edges[val - nT];
-        double2 a = P[E.x], b = P[E.y];
+        const int4 g = cv[E.z];  // cv: the triangles with the ids that index P
+        double2 a = P[geti(g, p1(E.w))], b = P[geti(g, m1(E.w))];
         p[0] = a.x; p[1] = a.y; p[2] = b.x; p[3] = b.y;
         *kind = 2;
     }
@@ -522,14 +529,14 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.keys, 0, sizeof(unsigned long long), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vals, 0, sizeof(int), c.stream));
-    launch_n(c, TriKeys{c.cv, c.cn, alpha_positions(c), e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
+    launch_n(c, TriKeys{c.cv, c.cn, alpha_geom_tris(c), c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->err) return c.hctr->err;
-    if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{c.cv, alpha_positions(c), c.list, c.keys, c.ctr}, c.hctr->nlist2);
+    if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{alpha_geom_tris(c), c.opos, c.list, c.keys, c.ctr}, c.hctr->nlist2);
     r = exclusive_scan_int(c, unatt, spos, nE, &c.ctr->nlist);
     if (r) return r;
-    launch_n(c, EdgeKeys{c.edges, alpha_positions(c), unatt, spos, c.keys, c.vals, 1 + nT, nT}, nE);
+    launch_n(c, EdgeKeys{c.edges, alpha_geom_tris(c), c.opos, unatt, spos, c.keys, c.vals, 1 + nT, nT}, nE);
     r = read_counters(c);
     if (r) return r;
     const int nIn = 1 + nT + c.hctr->nlist;
@@ -577,14 +584,14 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     int nunc = c.hctr->nlist;
     if (nunc > 0) {
         GALPHA_CUDA(cudaMemsetAsync(slowflag, 0, sizeof(int) * (size_t)nIn, c.stream));
-        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, c.cv, c.edges, alpha_positions(c), nT, c.ctr,
+        launch_n(c, ExactAdjacent{c.keys, c.vals, nr, slow, slowflag, unc, alpha_geom_tris(c), c.edges, c.opos, nT, c.ctr,
                                   segs ? segs->seg : nullptr},
                  nunc);
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
         if (c.hctr->nlist2 > 0)
-            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, c.cv, c.edges, alpha_positions(c), nIn, nT, c.ctr,
+            launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, alpha_geom_tris(c), c.edges, c.opos, nIn, nT, c.ctr,
                                     segs ? segs->seg : nullptr},
                      c.hctr->nlist2);
     }

@@ -2042,12 +2042,16 @@ struct CompactWrite {
     int4 *cv, *cn;
     gpudtTriangle *out;
     const int *perm;  // internal -> input vertex index (nullptr: identity)
+    int4 *cvi;        // with perm: the triangles with internal ids (alpha-stage geometry)
     __device__ void operator()(long long ii) const
     {
         int t = (int)ii;
         int4 v = tv[t];
         if (v.x < 0) return;
-        if (perm) v = make_int4(perm[v.x], perm[v.y], perm[v.z], 0);
+        if (perm) {
+            cvi[newidx[t]] = make_int4(v.x, v.y, v.z, 0);
+            v = make_int4(perm[v.x], perm[v.y], perm[v.z], 0);
+        }
         int4 n = tn[t];
         int k = newidx[t];
         int nn[3] = {n.x, n.y, n.z};
@@ -2096,18 +2100,11 @@ int ensure_outtri(Ctx &c)
     return GPUDT_OK;
 }
 
-struct PositionsByInput {
-    const double2 *opos;
-    const int *perm;
-    double2 *out;
-    __device__ void operator()(long long v) const { out[perm[v]] = opos[v]; }
-};
-
 void launch_compact_write(Ctx &c, const int *newidx, int nslots)
 {
-    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr}, nslots);
+    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr, c.fwd},
+             nslots);
     c.outtri_ready = true;
-    if (c.renumbered) launch_n(c, PositionsByInput{c.opos, c.perm, c.pos}, c.N);
 }
 
 int stage_compact(Ctx &c)
@@ -2119,11 +2116,8 @@ int stage_compact(Ctx &c)
     r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->nlist);
     if (r) return r;
     // cv / cn only: the gpudtTriangle records are built when a download asks for them
-    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, nullptr, c.renumbered ? c.perm : nullptr}, nt);
+    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, nullptr, c.renumbered ? c.perm : nullptr, c.fwd}, nt);
     c.outtri_ready = false;
-    // the input positions in input order for the alpha stage (pos, the moved
-    // positions of the mesh stages, is not needed any more)
-    if (c.renumbered) launch_n(c, PositionsByInput{c.opos, c.perm, c.pos}, c.N);
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
     if (r) return r;

@@ -432,9 +432,12 @@ int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *o
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n,
                bool *in_second);
 int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);
-// Positions by input index for the alpha stage: input order after a renumbered
-// mesh (written at compaction), else the original positions.
-inline const double2 *alpha_positions(const Ctx &c) { return c.renumbered ? c.pos : c.opos; }
+// Geometry of the compacted mesh for the alpha stage: triangles with the
+// mesh stages' vertex ids (cv holds input ids, which decide edge ownership
+// and index the point intervals; after a spatial numbering the internal ids
+// are kept in fwd, idle once the flips are done) and the positions by those
+// ids (opos).
+inline const int4 *alpha_geom_tris(const Ctx &c) { return c.renumbered ? c.fwd : c.cv; }
 long long radix_scratch_ints(long long n);
 
 // Prefix sums (scan.cu)
