@@ -63,7 +63,12 @@ struct BFirstDistinct {
     __device__ void operator()(long long i) const
     {
         int v = (int)i, s = vset[v], b = sets[s].vbase;
-        if (xy[2 * v] != xy[2 * b] || xy[2 * v + 1] != xy[2 * b + 1]) atomicMin(&first[s], v);
+        const int cand = (xy[2 * v] != xy[2 * b] || xy[2 * v + 1] != xy[2 * b + 1]) ? v : 0x7fffffff;
+        // sets are contiguous: the lanes of a warp share one or two sets, so
+        // one atomic per set and warp instead of one per point
+        const unsigned same = __match_any_sync(__activemask(), s);
+        const int mn = (int)__reduce_min_sync(same, (unsigned)cand);
+        if ((int)(threadIdx.x & 31) == __ffs(same) - 1 && mn != 0x7fffffff && mn < first[s]) atomicMin(&first[s], mn);
     }
 };
 
@@ -79,7 +84,7 @@ struct BCountOffLine {
         if (j == 0x7fffffff) return;
         int o = orient2d_filter(xy[2 * b], xy[2 * b + 1], xy[2 * j], xy[2 * j + 1], xy[2 * v], xy[2 * v + 1]);
         if (o == 2) o = orient2d_exact(xy[2 * b], xy[2 * b + 1], xy[2 * j], xy[2 * j + 1], xy[2 * v], xy[2 * v + 1]);
-        if (o != 0) atomicAdd(&offline[s], 1);
+        if (o != 0 && !offline[s]) offline[s] = 1;  // any point off the line: the set is not collinear
     }
 };
 
