@@ -432,18 +432,27 @@ struct FixPt {
 
 // ------------------------------------------------------- batched segments
 // Set of each value-sorted entry (triangle, or the triangle that owns the edge).
-struct EntrySet {
-    const int *vals;
+// Set of every entry id in entry order (triangles, then edges in triangle
+// order): coalesced reads, so the sorted entries need one gather each.
+struct SetOfEntry {
     const int4 *edges;
     const int *tset;
     int nT;
+    int *eset;
+    __device__ void operator()(long long v) const
+    {
+        eset[v] = tset[v < nT ? (int)v : edges[v - nT].z];
+    }
+};
+
+struct EntrySet {
+    const int *vals;
+    const int *eset;
     unsigned *key;
     int *pos;
     __device__ void operator()(long long i) const
     {
-        int v = vals[i];
-        int t = v < nT ? v : edges[v - nT].z;
-        key[i] = (unsigned)tset[t];
+        key[i] = (unsigned)eset[vals[i]];
         pos[i] = (int)i;
     }
 };
@@ -567,7 +576,9 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
         // stable sort by set: entries end up ordered by (set, value)
         const int m = nIn - 1;
         unsigned *ka = (unsigned *)c.keys2, *kb = ka + ((m + 63) & ~63);
-        launch_n(c, EntrySet{c.vals + 1, c.edges, segs->tset, nT, ka, c.vals2}, m);
+        int *eset = c.inc;  // the incidence / fan store of the mesh stages is free now
+        launch_n(c, SetOfEntry{c.edges, segs->tset, nT, eset}, nT + nE);
+        launch_n(c, EntrySet{c.vals + 1, eset, ka, c.vals2}, m);
         r = radix_sort32(c, ka, c.vals2, kb, c.aux2, m, c.rhist);
         if (r) return r;
         unsigned long long *tk = (unsigned long long *)c.spectrum;
