@@ -243,9 +243,24 @@ def batched_leg(G, D, torch, stream, reps=3):
                 "d2h_bytes": int(d2h)},
         "stages_ms": {nm: float(st.ms[i]) for i, nm in enumerate(
             ["upload", "voronoi", "triangles", "shift", "missing", "boundary", "flip", "compact", "alpha"])},
-        "stats": {k: getattr(st, k) for k in ("nVerts", "nMissing", "nRepairTiles", "nEscalated", "nFlips",
-                                              "flipRounds", "exactOrient", "exactIncircle")},
+        "stats": dict({k: getattr(st, k) for k in ("nVerts", "nMissing", "nRepairTiles", "nEscalated", "nFlips",
+                                                   "flipRounds")}, predicates=predicate_stages(st)),
     }
+
+
+def predicate_stages(st):
+    """Tests per predicate and the stage that decided them: the FP32 filter,
+    the FP64 filter (after FP32 was undecided) or exact expansions; rates are
+    fractions of all tests of that predicate."""
+    out = {}
+    for name, tot, f64, ex in (("incircle", st.incircleTests, st.filteredIncircle, st.exactIncircle),
+                               ("orient", st.orientTests, st.filteredOrient, st.exactOrient)):
+        tot, f64, ex = int(tot), int(f64), int(ex)
+        f32 = tot - f64 - ex
+        out[name] = {"tests": tot, "fp32": f32, "fp64": f64, "exact": ex,
+                     "fp32_undecided_rate": (f64 + ex) / tot if tot else 0.0,
+                     "exact_rate": ex / tot if tot else 0.0}
+    return out
 
 
 def serving_leg(G, D, seconds, rate=2000.0, nslots=6):
@@ -401,8 +416,8 @@ def main():
         stats_sort = (int(st.sortKeys), int(st.sortPasses))
         stats = {k: getattr(st, k) for k in ("nVerts", "nFake", "nDuplicates", "nMissing", "nBadShift", "nIslandPixels",
                                              "nRepairTiles", "nEscalated",
-                                             "nFlips", "flipRounds", "shiftRounds", "missingRounds", "exactOrient",
-                                             "exactIncircle", "filteredIncircle")}
+                                             "nFlips", "flipRounds", "shiftRounds", "missingRounds")}
+        stats["predicates"] = predicate_stages(st)
     torch.cuda.synchronize()
     launches = L.galphaLaunchCount() - launches0
     clk = clocks.stop()

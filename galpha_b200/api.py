@@ -72,7 +72,8 @@ class Status(ctypes.Structure):
         ("shiftRounds", ctypes.c_int), ("missingRounds", ctypes.c_int),
         ("nRepairTiles", ctypes.c_int), ("nEscalated", ctypes.c_int), ("nEnvelopeCells", ctypes.c_int),
         ("exactOrient", ctypes.c_longlong), ("exactIncircle", ctypes.c_longlong),
-        ("filteredIncircle", ctypes.c_longlong),
+        ("filteredIncircle", ctypes.c_longlong), ("incircleTests", ctypes.c_longlong),
+        ("orientTests", ctypes.c_longlong), ("filteredOrient", ctypes.c_longlong),
         ("ms", ctypes.c_float * 12),
         ("kernelMs", ctypes.c_float * 4),
         ("sortKeys", ctypes.c_longlong), ("sortPasses", ctypes.c_int), ("pad0", ctypes.c_int),

@@ -48,6 +48,21 @@ int read_counters(Ctx &c)
     return GPUDT_OK;
 }
 
+// Predicate stage counts of the last run (counter block already read).
+static void fill_predicate_stats(Ctx &c)
+{
+    const Counters &h = *c.hctr;
+    c.st.exactOrient = (long long)h.exact_orient;
+    c.st.exactIncircle = (long long)h.exact_incircle;
+    c.st.filteredIncircle = c.st.incircleTests = c.st.orientTests = c.st.filteredOrient = 0;
+    for (int k = 0; k < 64; k++) {
+        c.st.filteredIncircle += (long long)h.filt_spread[k];
+        c.st.incircleTests += (long long)h.icc_spread[k];
+        c.st.orientTests += (long long)h.ori_spread[k];
+        c.st.filteredOrient += (long long)h.ori64_spread[k];
+    }
+}
+
 int read_small(Ctx &c, void *host_dst, const void *dev_src, size_t bytes)
 {
     if (bytes == 0) return GPUDT_OK;
@@ -282,10 +297,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     if (c.hctr->err) return stage_fail(c, c.hctr->err, "final");
     c.st.nVerts = c.V;
     c.st.nFake = c.F;
-    c.st.exactOrient = (long long)c.hctr->exact_orient;
-    c.st.exactIncircle = (long long)c.hctr->exact_incircle;
-    c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
-    for (int k = 0; k < 64; k++) c.st.filteredIncircle += (long long)c.hctr->filt_spread[k];
+    fill_predicate_stats(c);
     c.have_mesh = true;
     return GPUDT_OK;
 }
@@ -377,10 +389,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     if (c.hctr->err) return stage_fail(c, c.hctr->err, "final");
     c.st.nVerts = c.V;
     c.st.nFake = c.F;
-    c.st.exactOrient = (long long)c.hctr->exact_orient;
-    c.st.exactIncircle = (long long)c.hctr->exact_incircle;
-    c.st.filteredIncircle = (long long)c.hctr->filt_incircle;
-    for (int k = 0; k < 64; k++) c.st.filteredIncircle += (long long)c.hctr->filt_spread[k];
+    fill_predicate_stats(c);
     bh.valid = true;
     return GPUDT_OK;
 }

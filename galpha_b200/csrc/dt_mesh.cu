@@ -42,30 +42,44 @@
 namespace galpha {
 
 // ------------------------------------------------------------ small helpers
-__device__ __forceinline__ int orientv(const double2 *P, int a, int b, int c, Counters *ct)
-{
-    double2 A = P[a], B = P[b], C = P[c];
-    int s = orient2d_filter(A.x, A.y, B.x, B.y, C.x, C.y);
-    if (s != 2) return s;
-    atomicAdd(&ct->exact_orient, 1ull);
-    s = orient2d_exact(A.x, A.y, B.x, B.y, C.x, C.y);
-    if (s == EXACT_OVERFLOW) {
-        set_err(ct, GPUDT_ERR_EXACT, 1);
-        return 0;
+// Orientation tests of one thread, added to the counters once (in a walk, an
+// atomic per test costs more than the FP32 test it counts).
+struct OrientTally {
+    int tests = 0, fp64 = 0;
+    __device__ __forceinline__ void flush(Counters *ct) const
+    {
+        warp_add_spread(ct->ori_spread, tests);
+        warp_add_spread(ct->ori64_spread, fp64);
     }
-    return s;
-}
+};
 
-__device__ __forceinline__ int orientp(double2 A, double2 B, double2 C, Counters *ct)
+// Staged orientation: FP32 filter, FP64 filter, exact.
+__device__ __forceinline__ int orient_staged(double2 A, double2 B, double2 C, Counters *ct, OrientTally &n)
 {
-    int s = orient2d_filter(A.x, A.y, B.x, B.y, C.x, C.y);
+    n.tests++;
+    int s = orient2d_filter32(A.x, A.y, B.x, B.y, C.x, C.y);
     if (s != 2) return s;
+    s = orient2d_filter(A.x, A.y, B.x, B.y, C.x, C.y);
+    if (s != 2) {
+        n.fp64++;
+        return s;
+    }
     atomicAdd(&ct->exact_orient, 1ull);
     s = orient2d_exact(A.x, A.y, B.x, B.y, C.x, C.y);
     if (s == EXACT_OVERFLOW) {
         set_err(ct, GPUDT_ERR_EXACT, 2);
         return 0;
     }
+    return s;
+}
+
+// One counted test (call sites outside loops).
+__device__ __forceinline__ int orientp(double2 A, double2 B, double2 C, Counters *ct)
+{
+    OrientTally n;
+    const int s = orient_staged(A, B, C, ct, n);
+    warp_count_spread(ct->ori_spread);
+    if (n.fp64) warp_count_spread(ct->ori64_spread);
     return s;
 }
 
@@ -320,15 +334,17 @@ struct ShiftRound {
         uint32_t pv = prio((uint32_t)v);
         bool wait = false, ok = true;
         double2 q = opos[v];
+        OrientTally tally;
         bool fine = walk_fan(tv, tn, vtri[v], [&](int t, int i, int a, int b) {
             int ra = vround[a];
             if ((ra == 0 || ra == round) && prio((uint32_t)a) < pv) {
                 wait = true;
                 return false;
             }
-            if (ok && orientp(q, pos[a], pos[b], ct) <= 0) ok = false;
+            if (ok && orient_staged(q, pos[a], pos[b], ct, tally) <= 0) ok = false;
             return true;
         });
+        tally.flush(ct);
         if (!fine) {
             set_err(ct, GPUDT_ERR_TOPOLOGY, 40);
             return;
@@ -719,8 +735,8 @@ int stage_shift(Ctx &c)
 // Straight-line walk from vertex a to point q.  Returns the triangle and the
 // location kind: 0 inside, 1 on the edge opposite vtx[k] (k in *edge),
 // 2 on vertex vtx[k] (coincident), -1 failure.
-__device__ int locate(const int4 *tv, const int4 *tn, const double2 *P, const int *vtri, int a, double2 q,
-                      int *tri, int *edge, Counters *ct)
+__device__ int locate_walk(const int4 *tv, const int4 *tn, const double2 *P, const int *vtri, int a, double2 q,
+                           int *tri, int *edge, Counters *ct, OrientTally &n)
 {
     int budget = 1 << 22;  // total walk steps over all restarts
     for (int restart = 0; restart < 4096; restart++) {
@@ -740,7 +756,7 @@ __device__ int locate(const int4 *tv, const int4 *tn, const double2 *P, const in
                 int tt = dtri(e), i = dori(e);
                 int4 w = tv[tt];
                 int b = geti(w, p1(i)), c = geti(w, m1(i));
-                if (orientp(A, P[b], q, ct) >= 0 && orientp(A, P[c], q, ct) <= 0) {
+                if (orient_staged(A, P[b], q, ct, n) >= 0 && orient_staged(A, P[c], q, ct, n) <= 0) {
                     t = tt;
                     ia = i;
                     break;
@@ -756,7 +772,7 @@ __device__ int locate(const int4 *tv, const int4 *tn, const double2 *P, const in
         int4 w = tv[t];
         int b = geti(w, p1(ia)), c = geti(w, m1(ia));
         int cross = ia;  // index (in t) of the vertex opposite the edge to cross
-        if (orientp(P[b], P[c], q, ct) >= 0) {
+        if (orient_staged(P[b], P[c], q, ct, n) >= 0) {
             goto classify_t;
         }
         for (; budget > 0; budget--) {
@@ -767,9 +783,9 @@ __device__ int locate(const int4 *tv, const int4 *tn, const double2 *P, const in
             int j = dori(nx);
             w = tv[t];
             int d = geti(w, j);  // new triangle (d, c, b)
-            int o1 = orientp(P[b], P[d], q, ct), o2 = orientp(P[d], P[c], q, ct);
+            int o1 = orient_staged(P[b], P[d], q, ct, n), o2 = orient_staged(P[d], P[c], q, ct, n);
             if (o1 >= 0 && o2 >= 0) goto classify_t;
-            int od = orientp(A, q, P[d], ct);
+            int od = orient_staged(A, q, P[d], ct, n);
             if (od > 0) {
                 // exit through (b, d): opposite c = vtx[p1(j)]
                 c = d;
@@ -789,7 +805,7 @@ __device__ int locate(const int4 *tv, const int4 *tn, const double2 *P, const in
         int x[3] = {v.x, v.y, v.z};
         int o[3], zeros = 0, zk = -1, nzk = -1;
         for (int k = 0; k < 3; k++) {
-            o[k] = orientp(P[x[p1(k)]], P[x[m1(k)]], q, ct);
+            o[k] = orient_staged(P[x[p1(k)]], P[x[m1(k)]], q, ct, n);
             if (o[k] < 0) return -1;
             if (o[k] == 0) {
                 zeros++;
@@ -837,7 +853,9 @@ struct MissingLocate {
         for (int g = 0; g < 64 && a >= 0 && vtri[a] < 0; g++) a = anchor[a];
         if (a < 0 || vtri[a] < 0) a = fallback;
         int t, e;
-        int k = locate(tv, tn, pos, vtri, a, opos[m], &t, &e, ct);
+        OrientTally tally;
+        int k = locate_walk(tv, tn, pos, vtri, a, opos[m], &t, &e, ct, tally);
+        tally.flush(ct);
         kind[ii] = k;
         if (k < 0) {
             set_err(ct, GPUDT_ERR_TOPOLOGY, 60);
@@ -1392,10 +1410,11 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
                     set_link(a.tn, ownv, loc);
                 }
             };
+            OrientTally tally;
             for (int k = 0; k <= d; k++) {
                 const int wv = U[k];
                 int wown = k > 0 ? -2 - (k - 1) : -1;  // chain edge U[k-1] -> U[k]: fan triangle k-1
-                while (top >= 2 && orientp(P[S[top - 2]], P[S[top - 1]], P[k], a.ct) > 0) {
+                while (top >= 2 && orient_staged(P[S[top - 2]], P[S[top - 1]], P[k], a.ct, tally) > 0) {
                     const int s = Fs[used++];
                     const int A = U[S[top - 2]], B = U[S[top - 1]];
                     a.tv[s] = make_int4(A, B, wv, 0);
@@ -1414,6 +1433,7 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
                 SO[top] = wown;
                 top++;
             }
+            tally.flush(a.ct);
             s_top = top;
             s_used = used;
             s_rbase = rbase;
@@ -1748,7 +1768,7 @@ struct FlipCheck {
     {
         const int t = act ? act[ii] : (int)ii;  // no list: every slot (the first round)
         const int4 v = tv[t];
-        int ci = -1, cu = -1, nfilt = 0;
+        int ci = -1, cu = -1, ntest = 0, nfilt = 0;
         bool err = false;
         // the first round tests every edge once (from the lower slot); later
         // rounds test the edges a flip or a lost vote left marked
@@ -1767,13 +1787,17 @@ struct FlipCheck {
                 const int d = geti(tv[u], dori(e));
                 const double2 A = P[p1(i)], B = P[m1(i)], C = P[i], D = pos[d];
                 double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
-                int s = incircle_filter(pa, pb, pc, pd);
+                ntest++;
+                int s = incircle_filter32(pa, pb, pc, pd);
                 if (s == 2) {
-                    atomicAdd(&ct->exact_incircle, 1ull);
-                    s = incircle_exact(pa, pb, pc, pd);
-                    if (s == EXACT_OVERFLOW) err = true;
-                } else {
-                    nfilt++;
+                    s = incircle_filter(pa, pb, pc, pd);
+                    if (s == 2) {
+                        atomicAdd(&ct->exact_incircle, 1ull);
+                        s = incircle_exact(pa, pb, pc, pd);
+                        if (s == EXACT_OVERFLOW) err = true;
+                    } else {
+                        nfilt++;
+                    }
                 }
                 if (!err && s > 0) {
                     ci = i;
@@ -1782,6 +1806,7 @@ struct FlipCheck {
             }
         }
         if (err) set_err(ct, GPUDT_ERR_EXACT, 90);
+        warp_add_spread(ct->icc_spread, ntest);
         warp_add_spread(ct->filt_spread, nfilt);
         const bool has = ci >= 0;
         if (act && !has && fl) eflag[t] = 0;  // every marked edge is locally Delaunay

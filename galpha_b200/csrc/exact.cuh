@@ -1,10 +1,12 @@
 // exact.cuh -- staged exact geometric predicates for the galpha-b200 kernels.
 //
-// Each predicate is staged: an FP64 evaluation with Shewchuk's certified
-// error bound decides almost every call; the rare undecided call falls through
-// to an exact evaluation in floating-point expansion arithmetic (Shewchuk,
-// "Adaptive Precision Floating-Point Arithmetic and Fast Robust Geometric
-// Predicates", 1997).  The reference's device predicates stop at the filter
+// Each mesh predicate is staged: an FP32 evaluation with a certified error
+// bound (orient2d_filter32, incircle_filter32) decides almost every call; an
+// undecided call goes to the FP64 evaluation with Shewchuk's certified error
+// bound; the rare call that is still undecided falls through to an exact
+// evaluation in floating-point expansion arithmetic (Shewchuk, "Adaptive
+// Precision Floating-Point Arithmetic and Fast Robust Geometric Predicates",
+// 1997).  The reference's device predicates stop at the filter
 // for in-circle (gpudt/Cuda/cudaCCW.h:484-524 returns "unsure") and hand the
 // edge to the host (gpudt.cpp:879-914); here the exact stage runs on the
 // device, so no host hand-off exists.
@@ -26,6 +28,26 @@ constexpr double kEps = 1.1102230246251565e-16;  // 2^-53
 constexpr double kCcwErrA = (3.0 + 16.0 * kEps) * kEps;
 constexpr double kIccErrA = (10.0 + 96.0 * kEps) * kEps;
 constexpr int EXACT_OVERFLOW = 0x7fff;
+
+// FP32 stage.  Its inputs are the FP64 coordinate differences rounded to
+// FP32, so each carries a relative error u <= 2^-24 + 2^-53 (two roundings)
+// where Shewchuk's analysis assumes 2^-24; every later operation rounds once
+// (an FMA contraction only removes roundings).  Shewchuk's relative bounds
+// for the same expression trees are 3 eps (orient2d) and 10 eps (in-circle);
+// the constants below are at least twice those.  Underflow adds an absolute
+// error below 2^-126 per FP32 operation or conversion (2^-150 with gradual
+// underflow; 2^-126 also covers flush-to-zero).  Weighted by the largest
+// factor each error is later multiplied by, with every difference at most
+// M = 2^10 in magnitude, those terms total below (4M + 3) 2^-126 < 2^-113 for
+// orient2d and (48 M^3 + 36 M^2 + 5) 2^-126 < 2^-90 for in-circle; the
+// absolute allowances below are 8 and 16 times those.  A call with a larger
+// difference, a NaN or an infinity starts at the FP64 stage.
+constexpr float kEps32 = 5.9604644775390625e-08f;  // 2^-24
+constexpr float kCcwErrF = 8.0f * kEps32;
+constexpr float kIccErrF = 20.0f * kEps32;
+constexpr float kCcwAbsF = 0x1p-110f;
+constexpr float kIccAbsF = 0x1p-86f;
+constexpr double kF32Span = 1024.0;  // largest coordinate difference the FP32 stage takes
 
 GALPHA_HD void two_sum(double a, double b, double &x, double &y)
 {
@@ -208,10 +230,28 @@ GALPHA_HD int orient2d_filter(double ax, double ay, double bx, double by, double
     return 2;
 }
 
+// FP32 stage of orient2d; returns 2 when undecided (a zero determinant is
+// always left to the FP64 stage).
+GALPHA_HD int orient2d_filter32(double ax, double ay, double bx, double by, double cx, double cy)
+{
+    const double dax = ax - cx, day = ay - cy, dbx = bx - cx, dby = by - cy;
+    if (!(fabs(dax) <= kF32Span && fabs(day) <= kF32Span && fabs(dbx) <= kF32Span && fabs(dby) <= kF32Span))
+        return 2;
+    const float acx = (float)dax, acy = (float)day, bcx = (float)dbx, bcy = (float)dby;
+    const float l = acx * bcy, r = acy * bcx;
+    const float det = l - r;
+    const float bound = kCcwErrF * (fabsf(l) + fabsf(r)) + kCcwAbsF;
+    if (det > bound) return 1;
+    if (-det > bound) return -1;
+    return 2;
+}
+
 // Orientation sign (>0 counterclockwise).  *nexact counts exact fall-throughs.
 GALPHA_HD int orient2d(double ax, double ay, double bx, double by, double cx, double cy, int *nexact)
 {
-    int s = orient2d_filter(ax, ay, bx, by, cx, cy);
+    int s = orient2d_filter32(ax, ay, bx, by, cx, cy);
+    if (s != 2) return s;
+    s = orient2d_filter(ax, ay, bx, by, cx, cy);
     if (s != 2) return s;
     if (nexact) (*nexact)++;
     return orient2d_exact(ax, ay, bx, by, cx, cy);
@@ -282,9 +322,36 @@ GALPHA_HD int incircle_filter(const double *a, const double *b, const double *c,
     return 2;
 }
 
+// FP32 stage of the in-circle test (same expression tree as incircle_filter);
+// returns 2 when undecided.
+GALPHA_HD int incircle_filter32(const double *a, const double *b, const double *c, const double *d)
+{
+    const double ex = a[0] - d[0], ey = a[1] - d[1], fx = b[0] - d[0], fy = b[1] - d[1];
+    const double gx = c[0] - d[0], gy = c[1] - d[1];
+    if (!(fabs(ex) <= kF32Span && fabs(ey) <= kF32Span && fabs(fx) <= kF32Span && fabs(fy) <= kF32Span &&
+          fabs(gx) <= kF32Span && fabs(gy) <= kF32Span))
+        return 2;
+    const float adx = (float)ex, ady = (float)ey, bdx = (float)fx, bdy = (float)fy, cdx = (float)gx, cdy = (float)gy;
+    const float bdxcdy = bdx * cdy, cdxbdy = cdx * bdy;
+    const float alift = adx * adx + ady * ady;
+    const float cdxady = cdx * ady, adxcdy = adx * cdy;
+    const float blift = bdx * bdx + bdy * bdy;
+    const float adxbdy = adx * bdy, bdxady = bdx * ady;
+    const float clift = cdx * cdx + cdy * cdy;
+    const float det = alift * (bdxcdy - cdxbdy) + blift * (cdxady - adxcdy) + clift * (adxbdy - bdxady);
+    const float permanent = (fabsf(bdxcdy) + fabsf(cdxbdy)) * alift + (fabsf(cdxady) + fabsf(adxcdy)) * blift +
+                            (fabsf(adxbdy) + fabsf(bdxady)) * clift;
+    const float bound = kIccErrF * permanent + kIccAbsF;
+    if (det > bound) return 1;
+    if (-det > bound) return -1;
+    return 2;
+}
+
 GALPHA_HD int incircle(const double *a, const double *b, const double *c, const double *d, int *nexact)
 {
-    int s = incircle_filter(a, b, c, d);
+    int s = incircle_filter32(a, b, c, d);
+    if (s != 2) return s;
+    s = incircle_filter(a, b, c, d);
     if (s != 2) return s;
     if (nexact) (*nexact)++;
     return incircle_exact(a, b, c, d);

@@ -55,9 +55,12 @@ struct Counters {
     unsigned long long exact_compares;
     unsigned long long exact_orient;
     unsigned long long exact_incircle;
-    unsigned long long filt_incircle;
     unsigned long long exact_attached;
-    unsigned long long filt_spread[64];  // in-circle tests decided by the filter, spread over 64 counters
+    // predicate stage counts, each spread over 64 counters (one per warp id mod 64)
+    unsigned long long filt_spread[64];  // in-circle tests decided by the FP64 filter
+    unsigned long long icc_spread[64];   // in-circle tests, all stages
+    unsigned long long ori_spread[64];   // orientation tests of the mesh stages, all stages
+    unsigned long long ori64_spread[64]; // orientation tests decided by the FP64 filter
     int qcount[12];  // alpha query: [type*4 + class], type 0 points, 1 edges, 2 triangles
     int qrank;       // alpha query: largest spectrum rank <= alpha (-1 if alpha < 0)
     int qpad;
@@ -276,6 +279,14 @@ __device__ __forceinline__ void warp_add_spread(unsigned long long *arr, int cnt
     const int tot = __reduce_add_sync(m, cnt);
     if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && tot)
         atomicAdd(&arr[((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & 63], (unsigned long long)tot);
+}
+
+// Counts one event per calling lane (one atomic per converged group of lanes).
+__device__ __forceinline__ void warp_count_spread(unsigned long long *arr)
+{
+    const unsigned m = __activemask();
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1)
+        atomicAdd(&arr[((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & 63], (unsigned long long)__popc(m));
 }
 
 // Reserves cnt consecutive slots of *counter for every calling thread with one

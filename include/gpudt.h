@@ -83,9 +83,14 @@ typedef struct {
     int nRepairTiles;        /* fused-path tiles with islands, repaired locally */
     int nEscalated;          /* textures (point sets) redone on the envelope path */
     int nEnvelopeCells;      /* textures (point sets) coloured on the envelope path */
+    /* Predicate stages (FP32 filter -> FP64 filter -> exact expansion).  A test
+     * decided by the FP32 filter is counted in the total only. */
     long long exactOrient;   /* orientation tests that needed exact arithmetic */
     long long exactIncircle; /* in-circle tests that needed exact arithmetic */
     long long filteredIncircle; /* in-circle tests decided by the FP64 filter */
+    long long incircleTests;    /* in-circle tests (flip stage), all stages */
+    long long orientTests;      /* orientation tests of the mesh stages, all stages */
+    long long filteredOrient;   /* orientation tests decided by the FP64 filter */
     float ms[12];            /* stage times (CUDA events), see galpha.h GALPHA_STAGE_* */
     float kernelMs[4];       /* single-kernel times (CUDA events on the launch stream):
                                 [0] colour + dual-triangle kernel (k_vd_tri; k_row_pass on

@@ -165,7 +165,8 @@ def test_c3_degenerate_properties(engine):
     duplicates and cocircular quads; texture 8192, about 7.5M sites inserted
     after the Voronoi stage): exact validity of the full mesh, exactly the
     lowest input index of each group of exact duplicates as vertex, the Euler
-    count, and a spectrum that increases strictly with every rank in range."""
+    count, the predicate stage counts, and a spectrum that increases strictly
+    with every rank in range."""
     pts, fbo = D.make("c3")
     dt = run(engine, pts, fbo)
     chk = O.check_mesh(pts, dt.vtx, dt.tri)
@@ -174,6 +175,12 @@ def test_c3_degenerate_properties(engine):
     _, first = np.unique(pts, axis=0, return_index=True)
     assert np.array_equal(verts, np.sort(first))
     assert dt.nTris == 2 * len(verts) - 2 - chk["hull_edges"]
+    # predicate stages: the FP32 filter decides nearly every test; the exact
+    # lattice degeneracies (collinear rows, cocircular quads) reach the later stages
+    st = dt.status
+    for tests, f64, ex in ((st.incircleTests, st.filteredIncircle, st.exactIncircle),
+                           (st.orientTests, st.filteredOrient, st.exactOrient)):
+        assert tests > 10 ** 7 and 0 < f64 and 0 < ex and f64 + ex < 0.05 * tests
     a = engine.alpha_resident()
     s = a["spectrum"]
     assert s[0] == 0.0 and np.all(np.diff(s[1:]) > 0)
