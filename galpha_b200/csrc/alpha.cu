@@ -541,7 +541,7 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     launch_n(c, TriKeys{c.cv, c.cn, alpha_geom_tris(c), c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
     r = read_counters(c);
     if (r) return r;
-    if (c.hctr->err) return c.hctr->err;
+    if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
     if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{alpha_geom_tris(c), c.opos, c.list, c.keys, c.ctr}, c.hctr->nlist2);
     r = exclusive_scan_int(c, unatt, spos, nE, &c.ctr->nlist);
     if (r) return r;
@@ -600,7 +600,7 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
                  nunc);
         r = read_counters(c);
         if (r) return r;
-        if (c.hctr->err) return c.hctr->err;
+        if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
         if (c.hctr->nlist2 > 0)
             launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, alpha_geom_tris(c), c.edges, c.opos, nIn, nT, c.ctr,
                                     segs ? segs->seg : nullptr},
@@ -628,7 +628,7 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
     if (r) return r;
-    if (c.hctr->err) return c.hctr->err;
+    if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
     c.nSpec = c.hctr->nlist + (segs ? segs->K : 1);  // distinct ranks incl. the sentinel(s)
     return GPUDT_OK;
 }

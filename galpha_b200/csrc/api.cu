@@ -147,7 +147,8 @@ static size_t plan(const Sizes &z, Ctx *c, Arena *A)
     TAKE(inc, int, 3 * cap);
     TAKE(tilecount, int, z.ntiles + 1);
     TAKE(hist, int, 65536);
-    TAKE(rhist, int, radix_scratch_ints((long long)(3 * cap)) + 16);
+    TAKE(rhist, int, radix_sort_scratch_ints((long long)(3 * cap)) + 16);
+    if (c) c->rhist_ints = radix_sort_scratch_ints((long long)(3 * cap)) + 16;
     TAKE(e_off, int, cap + 1);
     TAKE(edges, int4, 2 * cap);
     TAKE(edge_ro, int, 2 * cap);
@@ -232,7 +233,7 @@ static void ev_record(Ctx &c, int k)
 static int fbo_ok(int T) { return T >= 256 && T <= 16384 && (T & (T - 1)) == 0; }
 
 // Records which stage failed and the device-side detail code.
-static int stage_fail(Ctx &c, int r, const char *stage)
+int stage_fail(Ctx &c, int r, const char *stage)
 {
     if (r == GPUDT_ERR_CUDA || r == GPUDT_ERR_NOMEM) {
         if (g_err.find(stage) == std::string::npos) g_err = std::string(stage) + ": " + g_err;

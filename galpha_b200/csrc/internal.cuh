@@ -67,6 +67,7 @@ struct Counters {
     double qalpha;   // alpha query: the alpha value classified
     int tail_rounds; // flip: rounds run by the last in-block tail launch
     int runstage;    // fake runs: staged fan entries
+    int nlong;       // key sort: out-of-order pairs recorded in groups too long for one thread
 };
 
 // Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
@@ -156,6 +157,7 @@ struct Ctx {
     bool have_master = false;
     int *hist = nullptr;       // scan scratch
     int *rhist = nullptr;      // radix sort histograms
+    long long rhist_ints = 0;  // its size
     gpudtTriangle *outtri = nullptr;  // [cap] AoS output staging
     bool outtri_ready = false;          // outtri holds the current mesh (built on the first download)
     galphaEdgeInterval *edge_aos = nullptr;  // [2*cap] edge records for download
@@ -193,6 +195,8 @@ int read_counters(Ctx &c);
 // kernel writes into mapped pinned memory, so the read never queues behind
 // large copies on the copy engines; synchronises the handle's stream.
 int read_small(Ctx &c, void *host_dst, const void *dev_src, size_t bytes);
+// Records the failing stage and the device-side detail code (galphaLastError).
+int stage_fail(Ctx &c, int r, const char *stage);
 constexpr size_t kMailBytes = 65536;
 
 // Kernel launches issued by this library (all handles, all threads).
@@ -450,6 +454,7 @@ int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int
 // ids (opos).
 inline const int4 *alpha_geom_tris(const Ctx &c) { return c.renumbered ? c.fwd : c.cv; }
 long long radix_scratch_ints(long long n);
+long long radix_sort_scratch_ints(long long n);  // radix_sort and radix_sort32 of n keys
 
 // Prefix sums (scan.cu)
 int exclusive_scan_int(Ctx &c, const int *in, int *out, int n, int *total_dev);

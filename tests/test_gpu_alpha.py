@@ -51,6 +51,23 @@ def test_random_alpha(engine, seed):
         assert ok, rep
 
 
+def test_long_key_group(engine):
+    """A lattice whose unit edges share one spectrum value, with a few points
+    moved by about 1e-12 so that some edge keys agree with it in their top 40
+    bits but not below: a group of equal top bits far longer than one thread
+    fixes up, out of order, sorted as a sub-array (fewer passes than a full
+    64-bit sort); the spectrum and intervals match the oracle."""
+    rng = np.random.default_rng(77)
+    g = np.arange(60) / 128.0
+    pts = np.stack(np.meshgrid(g, g), -1).reshape(-1, 2).copy()
+    moved = rng.choice(len(pts), 60, replace=False)
+    pts[moved, 0] += rng.choice([-1.0, 1.0], 60) * rng.uniform(1e-12, 3e-12, 60)
+    dt, a = engine.compute_all(G.GPUDTParams(pts, fboSize=1024))
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+    assert ok, rep
+    assert 5 < dt.status.sortPasses < 13, dt.status.sortPasses
+
+
 def test_alpha_of_host_mesh_matches_resident(engine):
     pts = np.random.default_rng(11).random((5000, 2))
     p, dt, a = both(engine, pts, 1024)
