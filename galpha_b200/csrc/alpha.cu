@@ -318,10 +318,13 @@ struct ExactAdjacent {
     }
 };
 
-// Rare path: one thread sorts a whole run with the exact comparator and
-// recomputes its rank-start flags.  Runs longer than kMaxSlowRun are refused
-// (GPUDT_ERR_EXACT) rather than sorted in quadratic time.
-constexpr int kMaxSlowRun = 16384;
+// Rare path: a run with an order violation is re-sorted with the exact
+// comparator and its rank-start flags recomputed: one thread per run of at
+// most kThreadRun entries (insertion sort), one block per longer run
+// (k_resolve_long: merge sort).  Runs longer than kMaxSlowRun are refused
+// (GPUDT_ERR_EXACT).
+constexpr int kThreadRun = 512;
+constexpr int kMaxSlowRun = 1 << 22;
 struct ResolveRuns {
     unsigned long long *keys;
     int *vals, *nr;
@@ -331,14 +334,17 @@ struct ResolveRuns {
     int n, nT;
     Counters *ct;
     const int *seg;
+    int *longs;  // runs longer than kThreadRun, for k_resolve_long (count in ct->nlong)
     __device__ void operator()(long long ii) const
     {
         int s = runs[ii];
         int e = s;
-        while (e + 1 < n && (!seg || seg[e] == seg[e + 1]) && near_equal(keys[e], keys[e + 1])) e++;
-        if (e - s > kMaxSlowRun) {
-            set_err(ct, GPUDT_ERR_EXACT, 113);
-            return;
+        while (e + 1 < n && (!seg || seg[e] == seg[e + 1]) && near_equal(keys[e], keys[e + 1])) {
+            e++;
+            if (e - s >= kThreadRun) {
+                longs[atomicAdd(&ct->nlong, 1)] = s;
+                return;
+            }
         }
         for (int a = s + 1; a <= e; a++) {
             unsigned long long kc = keys[a];
@@ -367,6 +373,117 @@ struct ResolveRuns {
         }
     }
 };
+
+// Order of two spectrum entries: by key where the keys are more than 2 ulp
+// apart (each carries at most 1 ulp of error), else exactly.
+__device__ __forceinline__ int cmp_entries(unsigned long long ka, int va, unsigned long long kb, int vb, int nT,
+                                           const int4 *cv, const int4 *edges, const double2 *P)
+{
+    if (ka < kb && !near_equal(ka, kb)) return -1;
+    if (kb < ka && !near_equal(kb, ka)) return 1;
+    return exact_cmp_vals(va, vb, nT, cv, edges, P);
+}
+
+// One block per long run starting at runs[blockIdx.x]: the run's end by
+// block-wide scans, a stable bottom-up merge sort of (keys, vals)[s..e] with
+// the exact comparator (each thread merges a share of the outputs from a
+// merge-path split found by binary search; ties take the left run first),
+// through (tk, tv)[s..e] as the second buffer, then the rank-start flags.
+constexpr int kLongThreads = 256;
+__global__ void __launch_bounds__(kLongThreads) k_resolve_long(unsigned long long *keys, int *vals, int *nr,
+                                                               unsigned long long *tk, int *tv, const int *runs,
+                                                               const int4 *cv, const int4 *edges, const double2 *P,
+                                                               int n, int nT, Counters *ct, const int *seg)
+{
+    __shared__ int red[kLongThreads / 32];
+    __shared__ int s_end;
+    const int s = runs[blockIdx.x];
+    if (threadIdx.x == 0) s_end = n - 1;
+    __syncthreads();
+    // the run ends before the first j > s that is not linked to j - 1
+    for (long long w0 = s + 1; w0 < n; w0 += kLongThreads) {
+        const long long j = w0 + threadIdx.x;
+        const bool brk = j < n && (!((!seg || seg[j - 1] == seg[j]) && near_equal(keys[j - 1], keys[j])));
+        int m = __reduce_min_sync(0xffffffffu, brk ? (int)j : n);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        m = red[0];
+        for (int q = 1; q < kLongThreads / 32; q++) m = min(m, red[q]);
+        __syncthreads();
+        if (m < n) {
+            if (threadIdx.x == 0) s_end = m - 1;
+            break;
+        }
+    }
+    __syncthreads();
+    const int e = s_end, L = e - s + 1;
+    if (L > kMaxSlowRun) {
+        if (threadIdx.x == 0) set_err(ct, GPUDT_ERR_EXACT, 113);
+        return;
+    }
+    bool bad = false;
+    unsigned long long *sk = keys + s, *dk = tk + s;
+    int *sv = vals + s, *dv = tv + s;
+    const int chunk = (L + kLongThreads - 1) / kLongThreads;
+    for (int w = 1; w < L; w <<= 1) {
+        const int o0 = min(L, (int)threadIdx.x * chunk), o1 = min(L, o0 + chunk);
+        for (int pos = o0; pos < o1;) {
+            const int lo = pos / (2 * w) * (2 * w), mid = min(L, lo + w), hi = min(L, lo + 2 * w);
+            const int na = mid - lo, nb = hi - mid;
+            const int k0 = pos - lo, kend = min(o1, hi) - lo;
+            // merge-path split of diagonal k0: i elements of A before it
+            int a0 = max(0, k0 - nb), a1 = min(k0, na);
+            while (a0 < a1) {
+                const int m = (a0 + a1) >> 1;
+                int c = cmp_entries(sk[lo + m], sv[lo + m], sk[mid + k0 - m - 1], sv[mid + k0 - m - 1], nT, cv, edges, P);
+                if (c == EXACT_OVERFLOW) {
+                    bad = true;
+                    c = 0;
+                }
+                if (c <= 0) a0 = m + 1;
+                else a1 = m;
+            }
+            int i = a0, j = k0 - a0;
+            for (int k = k0; k < kend; k++) {
+                bool takeA = i < na;
+                if (takeA && j < nb) {
+                    int c = cmp_entries(sk[lo + i], sv[lo + i], sk[mid + j], sv[mid + j], nT, cv, edges, P);
+                    if (c == EXACT_OVERFLOW) {
+                        bad = true;
+                        c = 0;
+                    }
+                    takeA = c <= 0;
+                }
+                const int src = takeA ? lo + i++ : mid + j++;
+                dk[lo + k] = sk[src];
+                dv[lo + k] = sv[src];
+            }
+            pos = lo + kend;
+        }
+        __syncthreads();  // every output of this level written before the next reads it
+        unsigned long long *t1 = sk;
+        sk = dk;
+        dk = t1;
+        int *t2 = sv;
+        sv = dv;
+        dv = t2;
+    }
+    if (sk != keys + s)  // the last level wrote the second buffer
+        for (int k = threadIdx.x; k < L; k += kLongThreads) {
+            keys[s + k] = sk[k];
+            vals[s + k] = sv[k];
+        }
+    __syncthreads();
+    for (int a = s + 1 + threadIdx.x; a <= e; a += kLongThreads) {
+        int cmp = exact_cmp_vals(vals[a - 1], vals[a], nT, cv, edges, P);
+        if (cmp == EXACT_OVERFLOW) {
+            bad = true;
+            cmp = 1;
+        }
+        nr[a] = cmp != 0 ? 1 : 0;
+    }
+    if (bad) set_err(ct, GPUDT_ERR_EXACT, 111);
+}
 
 struct ScatterRanks {
     const unsigned long long *keys;
@@ -601,10 +718,26 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
-        if (c.hctr->nlist2 > 0)
+        if (c.hctr->nlist2 > 0) {
+            // runs longer than kThreadRun are listed after the slow runs
+            const int nslow = c.hctr->nlist2;
+            int *longs = slow + nslow;
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlong, 0, sizeof(int), c.stream));
             launch_n(c, ResolveRuns{c.keys, c.vals, nr, slow, alpha_geom_tris(c), c.edges, c.opos, nIn, nT, c.ctr,
-                                    segs ? segs->seg : nullptr},
-                     c.hctr->nlist2);
+                                    segs ? segs->seg : nullptr, longs},
+                     nslow);
+            r = read_counters(c);
+            if (r) return r;
+            if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
+            if (c.hctr->nlong > 0) {
+                // (keys2, vals2) are free now: the second buffer of each run's merge sort
+                k_resolve_long<<<(unsigned)c.hctr->nlong, kLongThreads, 0, c.stream>>>(
+                    c.keys, c.vals, nr, c.keys2, c.vals2, longs, alpha_geom_tris(c), c.edges, c.opos, nIn, nT, c.ctr,
+                    segs ? segs->seg : nullptr);
+                count_launch();
+                GALPHA_CUDA(cudaGetLastError());
+            }
+        }
     }
     r = exclusive_scan_int(c, nr, c.rank, nIn, &c.ctr->nlist);
     if (r) return r;

@@ -51,21 +51,26 @@ def test_random_alpha(engine, seed):
         assert ok, rep
 
 
-def test_long_key_group(engine):
+@pytest.mark.parametrize("side", [60, 100])
+def test_long_key_group(engine, side):
     """A lattice whose unit edges share one spectrum value, with a few points
     moved by about 1e-12 so that some edge keys agree with it in their top 40
     bits but not below: a group of equal top bits far longer than one thread
     fixes up, out of order, sorted as a sub-array (fewer passes than a full
-    64-bit sort); the spectrum and intervals match the oracle."""
+    64-bit sort).  Moving a vertex along its triangle's circumcircle changes
+    the radius only at second order, so the triangle values form a run of
+    keys within 2 ulp with exact order violations: at side 100 the run has
+    about 19,600 entries and is merge-sorted by one block with the exact
+    comparator.  The spectrum and intervals match the oracle."""
     rng = np.random.default_rng(77)
-    g = np.arange(60) / 128.0
+    g = np.arange(side) / 128.0
     pts = np.stack(np.meshgrid(g, g), -1).reshape(-1, 2).copy()
     moved = rng.choice(len(pts), 60, replace=False)
     pts[moved, 0] += rng.choice([-1.0, 1.0], 60) * rng.uniform(1e-12, 3e-12, 60)
     dt, a = engine.compute_all(G.GPUDTParams(pts, fboSize=1024))
     ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
     assert ok, rep
-    assert 5 < dt.status.sortPasses < 13, dt.status.sortPasses
+    assert dt.status.sortPasses > 5, dt.status.sortPasses  # the top-40 passes plus long-group passes
 
 
 def test_alpha_of_host_mesh_matches_resident(engine):
