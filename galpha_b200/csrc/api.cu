@@ -560,6 +560,7 @@ int galphaSetStream(galphaHandle h, void *stream)
 int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY, double maxX, double maxY,
                     int fboSize, int withAlpha, gpudtStatus *st)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h || n < 0 || !fbo_ok(fboSize)) return GPUDT_ERR_ARG;
     std::lock_guard<std::mutex> lk(h->mu);
     Ctx &c = h->H.c;
@@ -593,6 +594,7 @@ int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, doub
 
 int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *out, gpudtStatus *st)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h) return GPUDT_ERR_ARG;
     int r = check_params(params);
     if (r) return r;
@@ -784,6 +786,7 @@ static int download_alpha(Ctx &c, GAlphaOutput *out)
 
 int galphaComputeResident(galphaHandle h, GAlphaOutput *out)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h || !out) return GPUDT_ERR_ARG;
     std::lock_guard<std::mutex> lk(h->mu);
     Ctx &c = h->H.c;
@@ -814,6 +817,7 @@ struct AosToSoa {
 
 int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *dt, GAlphaOutput *out)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h || !params || !dt || !out || params->nPoints < 0 || dt->nTris < 0) return GPUDT_ERR_ARG;
     if (dt->nTris > 0 && !dt->triangles) return GPUDT_ERR_ARG;
     std::lock_guard<std::mutex> lk(h->mu);
@@ -847,6 +851,7 @@ int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *
 // the handle's stream, so their transfer overlaps the alpha computation.
 int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt, GAlphaOutput *out, gpudtStatus *st)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h || !dt || !out) return GPUDT_ERR_ARG;
     int r = check_params(params);
     if (r) return r;
@@ -920,6 +925,7 @@ int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt,
 int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double *d_xy, const double *bounds,
                    int withAlpha, gpudtStatus *st)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h || nSets <= 0 || !setSizes || !bounds) return GPUDT_ERR_ARG;
     std::lock_guard<std::mutex> lk(h->mu);
     Ctx &c = h->H.c;
@@ -936,6 +942,7 @@ int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double 
 int galphaRunBatchHost(galphaHandle h, int nSets, const int *setSizes, const double *xy, const double *bounds,
                        int withAlpha, gpudtStatus *st)
 {
+    g_err.clear();  // a compute call starts without a stale message
     if (!h || nSets <= 0 || !setSizes || !bounds) return GPUDT_ERR_ARG;
     long long n = 0;
     for (int s = 0; s < nSets; s++) n += setSizes[s] > 0 ? setSizes[s] : 0;
@@ -1137,6 +1144,7 @@ static galpha_ctx *default_handle(int *status)
 
 int gpudtComputeDTEx(const GPUDTPARAMS *pParam, GPUDTOUTPUT *pOutput, gpudtStatus *status)
 {
+    g_err.clear();  // a compute call starts without a stale message
     int r = GPUDT_OK;
     galpha_ctx *h = default_handle(&r);
     if (!h) {

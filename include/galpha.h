@@ -247,7 +247,8 @@ int galphaBatchQuery(galphaHandle h, const double *values, int byQuantile, galph
 int galphaEdgeListNoAlloc(const gpudtTriangle *d_tris, int nTris, int *d_edges, int edgeCapacity,
                           int *d_nEdges, void *stream);
 
-/* Text of the last error on the calling thread. */
+/* Text of the last error on the calling thread (cleared when a compute call
+ * -- RunDevice, Triangulate, Compute*, RunBatch*, gpudtComputeDTEx -- starts). */
 const char *galphaLastError(void);
 
 /* Number of CUDA kernels this library has launched since it was loaded. */
