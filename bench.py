@@ -466,7 +466,8 @@ def main():
     b_alg = 28.0 * T * T + 16.0 * n + 36.0 * nt + 8.0 * n_spec + 24.0 * n_spec + 12.0 * ne + 4.0 * nt + 8.0 * n
     roof = {
         "bound": "hbm",
-        "kernel": "spectrum key sort (k_rs_hist + scan + k_rs_scatter, %d passes of 8-bit digits)" % stats_sort[1],
+        "kernel": "spectrum key sort (k_rs_hist_top once + k_rs_onesweep per pass, %d passes of 8-bit digits, "
+                  "+ group fix-up)" % stats_sort[1],
         "achieved": sort_bytes / (sort_ms / 1e3) / 1e9 if sort_ms > 0 else None, "peak": peak, "unit": "GB/s",
         "frac": (sort_bytes / (sort_ms / 1e3) / 1e9) / peak if sort_ms > 0 else None,
         "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650",
