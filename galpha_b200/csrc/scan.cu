@@ -3,9 +3,11 @@
 // Replaces the reference's recursive Blelloch scan (cudaScanLargeArray.cu:
 // 222-477, prescanArray) and its host-side row prefix sum
 // (cudaReconstruction.cu:470-478).  Each block scans a 4096-element tile held
-// in registers (16 per thread) with warp shuffles; tile sums are scanned
-// recursively; a final pass adds the tile offsets.  Scratch comes from a
-// per-handle buffer, so a scan allocates nothing.
+// in registers (16 per thread) with warp shuffles.  Up to 32736 tiles, one
+// launch scans the whole array (tile offsets by decoupled look-back, int4
+// accesses); above that, tile sums are scanned recursively and a final pass
+// adds the tile offsets.  Scratch comes from a per-handle buffer, so a scan
+// allocates nothing.
 #include "internal.cuh"
 
 namespace galpha {
@@ -139,38 +141,63 @@ __device__ __forceinline__ unsigned long long sc_ld_acquire(const unsigned long 
     return v;
 }
 
+// A tile is kScanSlices slices of 4 * kScanThreads elements; thread t holds
+// elements [4t, 4t + 4) of each slice as one int4, so every load and store
+// of a warp covers 512 contiguous bytes.  The warp sums of all slices, in
+// slice-major order, are the tile's 32 partial sums in element order: one
+// warp scan gives every warp's offset and the tile total.
+constexpr int kScanSlices = kScanItems / 4;
+static_assert(kScanSlices * (kScanThreads / 32) == 32, "one warp scans the partial sums of a tile");
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_1p(const int *__restrict__ in, int *__restrict__ out,
                                                           long long n, unsigned long long *status, int *ticket,
-                                                          int *total, Counters *ct)
+                                                          int *total, Counters *ct, bool vec)
 {
     __shared__ int s_tile;
     __shared__ long long s_excl;
+    __shared__ int s_part[32];
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1);
     __syncthreads();
     const int tile = s_tile;
-    const long long base = (long long)tile * kScanTile + (long long)threadIdx.x * kScanItems;
-    int v[kScanItems];
-    int sum = 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long base = (long long)tile * kScanTile + 4ll * threadIdx.x;
+    int4 a[kScanSlices];
+    int incl[kScanSlices], sum[kScanSlices];
 #pragma unroll
-    for (int k = 0; k < kScanItems; k++) {
-        const long long i = base + k;
-        v[k] = i < n ? in[i] : 0;
-        sum += v[k];
+    for (int k = 0; k < kScanSlices; k++) {
+        const long long i = base + (long long)k * 4 * kScanThreads;
+        if (vec && i + 3 < n) {
+            a[k] = *reinterpret_cast<const int4 *>(in + i);
+        } else {
+            a[k].x = i < n ? in[i] : 0;
+            a[k].y = i + 1 < n ? in[i + 1] : 0;
+            a[k].z = i + 2 < n ? in[i + 2] : 0;
+            a[k].w = i + 3 < n ? in[i + 3] : 0;
+        }
+        sum[k] = a[k].x + a[k].y + a[k].z + a[k].w;
+        incl[k] = warp_incl(sum[k]);
+        if (lane == 31) s_part[k * (kScanThreads / 32) + w] = incl[k];
     }
-    int excl;
-    const int tot = block_scan(sum, excl);
+    __syncthreads();
+    if (w == 0) {
+        const int v = s_part[lane];
+        const int x = warp_incl(v);
+        s_part[lane] = x - v;  // exclusive offset of (slice, warp) in the tile
+        if (lane == 31) s_tile = x;  // the tile total (the ticket is no longer needed)
+    }
+    __syncthreads();
+    const int tot = s_tile;
     if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
         long long acc = 0;
         if (tile > 0) {
             if (lane == 0) sc_st_release(&status[tile], kScAgg | (unsigned long long)(unsigned)tot);
             bool bad = false;
             for (int j = tile - 1;; j -= 32) {
                 const int idx = j - lane;
-                unsigned long long w = kScPre;  // before tile 0: nothing to add
+                unsigned long long wd = kScPre;  // before tile 0: nothing to add
                 if (idx >= 0) {
                     int spins = 0;
-                    while (((w = sc_ld_acquire(&status[idx])) >> 62) == 0) {
+                    while (((wd = sc_ld_acquire(&status[idx])) >> 62) == 0) {
                         if (++spins > kScanSpinLimit) {
                             bad = true;
                             break;
@@ -182,9 +209,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_1p(const int *__restrict_
                     bad = true;
                     break;
                 }
-                const unsigned pre = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+                const unsigned pre = __ballot_sync(0xffffffffu, (wd >> 62) == 2);
                 const int first = pre ? __ffs(pre) - 1 : 31;  // lanes up to the nearest prefix count
-                long long mine = (lane <= first && idx >= 0) ? (long long)(w & kScVal) : 0;
+                long long mine = (lane <= first && idx >= 0) ? (long long)(wd & kScVal) : 0;
                 for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
                 acc += mine;
                 if (pre) break;
@@ -197,13 +224,22 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_1p(const int *__restrict_
         }
     }
     __syncthreads();
-    const int off = (int)s_excl + excl;
-    int e = off;
 #pragma unroll
-    for (int k = 0; k < kScanItems; k++) {
-        const long long i = base + k;
-        if (i < n) out[i] = e;
-        e += v[k];
+    for (int k = 0; k < kScanSlices; k++) {
+        const long long i = base + (long long)k * 4 * kScanThreads;
+        int4 o;
+        o.x = (int)s_excl + s_part[k * (kScanThreads / 32) + w] + incl[k] - sum[k];
+        o.y = o.x + a[k].x;
+        o.z = o.y + a[k].y;
+        o.w = o.z + a[k].z;
+        if (vec && i + 3 < n) {
+            *reinterpret_cast<int4 *>(out + i) = o;
+        } else {
+            if (i < n) out[i] = o.x;
+            if (i + 1 < n) out[i + 1] = o.y;
+            if (i + 2 < n) out[i + 2] = o.z;
+            if (i + 3 < n) out[i + 3] = o.w;
+        }
     }
     if (total && threadIdx.x == 0 && (long long)(tile + 1) * kScanTile >= n) *total = (int)(s_excl + tot);
 }
@@ -221,7 +257,8 @@ int exclusive_scan_int(Ctx &c, const int *in, int *out, int n, int *total_dev)
         unsigned long long *status = reinterpret_cast<unsigned long long *>(c.hist + kScanStatusOff);
         GALPHA_CUDA(cudaMemsetAsync(ticket, 0, sizeof(int), c.stream));
         GALPHA_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (size_t)tiles, c.stream));
-        k_scan_1p<<<(unsigned)tiles, kScanThreads, 0, c.stream>>>(in, out, n, status, ticket, total_dev, c.ctr);
+        const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+        k_scan_1p<<<(unsigned)tiles, kScanThreads, 0, c.stream>>>(in, out, n, status, ticket, total_dev, c.ctr, vec);
         count_launch();
         GALPHA_CUDA(cudaGetLastError());
         return GPUDT_OK;
