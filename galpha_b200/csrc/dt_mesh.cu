@@ -179,10 +179,13 @@ struct MatchLinks {
             tn[t] = make_int4(-1, -1, -1, 0);
             return;
         }
+        // A directed edge held by two triangles shows up as two twins in the
+        // twin's scan (cnt > 1) or, on the hull, in the hull edge count, which
+        // must equal the fake ring's; so a's own list is not scanned.
         int n[3];
         for (int k = 0; k < 3; k++) {
             int a = geti(v, p1(k)), b = geti(v, m1(k));  // edge a -> b, opposite vtx[k]
-            int found = -1, cnt = 0, same = 0;
+            int found = -1, cnt = 0;
             for (int s = start[b], e = start[b + 1]; s < e; s++) {
                 int2 x = inc[s];
                 if (x.y == a) {  // a triangle with b -> a
@@ -190,8 +193,7 @@ struct MatchLinks {
                     cnt++;
                 }
             }
-            for (int s = start[a], e = start[a + 1]; s < e; s++) same += inc[s].y == b;  // a -> b
-            if (cnt > 1 || same != 1) set_err(ct, GPUDT_ERR_TOPOLOGY, 20);
+            if (cnt > 1) set_err(ct, GPUDT_ERR_TOPOLOGY, 20);
             if (found < 0) atomicAdd(&ct->changed, 1);  // hull edge
             n[k] = found;
         }
