@@ -461,7 +461,7 @@ def main():
     row_bytes = 2.0 * T * T + 16.0 * nt
     col_ms = sum(k[1] for k in kernels) / len(kernels)
     stage_mean = [sum(s[i] for s in stages) / len(stages) for i in range(12)]
-    # whole-pipeline algorithmic byte model (SURVEY-style compulsory traffic)
+    # whole-pipeline algorithmic byte model (compulsory traffic of every stage)
     n_spec = ns
     b_alg = 28.0 * T * T + 16.0 * n + 36.0 * nt + 8.0 * n_spec + 24.0 * n_spec + 12.0 * ne + 4.0 * nt + 8.0 * n
     roof = {

@@ -691,7 +691,8 @@ int stage_shift(Ctx &c)
         launch_n(c, ShiftCommit{cand, c.pos, c.opos, c.vstate, c.vround}, c.V);
     }
     // vertices fixed from the start (fake ring) and the optimistic set count
-    // as decided in round 1; the rest go through priority rounds
+    // as decided in the first shifting round (id 1); the rest go through
+    // priority rounds
     for (int round = 2;; round++) {
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int) + 0, c.stream));
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));

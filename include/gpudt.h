@@ -23,8 +23,8 @@
  *     (t << 2) | j is the neighbour across the edge opposite vtx[i], -1 on the hull;
  *   - exact duplicates are dropped (the lowest input index survives);
  *   - nConstraints must be 0 (constrained edges are outside this engine).
- * Differences (documented in DESIGN.md): errors are returned, not exit(-1);
- * tmp[3] is zero-filled instead of internal chain garbage.
+ * Differences from the reference: errors are returned, not exit(-1); tmp[3]
+ * is zero-filled instead of internal chain garbage.
  */
 #ifndef GALPHA_GPUDT_H
 #define GALPHA_GPUDT_H
