@@ -432,9 +432,11 @@ def main():
     value = world * n / (max_ms / 1e3) / 1e6
 
     # rooflines.  The sort of the spectrum keys is the largest HBM-bound kernel
-    # of the step (k_rs_hist + k_rs_scatter, ~11 % of device time; the larger
-    # FlipCheck share is gather/latency-bound in-circle work): algorithmic
-    # bytes = passes x keys x (8 B key + 4 B value, read and written once).
+    # of the step (the FlipCheck share is gather/latency-bound in-circle work).
+    # Algorithmic bytes follow the fixed byte model: the sort is charged ONE
+    # read and one write of every (8 B key + 4 B value) pair, however many
+    # radix passes the implementation makes; the DRAM traffic of all passes is
+    # reported beside it as `traffic`.
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -444,7 +446,7 @@ def main():
     peak = peaks.get("hbm_gbs", 6650.0)
     T = fbo
     sort_ms = sum(k[3] for k in kernels) / len(kernels)
-    sort_bytes = 24.0 * stats_sort[0] * stats_sort[1]
+    sort_bytes = 24.0 * stats_sort[0]
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "spectrum_sort_traffic.txt")
     if os.path.exists(tfile):
@@ -476,8 +478,12 @@ def main():
                     "achieved": row_bytes / (row_ms / 1e3) / 1e9 if row_ms > 0 else None,
                     "frac": (row_bytes / (row_ms / 1e3) / 1e9) / peak if row_ms > 0 else None,
                     "algorithmic_bytes_per_launch": row_bytes, "launch_ms": row_ms}],
+        # the whole-path figure the 60 % target is stated on: compulsory bytes
+        # of the step (28 T^2 + 16 N + 36 nTris + 32 nSpec + 12 nEdges + 4 nTris
+        # + 8 N) over the measured step time
         "pipeline": {"algorithmic_bytes": b_alg, "achieved_gbs": b_alg / (max_ms / 1e3) / 1e9,
-                     "frac": b_alg / (max_ms / 1e3) / 1e9 / peak},
+                     "frac": b_alg / (max_ms / 1e3) / 1e9 / peak, "target_frac": 0.60,
+                     "ideal_ms": b_alg / (peak * 1e9) * 1e3},
     }
 
     # end to end through the host API

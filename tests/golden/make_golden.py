@@ -22,7 +22,9 @@ from oracle import oracle as O  # noqa: E402
 from galpha_b200 import datasets as D  # noqa: E402
 from galpha_b200.api import read_points_file  # noqa: E402
 
-REF_INPUT = "/root/reference/input"
+# the reference tree (read only for its input/ fixtures); GALPHA_REF_TREE overrides
+REF_TREE = os.environ.get("GALPHA_REF_TREE", "/root/reference")
+REF_INPUT = os.path.join(REF_TREE, "input")
 NAMES = ["bird", "alpha", "1000_1", "10000_1"]
 
 
