@@ -6,6 +6,7 @@ engine is libgalpha.so (CUDA, sm_100a, C ABI in include/gpudt.h and
 include/galpha.h); this package is its Python host mirror.
 """
 from .api import (  # noqa: F401
+    ALPHA_DTYPE,
     AlphaShapes2D,
     DTOutput,
     Engine,

@@ -644,6 +644,9 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     int r;
     const int nT = c.nT_out;
     int *cnt = c.aux, *e_off = c.e_off;
+    // an alpha call on a resident mesh starts without the error of an earlier
+    // failed alpha call (err and errinfo are adjacent words)
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->err, 0, 2 * sizeof(int), c.stream));
     launch_n(c, EdgeCount{c.cv, c.cn, cnt}, nT);
     r = exclusive_scan_int(c, cnt, e_off, nT, &c.ctr->nlist);
     if (r) return r;

@@ -557,6 +557,20 @@ int galphaSetStream(galphaHandle h, void *stream)
     return GPUDT_OK;
 }
 
+int galphaSetLimits(galphaHandle h, int maxRounds, int spinLimit, int holdFirstTile)
+{
+    if (!h) {
+        noalloc_set_limits(spinLimit, holdFirstTile);
+        return GPUDT_OK;
+    }
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    c.max_rounds = maxRounds > 0 ? maxRounds : kMaxRounds;
+    c.spin_limit = spinLimit > 0 ? spinLimit : kSpinLimit;
+    c.hold_first = holdFirstTile > 0 ? 1 : 0;
+    return GPUDT_OK;
+}
+
 int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY, double maxX, double maxY,
                     int fboSize, int withAlpha, gpudtStatus *st)
 {

@@ -525,7 +525,7 @@ int voronoi_global(Ctx &c, int cells, const int *cellmap)
         if (r) return r;
         from = to;
         to = c.hctr->nlist;
-        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (++guard > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     total = to;
     // recolour
@@ -537,7 +537,7 @@ int voronoi_global(Ctx &c, int cells, const int *cellmap)
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->changed == 0) break;
-        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (++guard > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     return GPUDT_OK;
 }

@@ -668,7 +668,8 @@ int stage_shift(Ctx &c)
         launch_n(c, ShiftCandidates{c.vstate, cand}, c.V);
         GALPHA_CUDA(cudaMemsetAsync(drop, 0, sizeof(int) * (size_t)c.V, c.stream));
         int nprev = 0;
-        for (int it = 0; it < kMaxRounds; it++) {
+        bool settled = false;
+        for (int it = 0; it < c.max_rounds; it++) {
             int *cur = lists[it & 1], *prev = lists[(it + 1) & 1];
             GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
             if (it == 0)
@@ -682,12 +683,16 @@ int stage_shift(Ctx &c)
             if (c.hctr->err) return c.hctr->err;
             shiftRounds++;
             const int nd = c.hctr->nlist2;
-            if (nd == 0) break;
+            if (nd == 0) {
+                settled = true;
+                break;
+            }
             if ((long long)ndropped + nd > c.N) return GPUDT_ERR_TOPOLOGY;
             launch_n(c, ShiftDropList{cur, cand, drop, dropped + ndropped}, nd);
             ndropped += nd;
             nprev = nd;
         }
+        if (!settled) return GPUDT_ERR_NOCONVERGE;
         launch_n(c, ShiftCommit{cand, c.pos, c.opos, c.vstate, c.vround}, c.V);
     }
     // vertices fixed from the start (fake ring) and the optimistic set count
@@ -705,7 +710,7 @@ int stage_shift(Ctx &c)
         shiftRounds++;
         badCount += c.hctr->changed;
         if (c.hctr->nlist == 0) break;
-        if (shiftRounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (shiftRounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     c.st.shiftRounds = shiftRounds;
     c.st.nBadShift = badCount;
@@ -729,7 +734,7 @@ int stage_shift(Ctx &c)
         r = run_relink(c, round, c.hctr->nrec);
         if (r) return r;
         badCount -= nsel;
-        if (++guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (++guard > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     return GPUDT_OK;
 }
@@ -1040,7 +1045,7 @@ int stage_missing(Ctx &c)
         int done = c.hctr->changed;
         remaining -= done;
         rounds++;
-        if (done == 0 || rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (done == 0 || rounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     // count drops
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
@@ -1677,7 +1682,7 @@ int stage_boundary(Ctx &c)
     // first pass: the four ring classes in turn (independent by construction);
     // then rounds of priority-minimal fakes among all that remain
     for (int pass = 0; removed < c.F; pass++) {
-        if (pass > kMaxRounds / 4) return GPUDT_ERR_NOCONVERGE;
+        if (pass > c.max_rounds / 4) return GPUDT_ERR_NOCONVERGE;
         // pass 0: three ring classes one fake at a time, then the last class
         // (a chain by then) as runs, one separator level after another; later
         // passes: priority rounds among the fakes left
@@ -1729,7 +1734,7 @@ int stage_boundary(Ctx &c)
     int *lin = c.list, *lout = c.list2;
     int4 *prop = c.fwd;
     for (int guard = 0; n > 0; guard++) {
-        if (guard > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (guard > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
         int round = next_round(c);
         GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
         launch_n(c, ConvexPropose{c.tv, c.tn, c.pos, c.vtri, lin, nullptr, c.vote, prop, c.ctr}, n);
@@ -2011,7 +2016,7 @@ int stage_flip(Ctx &c)
                 FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nullptr, nullptr, prop, target, cands,
                           c.rec, 0, c.ctr, c.eflag, false},
                 Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, 0, c.ctr}, FlipReset{c.vote, target, cands},
-                lists[0], lists[1], p, round0, kMaxRounds + 1 - rounds, kTailLeave);
+                lists[0], lists[1], p, round0, c.max_rounds + 1 - rounds, kTailLeave);
             count_launch();
             GALPHA_CUDA(cudaGetLastError());
             r = read_counters(c);
@@ -2022,7 +2027,7 @@ int stage_flip(Ctx &c)
             rounds += k;
             known = c.hctr->act[rounds & 1];
             if (known == 0) break;
-            if (rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+            if (rounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
             if (known <= kTailLeave) return set_last_error("flip: in-block rounds stopped early"), GPUDT_ERR_TOPOLOGY;
         }
         for (int k = 0; k < kFlipSync; k++) {
@@ -2050,7 +2055,7 @@ int stage_flip(Ctx &c)
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
         known = c.hctr->act[rounds & 1];
-        if (rounds > kMaxRounds) return GPUDT_ERR_NOCONVERGE;
+        if (rounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     c.st.nFlips = c.hctr->flips_total + c.hctr->nflips;
     c.st.flipRounds = rounds;

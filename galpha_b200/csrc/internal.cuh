@@ -22,7 +22,8 @@ namespace galpha {
 constexpr int kFakeSpacing = 32;                 // fake ring site every <= 32 pixels
 constexpr int kMargin = kFakeSpacing / 2 + 1;    // real sites stay >= 17 pixels from the border
 constexpr int kMaxFan = 64;                      // star holes / fans handled per thread
-constexpr int kMaxRounds = 100000;               // cap of every iterative stage
+constexpr int kMaxRounds = 100000;               // cap of every iterative stage (default)
+constexpr int kSpinLimit = 1 << 22;              // bound of every look-back wait (default)
 
 // vertex states
 enum : int8_t {
@@ -175,6 +176,14 @@ struct Ctx {
     int sort_passes = 0;  // radix passes of the last radix_sort call
     bool fused_done = false;  // triangles came from the fused colour + dual kernel
     int round_counter = 1;    // ids of operation rounds (per handle: stamps live in its arena)
+
+    // failure-detection limits (galphaSetLimits): the round cap of every
+    // iterative stage, the spin bound of the single-pass look-back waits, and
+    // a test switch under which tile 0 of each look-back kernel withholds its
+    // status so that the next tile's bounded wait runs out
+    int max_rounds = kMaxRounds;
+    int spin_limit = kSpinLimit;
+    int hold_first = 0;
 };
 
 // ------------------------------------------------------------- error helpers
@@ -198,6 +207,9 @@ int read_small(Ctx &c, void *host_dst, const void *dev_src, size_t bytes);
 // Records the failing stage and the device-side detail code (galphaLastError).
 int stage_fail(Ctx &c, int r, const char *stage);
 constexpr size_t kMailBytes = 65536;
+
+// Limits of galphaEdgeListNoAlloc (noalloc.cu), set by galphaSetLimits(NULL, ...).
+void noalloc_set_limits(int spin_limit, int hold_first);
 
 // Kernel launches issued by this library (all handles, all threads).
 extern unsigned long long g_launches;

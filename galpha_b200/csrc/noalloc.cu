@@ -9,7 +9,7 @@
 // triangles own, finds the tile's global offset by a single-pass decoupled
 // look-back over the per-tile descriptors of earlier tiles, and writes the
 // (tIndex, vOpp) pairs.  The descriptors, the ticket and a done counter live in
-// one file-scope device array (g_el_scratch, 256 KB), so a call allocates
+// one file-scope device array (g_el_scratch, 512 KB), so a call allocates
 // nothing: not device memory, not pinned host memory, not events.
 //
 // Shared-state rules:
@@ -17,8 +17,9 @@
 //    be ordered (same stream, or synchronised): two calls in flight at once
 //    race on the ticket and descriptors and give wrong results;
 //  * the ticket, the done counter, the error word and every descriptor must
-//    be zero when a call starts; the first call on a device zeroes the array
-//    (stream-ordered on the caller's stream) and the last block of every call
+//    be zero when a call starts; the first call on a device (and the first
+//    after a cudaDeviceReset, which reloads the module) zeroes the array,
+//    stream-ordered on the caller's stream, and the last block of every call
 //    zeroes what the call used before it exits.
 #include <cstdint>
 #include <cstdio>
@@ -29,17 +30,17 @@ namespace galpha {
 namespace {
 
 constexpr int kElThreads = 256;
-constexpr int kElItems = 8;
-constexpr int kElTile = kElThreads * kElItems;  // 2048 triangles per tile
-constexpr int kElMaxTiles = 32768;
+constexpr int kElItems = 4;
+constexpr int kElTile = kElThreads * kElItems;  // 1024 triangles per tile
+constexpr int kElMaxTiles = 65536;
 constexpr long long kElMaxTris = (long long)kElTile * kElMaxTiles;  // 67,108,864
 constexpr int kElHeader = 32;  // [0] ticket, [1] blocks done, [2] error word
-constexpr int kElSpinLimit = 1 << 22;
 constexpr unsigned long long kStAgg = 1ull << 62;   // descriptor holds the tile's own count
 constexpr unsigned long long kStPre = 2ull << 62;   // descriptor holds the inclusive prefix
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
 constexpr int kMaxDevices = 64;
 
+// 512 KB: the header words and one descriptor per tile
 static __device__ __align__(256) unsigned long long g_el_scratch[kElHeader + kElMaxTiles];
 
 __device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v)
@@ -54,24 +55,31 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
     return v;
 }
 
-// An edge (vtx[i+1], vtx[i+2]) of triangle t belongs to t when its first
-// vertex has the smaller index or it lies on the hull (kernel.cu's
+// Owned edges of one triangle record staged in shared memory (9 ints: tri[3],
+// vtx[3], tmp[3]): edge i = (vtx[i+1], vtx[i+2]) belongs to the triangle when
+// its first vertex has the smaller index or it lies on the hull (kernel.cu's
 // computeTriEdgeCount rule, the same test as EdgeCount in alpha.cu).
-__device__ __forceinline__ int owned_mask(const gpudtTriangle &g)
+__device__ __forceinline__ int owned_mask(const int *r)
 {
     int m = 0;
     for (int i = 0; i < 3; i++) {
-        int a = g.vtx[p1(i)], b = g.vtx[m1(i)];
-        if (a < b || g.tri[i] == -1) m |= 1 << i;
+        int a = r[3 + p1(i)], b = r[3 + m1(i)];
+        if (a < b || r[i] == -1) m |= 1 << i;
     }
     return m;
 }
 
-__global__ void __launch_bounds__(kElThreads) k_edge_list(const gpudtTriangle *__restrict__ tris, int nTris,
+// spin_limit bounds every look-back wait; hold_first (a failure-detection
+// test switch, 0 in normal use) makes tile 0 withhold its descriptor so that
+// tile 1's wait runs out and the call reports GPUDT_ERR_NOCONVERGE.
+__global__ void __launch_bounds__(kElThreads) k_edge_list(const int *__restrict__ tris, int nTris,
                                                           int2 *__restrict__ edges, int cap,
                                                           int *__restrict__ nEdges,
-                                                          unsigned long long *__restrict__ scratch)
+                                                          unsigned long long *__restrict__ scratch,
+                                                          int spin_limit, int hold_first)
 {
+    __shared__ int s_rec[kElTile * 9];  // the tile's triangle records, 36 KB
+    __shared__ unsigned char s_mask[kElTile];
     __shared__ int s_tile, s_last;
     __shared__ int s_warp[kElThreads / 32];
     __shared__ unsigned long long s_excl;
@@ -83,19 +91,27 @@ __global__ void __launch_bounds__(kElThreads) k_edge_list(const gpudtTriangle *_
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(&hdr[0], 1ull);
     __syncthreads();
     const int tile = s_tile;
+    const long long tbase = (long long)tile * kElTile;
+    const int ntile = (int)min((long long)kElTile, (long long)nTris - tbase);
 
-    // owned edges of this thread's kElItems consecutive triangles
-    const long long t0 = (long long)tile * kElTile + (long long)threadIdx.x * kElItems;
+    // stage the records with consecutive 4-byte loads (a warp reads 128
+    // contiguous bytes), then find each triangle's owned edges from shared
+    // memory (stride 9 words between threads: no bank conflicts)
+    const int *src = tris + tbase * 9;
+    for (int j = threadIdx.x; j < ntile * 9; j += kElThreads) s_rec[j] = src[j];
+    __syncthreads();
+    for (int t = threadIdx.x; t < kElTile; t += kElThreads)
+        s_mask[t] = t < ntile ? (unsigned char)owned_mask(s_rec + 9 * t) : 0;
+    __syncthreads();
+
+    // this thread's kElItems consecutive triangles
     unsigned masks = 0;  // 3 bits per item
     int cnt = 0;
 #pragma unroll
     for (int k = 0; k < kElItems; k++) {
-        long long t = t0 + k;
-        if (t < nTris) {
-            int m = owned_mask(tris[t]);
-            masks |= (unsigned)m << (3 * k);
-            cnt += __popc(m);
-        }
+        int m = s_mask[threadIdx.x * kElItems + k];
+        masks |= (unsigned)m << (3 * k);
+        cnt += __popc(m);
     }
     // block-wide exclusive scan of the counts
     int incl = cnt;
@@ -117,7 +133,7 @@ __global__ void __launch_bounds__(kElThreads) k_edge_list(const gpudtTriangle *_
     if (threadIdx.x == 0) {
         unsigned long long excl = 0;
         if (tile == 0) {
-            st_release(&desc[0], kStPre | (unsigned long long)agg);
+            if (!hold_first) st_release(&desc[0], kStPre | (unsigned long long)agg);
         } else {
             st_release(&desc[tile], kStAgg | (unsigned long long)agg);
             bool bad = false;
@@ -127,7 +143,7 @@ __global__ void __launch_bounds__(kElThreads) k_edge_list(const gpudtTriangle *_
                 // tile j took its ticket before this one, so its block is running
                 // and publishes; the bound only guards against a broken invariant
                 while (((d = ld_acquire(&desc[j])) >> 62) == 0) {
-                    if (++spins > kElSpinLimit) {
+                    if (++spins > spin_limit) {
                         bad = true;
                         break;
                     }
@@ -147,7 +163,7 @@ __global__ void __launch_bounds__(kElThreads) k_edge_list(const gpudtTriangle *_
     long long e = (long long)s_excl + texcl;
 #pragma unroll
     for (int k = 0; k < kElItems; k++) {
-        long long t = t0 + k;
+        long long t = tbase + threadIdx.x * kElItems + k;
         if (t >= nTris) break;
         for (int i = 0; i < 3; i++) {
             if ((masks >> (3 * k + i)) & 1u) {
@@ -175,10 +191,15 @@ __global__ void __launch_bounds__(kElThreads) k_edge_list(const gpudtTriangle *_
 }
 
 std::mutex g_el_mu;
-unsigned long long *g_el_ptr[kMaxDevices];
+unsigned long long *g_el_ptr[kMaxDevices];  // the address the array was last zeroed at
+int g_el_spin_limit = kSpinLimit;
+int g_el_hold_first = 0;
 
-// Once per device, with that device current: the address of the array, and a
-// zero fill ordered on the caller's stream.
+// The array's device address, looked up on every call with the caller's
+// device current (a cudaDeviceReset reloads the module, so an address kept
+// from before would be stale), and a zero fill ordered on the caller's stream
+// whenever the address is new: the first call on a device, the first after a
+// reset.
 int el_scratch(cudaStream_t stream, unsigned long long **out)
 {
     int dev = -1;
@@ -188,20 +209,30 @@ int el_scratch(cudaStream_t stream, unsigned long long **out)
         set_last_error("galphaEdgeListNoAlloc: device index out of range");
         return GPUDT_ERR_NODEVICE;
     }
+    unsigned long long *p = nullptr;
+    e = cudaGetSymbolAddress((void **)&p, g_el_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "galphaEdgeListNoAlloc: cudaGetSymbolAddress"), GPUDT_ERR_CUDA;
     std::lock_guard<std::mutex> lk(g_el_mu);
-    if (!g_el_ptr[dev]) {
-        unsigned long long *p = nullptr;
-        e = cudaGetSymbolAddress((void **)&p, g_el_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "galphaEdgeListNoAlloc: cudaGetSymbolAddress"), GPUDT_ERR_CUDA;
+    if (g_el_ptr[dev] != p) {
         e = cudaMemsetAsync(p, 0, sizeof(g_el_scratch), stream);
         if (e != cudaSuccess) return cuda_fail(e, "galphaEdgeListNoAlloc: zeroing scratch"), GPUDT_ERR_CUDA;
         g_el_ptr[dev] = p;
     }
-    *out = g_el_ptr[dev];
+    *out = p;
     return GPUDT_OK;
 }
 
 }  // namespace
+
+// Failure-detection limits of galphaEdgeListNoAlloc (galphaSetLimits with a
+// NULL handle); values <= 0 restore the defaults.
+void noalloc_set_limits(int spin_limit, int hold_first)
+{
+    std::lock_guard<std::mutex> lk(g_el_mu);
+    g_el_spin_limit = spin_limit > 0 ? spin_limit : kSpinLimit;
+    g_el_hold_first = hold_first > 0 ? 1 : 0;
+}
+
 }  // namespace galpha
 
 using namespace galpha;
@@ -235,7 +266,14 @@ extern "C" int galphaEdgeListNoAlloc(const gpudtTriangle *d_tris, int nTris, int
         return GPUDT_OK;
     }
     int ntiles = (int)(((long long)nTris + kElTile - 1) / kElTile);
-    k_edge_list<<<ntiles, kElThreads, 0, stream>>>(d_tris, nTris, (int2 *)d_edges, edgeCapacity, d_nEdges, scratch);
+    int spin_limit, hold_first;
+    {
+        std::lock_guard<std::mutex> lk(g_el_mu);
+        spin_limit = g_el_spin_limit;
+        hold_first = g_el_hold_first;
+    }
+    k_edge_list<<<ntiles, kElThreads, 0, stream>>>((const int *)d_tris, nTris, (int2 *)d_edges, edgeCapacity,
+                                                   d_nEdges, scratch, spin_limit, hold_first);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "galphaEdgeListNoAlloc: launch"), GPUDT_ERR_CUDA;

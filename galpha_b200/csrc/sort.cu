@@ -403,7 +403,6 @@ constexpr int kOsTicketOff = kOsPasses * 256;  // after the digit counts [kOsPas
 constexpr int kOsHeadInts = 2048;              // then the status words (256 per tile)
 constexpr unsigned long long kOsAgg = 1ull << 62, kOsInc = 2ull << 62;
 constexpr unsigned long long kOsPassMask = ((1ull << 30) - 1) << 32;
-constexpr int kOsSpinLimit = 1 << 22;
 constexpr int kOsWindow = 8;  // earlier tiles read at once by the look-back
 
 // A status word carries its own payload (nothing else is read after it), so
@@ -469,7 +468,8 @@ __global__ void __launch_bounds__(kRsThreads, 5) k_rs_onesweep(const unsigned lo
                                                             int *__restrict__ vout, int n, int shift,
                                                             const int *__restrict__ dcount,
                                                             unsigned long long *status, int *ticket,
-                                                            unsigned long long pass_tag, Counters *ct)
+                                                            unsigned long long pass_tag, Counters *ct,
+                                                            int spin_limit, int hold_first)
 {
     typedef unsigned long long K;
     extern __shared__ __align__(16) unsigned char rs_smem[];
@@ -520,7 +520,9 @@ __global__ void __launch_bounds__(kRsThreads, 5) k_rs_onesweep(const unsigned lo
     }
     S.lstart[d] = tot;
     unsigned long long *mine = status + (long long)tile * 256 + d;
-    os_st(mine, (tile == 0 ? kOsInc : kOsAgg) | pass_tag | (unsigned)tot);
+    // (hold_first: a failure-detection test switch under which tile 0 withholds
+    // its counts, so that tile 1's bounded wait runs out; 0 in normal use)
+    if (tile != 0 || !hold_first) os_st(mine, (tile == 0 ? kOsInc : kOsAgg) | pass_tag | (unsigned)tot);
     __syncthreads();
     if (w == 0) {  // tile-local digit starts
         int carry = 0;
@@ -576,12 +578,12 @@ __global__ void __launch_bounds__(kRsThreads, 5) k_rs_onesweep(const unsigned lo
                 if (!done && !bad) {
                     unsigned long long x = v[k];
                     int spins = 0;
-                    while (((x >> 62) == 0 || (x & kOsPassMask) != pass_tag) && spins <= kOsSpinLimit) {
+                    while (((x >> 62) == 0 || (x & kOsPassMask) != pass_tag) && spins <= spin_limit) {
                         spins++;
                         __nanosleep(32);
                         x = os_ld(status + (j - k) * 256 + d);
                     }
-                    if (spins > kOsSpinLimit) {
+                    if (spins > spin_limit) {
                         bad = true;
                     } else {
                         acc += (unsigned)x;
@@ -651,7 +653,8 @@ static int onesweep_top40(Ctx &c, unsigned long long *keys, int *vals, unsigned 
         c.sort_passes++;
         k_rs_onesweep<<<(unsigned)tiles, kRsThreads, smem, c.stream>>>(ki, vi, ko, vo, n, kLowBits + 8 * p,
                                                                       ghist + 256 * p, status, tickets + p,
-                                                                      (unsigned long long)(p + 1) << 32, c.ctr);
+                                                                      (unsigned long long)(p + 1) << 32, c.ctr,
+                                                                      c.spin_limit, c.hold_first);
         count_launch();
         GALPHA_CUDA(cudaGetLastError());
         std::swap(ki, ko);

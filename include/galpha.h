@@ -238,14 +238,32 @@ int galphaBatchQuery(galphaHandle h, const double *values, int byQuantile, galph
  *      *d_nEdges = the number of edges (may exceed edgeCapacity), or a
  *      negative GPUDT_ERR_* code written by the kernel.
  * Limit: nTris <= 67,108,864; larger meshes are rejected with GPUDT_ERR_ARG
- * (the kernel's scratch is a fixed 256 KB device array inside the library).
+ * (the kernel's scratch is a fixed 512 KB device array inside the library,
+ * held by every device that loads it until the process exits).
  * Every call on a device shares that array: calls on one device must be
  * ordered (one stream, or synchronised); two calls in flight at once race.
- * The first call on each device looks up and zeroes the array on `stream`.
+ * The first call on each device (and the first after a cudaDeviceReset)
+ * zeroes the array on `stream`; make that call before any stream capture.
  * No counterpart in the reference: there the edge list is built inside
  * Alpha_Shapes_2D (Alpha_Shapes_2D.cu:170-199) in thrust-allocated memory. */
 int galphaEdgeListNoAlloc(const gpudtTriangle *d_tris, int nTris, int *d_edges, int edgeCapacity,
                           int *d_nEdges, void *stream);
+
+/* Failure-detection limits, for tests of the error paths.  On a handle:
+ * maxRounds caps every iterative stage (shifting, insertion, fake removal,
+ * flipping, island recolouring; default 100,000), after which the call
+ * returns GPUDT_ERR_NOCONVERGE; spinLimit bounds each wait of the spectrum
+ * sort's single-pass look-back (default 2^22 polls), after which the call
+ * returns GPUDT_ERR_NOCONVERGE with detail 98; holdFirstTile != 0 makes the
+ * first tile of that look-back withhold its counts, so that the next tile's
+ * wait runs out.  With h == NULL, spinLimit and holdFirstTile apply in the
+ * same way to galphaEdgeListNoAlloc (process-wide; its *d_nEdges then reads
+ * GPUDT_ERR_NOCONVERGE).  Values <= 0 restore the defaults.  Every wait stays
+ * bounded, a failed call leaves the handle usable, and the next call with
+ * the defaults restored computes the full result.
+ * No counterpart in the reference, whose stages loop until done and whose
+ * CUDA failures exit the process (common.h:55-93). */
+int galphaSetLimits(galphaHandle h, int maxRounds, int spinLimit, int holdFirstTile);
 
 /* Text of the last error on the calling thread (cleared when a compute call
  * -- RunDevice, Triangulate, Compute*, RunBatch*, gpudtComputeDTEx -- starts). */

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import galpha_b200 as G
+from alphacheck import compare_alpha
 from galpha_b200 import datasets as D
 from dtcheck import canon_set, compare_dt
 from oracle import oracle as O
@@ -187,6 +188,12 @@ def test_c3_degenerate_properties(engine):
     ro = a["tri_list"]["ro_rank"]
     assert ro.min() >= 1 and ro.max() < len(s)
     assert a["edge_list"]["ro_rank"].max() < len(s)
+    # the full alpha result against the CPU oracle on the same triangles
+    # (about 100 s on one core): ranks and intervals identical, values within
+    # 4 ulp of the exactly rounded FP64 value
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, 4)
+    assert ok, rep
+    print("c3 alpha vs oracle: %r" % rep)
 
 
 def test_voronoi_paths(engine):

@@ -72,7 +72,7 @@ def results(engine, tmp_path_factory):
     ours, feed = {}, {}
     for name, pts, fbo in _cases():
         tris, a, ml, sp = _ours(engine, pts, fbo)
-        ours[name] = (pts, a, ml, sp)
+        ours[name] = (pts, a, ml, sp, tris)
         feed["pts_" + name] = np.ascontiguousarray(pts, np.float64)
         feed["tris_" + name] = np.ascontiguousarray(tris).view(np.int32).reshape(-1, 9)
     np.savez(d / "in.npz", **feed)
@@ -93,7 +93,7 @@ def ulp_gap(a, b):
 
 
 def compare(ours, ref):
-    _, a, ml, sp = ours
+    _, a, ml, sp, _ = ours
     rep = {}
     assert len(a["spectrum"]) == len(ref["spectrum"]), (len(a["spectrum"]), len(ref["spectrum"]))
     np.testing.assert_array_equal(a["tri_list"]["ro_rank"], ref["tri_list"])
@@ -117,8 +117,23 @@ def compare(ours, ref):
     return rep
 
 
+def formula_gap(ours, ref, tris):
+    """The reference's stored values against the oracle's restatement of the
+    reference's FP64 formulas (oracle spectrum_ref) for the same ranks: the
+    two differ only where the device code contracts to FMA or where an
+    exactly tied rank keeps a different member's formula value."""
+    from oracle import oracle as O
+
+    pts = ours[0]
+    t = np.ascontiguousarray(tris).view(np.int32).reshape(-1, 9)
+    o = O.alpha(pts, t[:, 3:6], t[:, 0:3])
+    g = ulp_gap(o["spectrum_ref"][1:], ref["spectrum"][1:])
+    return {"formula_max_ulp": int(g.max()) if len(g) else 0, "formula_equal": float((g == 0).mean()) if len(g) else 1.0}
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_alpha_matches_reference_engine(results, name):
     ours, ref = results
     rep = compare(ours[name], ref[name])
+    rep.update(formula_gap(ours[name], ref[name], ours[name][4]))
     print("reference alpha engine vs galpha, %s: %s" % (name, json.dumps(rep)))

@@ -1,7 +1,8 @@
 """galphaEdgeListNoAlloc: the allocation-free edge numbering, called through
 the C ABI on device buffers and checked against the edge list that the
 handle entry points (galphaTriangulate + galphaComputeResident) return for
-the same mesh.  Integer output, so the tolerance is zero.
+the same mesh, which the CPU oracle's edge numbering pins in turn.  Integer
+output, so the tolerance is zero.
 
 Two meshes, three calls in a row (A, A, B): the second call shows that the
 kernel leaves its shared scratch zeroed, the third that a different tile
@@ -14,6 +15,7 @@ import pytest
 
 import galpha_b200 as G
 from galpha_b200 import datasets as D
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -34,6 +36,9 @@ def _mesh(engine, n, seed, fbo):
     dt = engine.triangulate(G.GPUDTParams(pts, fboSize=fbo))
     al = engine.alpha_resident()
     want = np.stack([al["edge_list"]["tIndex"], al["edge_list"]["vOpp"]], axis=1).astype(np.int32)
+    # the CPU oracle numbers the same triangle array's edges identically
+    ref = O.alpha(pts, dt.vtx, dt.tri)["edge"]
+    np.testing.assert_array_equal(want, ref[:, 5:7].astype(np.int32))
     return dt.triangles.copy(), want
 
 
@@ -77,6 +82,51 @@ def test_edge_list_no_alloc_capacity_and_limits(engine):
     assert rc == -1  # GPUDT_ERR_ARG
     assert b"scratch limit" in L.galphaLastError()
     # the call after a rejected one still works
+    n, got = _no_alloc(L, torch, tris, len(want))
+    assert n == len(want)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_edge_list_no_alloc_allocates_nothing(engine):
+    """Free device memory is the same before and after calls (all buffers
+    made beforehand, the first call's set-up done)."""
+    import torch
+
+    L = _lib()
+    tris, want = _mesh(engine, 50000, 14, 1024)
+    d_tris = torch.from_numpy(tris.view(np.int32).reshape(-1).copy()).cuda()
+    d_edges = torch.empty((len(want), 2), dtype=torch.int32, device="cuda")
+    d_n = torch.empty((1,), dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    args = (d_tris.data_ptr(), len(tris), d_edges.data_ptr(), len(want), d_n.data_ptr(), s)
+    assert L.galphaEdgeListNoAlloc(*args) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert L.galphaEdgeListNoAlloc(*args) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert int(d_n.item()) == len(want)
+    np.testing.assert_array_equal(d_edges.cpu().numpy(), want)
+
+
+def test_edge_list_no_alloc_bounded_wait_reports_error(engine):
+    """Failure detection without a GPU fault: with the first tile made to
+    withhold its count (galphaSetLimits, NULL handle) the next tile's bounded
+    wait runs out, the call reports GPUDT_ERR_NOCONVERGE in *d_nEdges and
+    clears the shared scratch, and the next call with the defaults restored
+    is exact."""
+    import torch
+
+    L = _lib()
+    L.galphaSetLimits.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    tris, want = _mesh(engine, 20000, 15, 1024)
+    try:
+        assert L.galphaSetLimits(None, 0, 2000, 1) == 0
+        n, _ = _no_alloc(L, torch, tris, len(want))
+        assert n == -5  # GPUDT_ERR_NOCONVERGE
+    finally:
+        assert L.galphaSetLimits(None, 0, 0, 0) == 0
     n, got = _no_alloc(L, torch, tris, len(want))
     assert n == len(want)
     np.testing.assert_array_equal(got, want)
