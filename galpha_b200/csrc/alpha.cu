@@ -21,6 +21,7 @@
 //   (kernel.cu:427-624)                             vertex min/max by atomics over edges
 #include <cstdio>
 #include <algorithm>
+#include <vector>
 #include "internal.cuh"
 #include "exact.cuh"
 
@@ -321,10 +322,10 @@ struct ExactAdjacent {
 // Rare path: a run with an order violation is re-sorted with the exact
 // comparator and its rank-start flags recomputed: one thread per run of at
 // most kThreadRun entries (insertion sort), one block per longer run
-// (k_resolve_long: merge sort).  Runs longer than kMaxSlowRun are refused
-// (GPUDT_ERR_EXACT).
+// (k_resolve_long: merge sort), and a run longer than Ctx::block_run by many
+// blocks, one launch per merge level (k_merge_level; a lattice of
+// non-dyadic spacing gives runs of millions of near-equal radii).
 constexpr int kThreadRun = 512;
-constexpr int kMaxSlowRun = 1 << 22;
 struct ResolveRuns {
     unsigned long long *keys;
     int *vals, *nr;
@@ -393,7 +394,8 @@ constexpr int kLongThreads = 256;
 __global__ void __launch_bounds__(kLongThreads) k_resolve_long(unsigned long long *keys, int *vals, int *nr,
                                                                unsigned long long *tk, int *tv, const int *runs,
                                                                const int4 *cv, const int4 *edges, const double2 *P,
-                                                               int n, int nT, Counters *ct, const int *seg)
+                                                               int n, int nT, Counters *ct, const int *seg,
+                                                               int block_run, int2 *huge)
 {
     __shared__ int red[kLongThreads / 32];
     __shared__ int s_end;
@@ -417,8 +419,8 @@ __global__ void __launch_bounds__(kLongThreads) k_resolve_long(unsigned long lon
     }
     __syncthreads();
     const int e = s_end, L = e - s + 1;
-    if (L > kMaxSlowRun) {
-        if (threadIdx.x == 0) set_err(ct, GPUDT_ERR_EXACT, 113);
+    if (L > block_run) {  // left to the multi-block merge
+        if (threadIdx.x == 0) huge[atomicAdd(&ct->nhuge, 1)] = make_int2(s, L);
         return;
     }
     bool bad = false;
@@ -483,6 +485,107 @@ __global__ void __launch_bounds__(kLongThreads) k_resolve_long(unsigned long lon
         nr[a] = cmp != 0 ? 1 : 0;
     }
     if (bad) set_err(ct, GPUDT_ERR_EXACT, 111);
+}
+
+// One merge level of the multi-block exact sort of a run of L entries:
+// sorted blocks of w entries are merged pairwise from (sk, sv) into (dk, dv).
+// Thread t writes outputs [t*kMergeChunk, (t+1)*kMergeChunk): for each pair
+// of blocks its outputs fall in, it finds where its first output's merge path
+// crosses the pair by binary search (ties take the left block first, so the
+// sort is stable), then merges.
+constexpr int kMergeChunk = 16;
+__global__ void __launch_bounds__(256) k_merge_level(const unsigned long long *__restrict__ sk,
+                                                     const int *__restrict__ sv, unsigned long long *__restrict__ dk,
+                                                     int *__restrict__ dv, int L, int w, const int4 *cv,
+                                                     const int4 *edges, const double2 *P, int nT, Counters *ct)
+{
+    const long long o0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kMergeChunk;
+    if (o0 >= L) return;
+    const long long o1 = min((long long)L, o0 + kMergeChunk);
+    bool bad = false;
+    // the chunk may span several pairs of blocks while 2w < kMergeChunk
+    for (long long pos = o0; pos < o1;) {
+        const int lo = (int)(pos / (2ll * w) * (2ll * w));
+        const int mid = (int)min((long long)L, (long long)lo + w);
+        const int hi = (int)min((long long)L, (long long)lo + 2ll * w);
+        const int na = mid - lo, nb = hi - mid;
+        const int k0 = (int)pos - lo, kend = (int)min((long long)hi, o1) - lo;
+        int a0 = max(0, k0 - nb), a1 = min(k0, na);
+        while (a0 < a1) {
+            const int m = (a0 + a1) >> 1;
+            int c = cmp_entries(sk[lo + m], sv[lo + m], sk[mid + k0 - m - 1], sv[mid + k0 - m - 1], nT, cv, edges,
+                                P);
+            if (c == EXACT_OVERFLOW) {
+                bad = true;
+                c = 0;
+            }
+            if (c <= 0) a0 = m + 1;
+            else a1 = m;
+        }
+        int i = a0, j = k0 - a0;
+        for (int k = k0; k < kend; k++) {
+            bool takeA = i < na;
+            if (takeA && j < nb) {
+                int c = cmp_entries(sk[lo + i], sv[lo + i], sk[mid + j], sv[mid + j], nT, cv, edges, P);
+                if (c == EXACT_OVERFLOW) {
+                    bad = true;
+                    c = 0;
+                }
+                takeA = c <= 0;
+            }
+            const int src = takeA ? lo + i++ : mid + j++;
+            dk[lo + k] = sk[src];
+            dv[lo + k] = sv[src];
+        }
+        pos = lo + kend;
+    }
+    if (bad) set_err(ct, GPUDT_ERR_EXACT, 114);
+}
+
+// Rank-start flags of a sorted run [s, s + L): an entry starts a new rank
+// unless it equals its left neighbour exactly.
+struct RunFlags {
+    const int *vals;
+    int *nr;
+    const int4 *cv, *edges;
+    const double2 *P;
+    int s, nT;
+    Counters *ct;
+    __device__ void operator()(long long ii) const
+    {
+        const int a = s + 1 + (int)ii;
+        int cmp = exact_cmp_vals(vals[a - 1], vals[a], nT, cv, edges, P);
+        if (cmp == EXACT_OVERFLOW) {
+            set_err(ct, GPUDT_ERR_EXACT, 115);
+            cmp = 1;
+        }
+        nr[a] = cmp != 0 ? 1 : 0;
+    }
+};
+
+// The multi-block exact sort of one long run [s, s + L) of (keys, vals),
+// through (tk, tv)[s, s + L) as the second buffer.
+static int merge_sort_run(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *tk, int *tv, int *nr,
+                          int s, int L, int nT)
+{
+    unsigned long long *sk = keys + s, *dk = tk + s;
+    int *sv = vals + s, *dv = tv + s;
+    const long long threads = ((long long)L + kMergeChunk - 1) / kMergeChunk;
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    for (long long w = 1; w < L; w <<= 1) {
+        k_merge_level<<<blocks, 256, 0, c.stream>>>(sk, sv, dk, dv, L, (int)w, alpha_geom_tris(c), c.edges, c.opos,
+                                                     nT, c.ctr);
+        count_launch();
+        std::swap(sk, dk);
+        std::swap(sv, dv);
+    }
+    GALPHA_CUDA(cudaGetLastError());
+    if (sk != keys + s) {
+        launch_n(c, CopyElems<unsigned long long>{keys + s, sk}, L);
+        launch_n(c, CopyElems<int>{vals + s, sv}, L);
+    }
+    launch_n(c, RunFlags{vals, nr, alpha_geom_tris(c), c.edges, c.opos, s, nT, c.ctr}, L - 1);
+    return GPUDT_OK;
 }
 
 struct ScatterRanks {
@@ -734,11 +837,32 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
             if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
             if (c.hctr->nlong > 0) {
                 // (keys2, vals2) are free now: the second buffer of each run's merge sort
-                k_resolve_long<<<(unsigned)c.hctr->nlong, kLongThreads, 0, c.stream>>>(
+                const int nlong = c.hctr->nlong;
+                // runs for the multi-block merge: (start, length) pairs after the long runs, 8-byte aligned
+                uintptr_t hp = reinterpret_cast<uintptr_t>(longs + nlong);
+                int2 *huge = reinterpret_cast<int2 *>((hp + 7) & ~(uintptr_t)7);
+                GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nhuge, 0, sizeof(int), c.stream));
+                k_resolve_long<<<(unsigned)nlong, kLongThreads, 0, c.stream>>>(
                     c.keys, c.vals, nr, c.keys2, c.vals2, longs, alpha_geom_tris(c), c.edges, c.opos, nIn, nT, c.ctr,
-                    segs ? segs->seg : nullptr);
+                    segs ? segs->seg : nullptr, c.block_run, huge);
                 count_launch();
                 GALPHA_CUDA(cudaGetLastError());
+                r = read_counters(c);
+                if (r) return r;
+                if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
+                const int nhuge = c.hctr->nhuge;
+                if (nhuge > 0) {
+                    std::vector<int2> hs(nhuge);
+                    r = read_small(c, hs.data(), huge, sizeof(int2) * (size_t)nhuge);
+                    if (r) return r;
+                    for (const int2 &h : hs) {
+                        r = merge_sort_run(c, c.keys, c.vals, c.keys2, c.vals2, nr, h.x, h.y, nT);
+                        if (r) return r;
+                    }
+                    r = read_counters(c);
+                    if (r) return r;
+                    if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
+                }
             }
         }
     }

@@ -571,6 +571,14 @@ int galphaSetLimits(galphaHandle h, int maxRounds, int spinLimit, int holdFirstT
     return GPUDT_OK;
 }
 
+int galphaSetBlockRun(galphaHandle h, int entries)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->H.c.block_run = entries > 0 ? entries : kBlockRun;
+    return GPUDT_OK;
+}
+
 int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY, double maxX, double maxY,
                     int fboSize, int withAlpha, gpudtStatus *st)
 {

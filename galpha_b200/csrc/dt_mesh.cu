@@ -1785,16 +1785,26 @@ struct FlipCheck {
             const int4 n = tn[t];
             const int nb[3] = {n.x, n.y, n.z};
             const double2 P[3] = {pos[v.x], pos[v.y], pos[v.z]};  // once per triangle, not per edge
+            // the neighbours and their apexes of every edge to be tested are
+            // gathered up front, each level of loads in flight together (the
+            // kernel is bound by the latency of these dependent gathers)
+            bool want[3];
+            int4 tu[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const int e = nb[i];
+                want[i] = e >= 0 && ((fl >> i) & 1) && (act || dtri(e) >= t);  // first round: the lower slot tests
+                tu[i] = want[i] ? tv[dtri(e)] : make_int4(0, 0, 0, 0);
+            }
+            double2 D[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) D[i] = want[i] ? pos[geti(tu[i], dori(nb[i]))] : make_double2(0.0, 0.0);
 #pragma unroll
             for (int i = 0; i < 3; i++) {
                 if (ci >= 0 || err) break;
-                const int e = nb[i];
-                if (e < 0 || !((fl >> i) & 1)) continue;
-                const int u = dtri(e);
-                if (!act && u < t) continue;  // first round: u tests this edge
-                const int d = geti(tv[u], dori(e));
-                const double2 A = P[p1(i)], B = P[m1(i)], C = P[i], D = pos[d];
-                double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D.x, D.y};
+                if (!want[i]) continue;
+                const double2 A = P[p1(i)], B = P[m1(i)], C = P[i];
+                double pa[2] = {A.x, A.y}, pb[2] = {B.x, B.y}, pc[2] = {C.x, C.y}, pd[2] = {D[i].x, D[i].y};
                 ntest++;
                 int s = incircle_filter32(pa, pb, pc, pd);
                 if (s == 2) {
@@ -1809,7 +1819,7 @@ struct FlipCheck {
                 }
                 if (!err && s > 0) {
                     ci = i;
-                    cu = u;
+                    cu = dtri(nb[i]);
                 }
             }
         }
@@ -1849,18 +1859,20 @@ struct FlipApply {
         const int t = cands[ii];
         const int u = target[t];
         const unsigned pt = prio((uint32_t)t);
-        const bool win = (unsigned)vote[t] == pt && (unsigned)vote[u] == pt;
+        // the vote words and both triangles are loaded together (a winner
+        // needs all of them; the kernel is bound by these gathers' latency)
+        const unsigned vt = (unsigned)vote[t], vu = (unsigned)vote[u];
+        const int i = prop[t];
+        const int4 tvv = tv[t], tnn = tn[t], uvv = tv[u], unn = tn[u];
+        const bool win = vt == pt && vu == pt;
         int nx[6], nn = 0;
         Relink r4[4];
         if (!win) {
             if (first) eflag[t] = 7;
             if (fresh(t)) nx[nn++] = t;
         } else {
-            const int i = prop[t];
-            const int4 tvv = tv[t], tnn = tn[t];
             const int e = geti(tnn, i);
             const int j = dori(e);
-            const int4 uvv = tv[u], unn = tn[u];
             const int a = geti(tvv, i), b = geti(tvv, p1(i)), cc = geti(tvv, m1(i)), d = geti(uvv, j);
             const int ot1 = geti(tnn, p1(i)), ot2 = geti(tnn, m1(i));
             const int ou1 = geti(unn, p1(j)), ou2 = geti(unn, m1(j));

@@ -24,6 +24,7 @@ constexpr int kMargin = kFakeSpacing / 2 + 1;    // real sites stay >= 17 pixels
 constexpr int kMaxFan = 64;                      // star holes / fans handled per thread
 constexpr int kMaxRounds = 100000;               // cap of every iterative stage (default)
 constexpr int kSpinLimit = 1 << 22;              // bound of every look-back wait (default)
+constexpr int kBlockRun = 1 << 16;               // longest exact-sort run for one block (default)
 
 // vertex states
 enum : int8_t {
@@ -69,6 +70,7 @@ struct Counters {
     int tail_rounds; // flip: rounds run by the last in-block tail launch
     int runstage;    // fake runs: staged fan entries
     int nlong;       // key sort: out-of-order pairs recorded in groups too long for one thread
+    int nhuge;       // alpha ranks: runs too long for one block, listed for the multi-block merge
 };
 
 // Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
@@ -184,6 +186,10 @@ struct Ctx {
     int max_rounds = kMaxRounds;
     int spin_limit = kSpinLimit;
     int hold_first = 0;
+    // runs of near-equal spectrum keys longer than this are merge-sorted with
+    // the exact comparator by many blocks (one launch per merge level)
+    // instead of by one block
+    int block_run = kBlockRun;
 };
 
 // ------------------------------------------------------------- error helpers

@@ -282,7 +282,13 @@ struct FixFind {
                 long_pair(i);
                 return;
             }
-        starts[atomicAdd(&ct->nlist2, 1)] = s;
+        // one counter atomic per converged group of lanes
+        const unsigned m = __activemask();
+        const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&ct->nlist2, __popc(m));
+        base = __shfl_sync(m, base, leader);
+        starts[base + __popc(m & ((1u << lane) - 1u))] = s;
     }
 };
 
@@ -396,7 +402,7 @@ struct FixGroups {
 // its own inclusive count.  A tile waits only on tiles with earlier tickets,
 // whose blocks are running; the bounded wait guards a broken invariant and
 // reports it in the counter block.  Status words: bits 63-62 kind (1 the
-// tile's count, 2 inclusive), bits 61-32 the pass (so the 5 passes share
+// tile's count, 2 inclusive), bits 61-32 the pass (so the passes share
 // the words, zeroed once per sort), bits 31-0 the count.
 constexpr int kOsPasses = (64 - kLowBits) / 8;
 constexpr int kOsTicketOff = kOsPasses * 256;  // after the digit counts [kOsPasses][256]
@@ -620,11 +626,11 @@ long long radix_sort_scratch_ints(long long n)
     return std::max(radix_scratch_ints(n), onesweep_scratch_ints(n));
 }
 
-// The kOsPasses passes; the result ends in (keys2, vals2) (an odd number of passes).
-static int onesweep_top40(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
+// The kOsPasses passes; the result ends in (keys, vals) after an even number
+// of passes, in (keys2, vals2) after an odd one.
+static int onesweep_top(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n)
 {
     typedef unsigned long long K;
-    static_assert(kOsPasses % 2 == 1, "the result is taken from the second buffer");
     const int smem = (int)sizeof(RsSmem<K>);
     {
         static std::mutex mu;
@@ -664,7 +670,7 @@ static int onesweep_top40(Ctx &c, unsigned long long *keys, int *vals, unsigned 
 }
 
 // The result is left in (keys, vals) or, when *in_second comes back true, in
-// (keys2, vals2): an odd number of passes ends there, and a copy back would
+// (keys2, vals2): where the last digit pass left it, since a copy back would
 // cost a full read and write of both arrays.
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n,
                bool *in_second)
@@ -672,8 +678,8 @@ int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *
     bool sec = false;
     int r;
     if (n > 1 && n < (1 << 30) && onesweep_scratch_ints(n) <= c.rhist_ints) {
-        r = onesweep_top40(c, keys, vals, keys2, vals2, n);
-        sec = true;
+        r = onesweep_top(c, keys, vals, keys2, vals2, n);
+        sec = (kOsPasses & 1) != 0;  // the passes alternate between the two buffer pairs
     } else {
         r = radix_sort_keys<unsigned long long>(c, keys, vals, keys2, vals2, n, c.rhist, kLowBits, &sec);
     }

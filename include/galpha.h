@@ -265,6 +265,16 @@ int galphaEdgeListNoAlloc(const gpudtTriangle *d_tris, int nTris, int *d_edges, 
  * CUDA failures exit the process (common.h:55-93). */
 int galphaSetLimits(galphaHandle h, int maxRounds, int spinLimit, int holdFirstTile);
 
+/* Spectrum entries whose keys lie within 2 ulp of their neighbours form runs
+ * that are ordered with exact arithmetic.  A run of more than `entries`
+ * entries (default 65,536; <= 0 restores it) is merge-sorted by many blocks,
+ * one launch per merge level, instead of by one block; there is no upper
+ * limit on a run's length (a lattice of non-dyadic spacing gives runs of
+ * millions).  No counterpart in the reference, whose odd-even rounds and
+ * host insertion sort (kernel.cu:962-1102, Alpha_Shapes_2D.cu:524-610)
+ * order such runs without a size limit. */
+int galphaSetBlockRun(galphaHandle h, int entries);
+
 /* Text of the last error on the calling thread (cleared when a compute call
  * -- RunDevice, Triangulate, Compute*, RunBatch*, gpudtComputeDTEx -- starts). */
 const char *galphaLastError(void);

@@ -135,3 +135,77 @@ def test_compute_all_matches_two_calls(engine, n, seed):
     dt3, a3 = engine.compute_all(p, copy=False)
     assert canon_set(dt3.vtx) == canon_set(dt1.vtx)
     assert np.array_equal(a3["spectrum"], a1["spectrum"])
+
+
+def _set_block_run(engine, entries):
+    import ctypes
+
+    L = G.load()
+    L.galphaSetBlockRun.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    assert L.galphaSetBlockRun(engine._h, entries) == 0
+
+
+def _lattice(side, spacing_den):
+    g = np.arange(side) / float(spacing_den)
+    return np.stack(np.meshgrid(g, g), -1).reshape(-1, 2).copy()
+
+
+def test_multi_block_exact_runs(engine):
+    """Runs of near-equal spectrum keys longer than one block takes are
+    merge-sorted with the exact comparator by many blocks.  A 200 x 200
+    lattice of spacing 1/1500 (not representable: its squared lengths differ
+    in the last bits) gives runs of about 79,000 triangle values and 79,000
+    edge values, above the 65,536 default; the perturbed 100 x 100 lattice of
+    test_long_key_group takes the multi-block path with the threshold lowered
+    to 512.  Both match the oracle."""
+    pts = _lattice(200, 1500)
+    dt, a = engine.compute_all(G.GPUDTParams(pts, fboSize=1024))
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+    assert ok, rep
+    rng = np.random.default_rng(77)
+    g = np.arange(100) / 128.0
+    pts = np.stack(np.meshgrid(g, g), -1).reshape(-1, 2).copy()
+    moved = rng.choice(len(pts), 60, replace=False)
+    pts[moved, 0] += rng.choice([-1.0, 1.0], 60) * rng.uniform(1e-12, 3e-12, 60)
+    try:
+        _set_block_run(engine, 512)
+        dt, a = engine.compute_all(G.GPUDTParams(pts, fboSize=1024))
+    finally:
+        _set_block_run(engine, 0)
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, a, ULP_TOL)
+    assert ok, rep
+
+
+def test_lattice_1500_runs_above_four_million(engine):
+    """A 1500 x 1500 lattice of spacing 1/1500: about 4.5 M triangle values and
+    4.5 M edge values, each set within a few ulp of one value, forming runs of
+    more than 2^22 entries that the exact comparator must order (the
+    reference orders them in its odd-even rounds; nothing is refused).  Too
+    large for the oracle; checked instead: the spectrum does not decrease
+    (distinct exact values may round to the same double), every rank is in
+    range, and a sample of entry pairs is ordered as exact rational
+    arithmetic orders their values."""
+    from fractions import Fraction
+
+    from fraction_alpha import rho_edge, rho_tri
+
+    pts = _lattice(1500, 1500)
+    dt, a = engine.compute_all(G.GPUDTParams(pts, fboSize=4096))
+    s = a["spectrum"]
+    assert s[0] == 0.0 and np.all(np.diff(s[1:]) >= 0)
+    tri_ro = a["tri_list"]["ro_rank"]
+    e = a["edge_list"]
+    assert dt.nTris == 2 * 1499 * 1499
+    assert tri_ro.min() >= 1 and tri_ro.max() < len(s) and e["ro_rank"].max() < len(s)
+    P = [(Fraction(float(x)), Fraction(float(y))) for x, y in pts]
+    vtx = dt.vtx
+    rng = np.random.default_rng(5)
+    unatt = np.nonzero(e["ro_rank"] > 0)[0]
+    for _ in range(400):
+        t1, t2 = (int(x) for x in rng.integers(0, dt.nTris, 2))
+        r1, r2 = rho_tri(P, *map(int, vtx[t1])), rho_tri(P, *map(int, vtx[t2]))
+        assert (r1 < r2) == (tri_ro[t1] < tri_ro[t2]) and (r1 == r2) == (tri_ro[t1] == tri_ro[t2])
+        k = int(unatt[int(rng.integers(0, len(unatt)))])
+        t, i = int(e["tIndex"][k]), int(e["vOpp"][k])
+        re = rho_edge(P, int(vtx[t][(i + 1) % 3]), int(vtx[t][(i + 2) % 3]))
+        assert (re < r1) == (e["ro_rank"][k] < tri_ro[t1]) and (re == r1) == (e["ro_rank"][k] == tri_ro[t1])
