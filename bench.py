@@ -422,7 +422,7 @@ def main():
         stats_sort = (int(st.sortKeys), int(st.sortPasses))
         stats = {k: getattr(st, k) for k in ("nVerts", "nFake", "nDuplicates", "nMissing", "nBadShift", "nIslandPixels",
                                              "nRepairTiles", "nEscalated",
-                                             "nFlips", "flipRounds", "shiftRounds", "missingRounds")}
+                                             "nFlips", "flipRounds", "shiftRounds", "missingRounds", "hostReads")}
         stats["predicates"] = predicate_stages(st)
     torch.cuda.synchronize()
     launches = L.galphaLaunchCount() - launches0

@@ -76,7 +76,7 @@ class Status(ctypes.Structure):
         ("orientTests", ctypes.c_longlong), ("filteredOrient", ctypes.c_longlong),
         ("ms", ctypes.c_float * 12),
         ("kernelMs", ctypes.c_float * 4),
-        ("sortKeys", ctypes.c_longlong), ("sortPasses", ctypes.c_int), ("pad0", ctypes.c_int),
+        ("sortKeys", ctypes.c_longlong), ("sortPasses", ctypes.c_int), ("hostReads", ctypes.c_int),
     ]
 
     def as_dict(self):

@@ -43,6 +43,7 @@ int read_counters(Ctx &c)
     const int nw = (int)(sizeof(Counters) / 4);
     k_read_words<<<1, 256, 0, c.stream>>>((const unsigned *)c.ctr, (unsigned *)c.hctr_dev, nw);
     count_launch();
+    c.host_reads++;
     GALPHA_CUDA(cudaGetLastError());
     GALPHA_CUDA(cudaStreamSynchronize(c.stream));
     return GPUDT_OK;
@@ -66,6 +67,7 @@ static void fill_predicate_stats(Ctx &c)
 int read_small(Ctx &c, void *host_dst, const void *dev_src, size_t bytes)
 {
     if (bytes == 0) return GPUDT_OK;
+    c.host_reads++;
     if (bytes > kMailBytes || (bytes & 3) || ((uintptr_t)dev_src & 3)) {
         GALPHA_CUDA(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, c.stream));
         GALPHA_CUDA(cudaStreamSynchronize(c.stream));
@@ -257,6 +259,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     r = ensure(H, V, T, 0);
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
+    c.host_reads = 0;
     for (int k = 0; k < 10; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
@@ -341,6 +344,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     r = batch_buffers(c, H.bd, K, bh.N, (int)z.V, c.cap_tris, 3 * c.cap_tris + 8, bh.ntiles);
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
+    c.host_reads = 0;
     for (int k = 0; k < 10; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
@@ -610,6 +614,7 @@ int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, doub
         fill_times(c, 8);
     }
     c.st.status = r;
+    c.st.hostReads = c.host_reads;
     if (st) *st = c.st;
     return r;
 }
@@ -660,6 +665,7 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
     }
     if (!r) fill_times(c, 8);
     c.st.status = r;
+    c.st.hostReads = c.host_reads;
     if (st) *st = c.st;
     return r;
 }
@@ -940,6 +946,7 @@ int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt,
         delete[] tris;
     }
     c.st.status = r;
+    c.st.hostReads = c.host_reads;
     if (st) *st = c.st;
     return r;
 }
@@ -957,6 +964,7 @@ int galphaRunBatch(galphaHandle h, int nSets, const int *setSizes, const double 
     int r = run_batch(h->H, nSets, setSizes, d_xy, bounds, withAlpha);
     if (!r) fill_times(c, withAlpha ? 9 : 8);
     c.st.status = r;
+    c.st.hostReads = c.host_reads;
     if (st) *st = c.st;
     return r;
 }

@@ -178,6 +178,7 @@ struct Ctx {
     int sort_passes = 0;  // radix passes of the last radix_sort call
     bool fused_done = false;  // triangles came from the fused colour + dual kernel
     int round_counter = 1;    // ids of operation rounds (per handle: stamps live in its arena)
+    int host_reads = 0;       // device -> host reads (each a stream synchronisation) of the current call
 
     // failure-detection limits (galphaSetLimits): the round cap of every
     // iterative stage, the spin bound of the single-pass look-back waits, and

@@ -99,7 +99,8 @@ typedef struct {
                                 [3] spectrum key sort (all radix passes, alpha stage) */
     long long sortKeys;      /* keys of the spectrum sort */
     int sortPasses;          /* radix passes it took (8-bit digits) */
-    int pad0;
+    int hostReads;           /* device -> host reads of the call, each one stream synchronisation
+                                (the host reads work-list sizes between stages) */
 } gpudtStatus;
 
 #ifdef __cplusplus

@@ -16,7 +16,7 @@ the gap is reported per case, not asserted.  Both engines rank by exact
 comparison, which is why the ranks agree although the stored values may not.
 
 Sizes stay within one 140,000-entry chunk of the reference's odd-even sort
-(Alpha_Shapes_2D.cu:341-345), the regime its chunk-boundary bookkeeping was
+(Alpha_Shapes_2D.cu:359-363), the regime its chunk-boundary bookkeeping was
 written for.
 """
 import json
