@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched (c4) and serving (c5) legs")
-    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window of the serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the serving leg")
     return ap.parse_args()
 
 

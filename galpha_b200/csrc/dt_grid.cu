@@ -324,10 +324,12 @@ struct FirstDistinct {
 struct CountOffLine {
     const double *xy;
     const int *b;
+    long long n;
     Counters *ct;
     __device__ void operator()(long long i) const
     {
         int j = *b;
+        if (j >= n) return;  // every point equals point 0: nothing is off the line
         int s = orient2d_filter(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
         if (s == 2) s = orient2d_exact(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
         if (s != 0) atomicAdd(&ct->changed, 1);
@@ -339,15 +341,12 @@ int has_triangles(Ctx &c, const double *d_xy, int n)
 {
     if (n < 3) return 0;
     int *first = c.aux;
-    const int big = 0x7f7f7f7f;  // above every point index
     GALPHA_CUDA(cudaMemsetAsync(first, 0x7f, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
     launch_n(c, FirstDistinct{d_xy, first}, n);
-    int hfirst = 0;
-    int rr = read_small(c, &hfirst, first, sizeof(int));
-    if (rr) return rr;
-    if (hfirst == big) return 0;
-    launch_n(c, CountOffLine{d_xy, first, c.ctr}, n);
+    // the line through point 0 and the first point distinct from it (none:
+    // `first` stays above every index and no point counts), one host read
+    launch_n(c, CountOffLine{d_xy, first, n, c.ctr}, n);
     int r = read_counters(c);
     if (r) return r;
     return c.hctr->changed > 0 ? 1 : 0;

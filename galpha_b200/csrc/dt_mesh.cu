@@ -1775,12 +1775,13 @@ struct FlipCheck {
     __device__ void operator()(long long ii) const
     {
         const int t = act ? act[ii] : (int)ii;  // no list: every slot (the first round)
-        const int4 v = tv[t];
+        // a list entry of -1 is a hole left by a fixed-slot FlipApply: nothing to test
+        const int4 v = t >= 0 ? tv[t] : make_int4(-1, -1, -1, 0);
         int ci = -1, cu = -1, ntest = 0, nfilt = 0;
         bool err = false;
         // the first round tests every edge once (from the lower slot); later
         // rounds test the edges a flip or a lost vote left marked
-        const int fl = act ? eflag[t] : 7;
+        const int fl = t < 0 ? 0 : (act ? eflag[t] : 7);
         if (v.x >= 0 && fl) {
             const int4 n = tn[t];
             const int nb[3] = {n.x, n.y, n.z};
@@ -1843,6 +1844,12 @@ struct FlipCheck {
     }
 };
 
+// Outputs of candidate ii go to fixed slots when the record array has room
+// for four per candidate: relink records rec[4ii, 4ii+4) and next-round
+// entries next[2ii, 2ii+2), unused ones written as no-ops ({-1, -1} records,
+// -1 entries, which the relinker and FlipCheck skip).  That replaces three
+// returning atomics per candidate (record, flip and list reservations) --
+// the tail of the kernel's latency chain -- by plain stores.
 struct FlipApply {
     int4 *tv, *tn, *fwd;
     int *epoch, *vtri, *vote, *stamp, *next;
@@ -1853,6 +1860,8 @@ struct FlipApply {
     Counters *ct;
     int8_t *eflag;
     bool first;  // first round: a losing candidate was tested one-sided, so all its edges stay marked
+    const int *cand_n;  // candidates of the round (the launch count)
+    long long rec_cap;  // relink records the array holds
     __device__ bool fresh(int x) const { return x >= 0 && atomicExch(&stamp[x], round) != round; }
     __device__ void operator()(long long ii) const
     {
@@ -1905,6 +1914,21 @@ struct FlipApply {
             eflag[u] = 5;
             if (fresh(t)) nx[nn++] = t;
             if (fresh(u)) nx[nn++] = u;
+        }
+        const int nc = *cand_n;  // the same for every thread of the launch
+        if (4ll * nc <= rec_cap) {
+            if (ii == 0) {
+                ct->nrec = 4 * nc;
+                *next_n = 2 * nc;
+            }
+            Relink *rr = rec + 4 * ii;
+            for (int k = 0; k < 4; k++) rr[k] = win ? r4[k] : Relink{-1, -1};
+            next[2 * ii] = nn > 0 ? nx[0] : -1;
+            next[2 * ii + 1] = nn > 1 ? nx[1] : -1;
+            const unsigned m = __activemask();
+            const int wins = __popc(__ballot_sync(m, win));
+            if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && wins) atomicAdd(&ct->nflips, wins);
+            return;
         }
         // one atomic per warp for each of the records, the flip count and the next list
         const int rb = warp_reserve(&ct->nrec, win ? 4 : 0);
@@ -2026,7 +2050,7 @@ int stage_flip(Ctx &c)
             k_flip_tail<<<1, kTailThreads, 0, c.stream>>>(
                 FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr, c.eflag},
                 FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nullptr, nullptr, prop, target, cands,
-                          c.rec, 0, c.ctr, c.eflag, false},
+                          c.rec, 0, c.ctr, c.eflag, false, &c.ctr->cand, 3ll * c.cap_tris},
                 Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, 0, c.ctr}, FlipReset{c.vote, target, cands},
                 lists[0], lists[1], p, round0, c.max_rounds + 1 - rounds, kTailLeave);
             count_launch();
@@ -2056,7 +2080,7 @@ int stage_flip(Ctx &c)
                            &c.ctr->act[p], capn);
             launch_dev(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, lists[1 - p],
                                     &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr, c.eflag,
-                                    rounds == 0},
+                                    rounds == 0, &c.ctr->cand, 3ll * c.cap_tris},
                        &c.ctr->cand, capn);
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
             launch_dev(c, FlipReset{c.vote, target, cands}, &c.ctr->cand, capn);
