@@ -654,40 +654,47 @@ struct FixPt {
 // Set of each value-sorted entry (triangle, or the triangle that owns the edge).
 // Set of every entry id in entry order (triangles, then edges in triangle
 // order): coalesced reads, so the sorted entries need one gather each.
-struct SetOfEntry {
-    const int4 *edges;
-    const int *tset;
-    int nT;
-    int *eset;
-    __device__ void operator()(long long v) const
+// First edge of each set (and [K] = nE): edges are numbered in triangle
+// order and triangles are grouped by set.
+struct SetEdgeBases {
+    const int *e_off, *tbase;
+    int nT, nE;
+    int *ebase;
+    __device__ void operator()(long long s) const
     {
-        eset[v] = tset[v < nT ? (int)v : edges[v - nT].z];
+        const int t = tbase[s];
+        ebase[s] = t < nT ? e_off[t] : nE;
     }
 };
 
+// Set of each value-sorted entry, by binary search of its id in the per-set
+// bases (triangles and edges are each grouped by set, bases non-decreasing;
+// the last set whose base is at most the id owns it) -- no gather by id.
 struct EntrySet {
     const int *vals;
-    const int *eset;
+    const int *tbase, *ebase;
+    int K, nT;
     unsigned *key;
-    int *pos;
     __device__ void operator()(long long i) const
     {
-        key[i] = (unsigned)eset[vals[i]];
-        pos[i] = (int)i;
+        const int v = vals[i];
+        const int *b = v < nT ? tbase : ebase;
+        const int x = v < nT ? v : v - nT;
+        int lo = 0, hi = K;  // the answer lies in [lo, hi): b[lo] <= x < b[hi]
+        while (hi - lo > 1) {
+            const int m = (lo + hi) >> 1;
+            if (b[m] <= x) lo = m;
+            else hi = m;
+        }
+        key[i] = (unsigned)lo;
     }
 };
 
-struct GatherEntries {
-    const unsigned long long *keys;
-    const int *vals, *pos;
+struct SetOfSorted {
     const unsigned *setkey;
-    unsigned long long *okeys;
-    int *ovals, *seg;  // seg is indexed like the full entry array (entry 0 = sentinel)
+    int *seg;  // indexed like the full entry array (entry 0 = sentinel)
     __device__ void operator()(long long i) const
     {
-        int p = pos[i];
-        okeys[i] = keys[p];
-        ovals[i] = vals[p];
         seg[1 + i] = (int)setkey[i];
         if (i == 0) seg[0] = -1;
     }
@@ -796,18 +803,17 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     c.st.sortKeys = nIn - 1;
     c.st.sortPasses = c.sort_passes;
     if (segs) {
-        // stable sort by set: entries end up ordered by (set, value)
+        // stable sort by set, carrying each entry's key and value: entries end
+        // up ordered by (set, value)
         const int m = nIn - 1;
-        unsigned *ka = (unsigned *)c.keys2, *kb = ka + ((m + 63) & ~63);
-        int *eset = c.inc;  // the incidence / fan store of the mesh stages is free now
-        launch_n(c, SetOfEntry{c.edges, segs->tset, nT, eset}, nT + nE);
-        launch_n(c, EntrySet{c.vals + 1, eset, ka, c.vals2}, m);
-        r = radix_sort32(c, ka, c.vals2, kb, c.aux2, m, c.rhist);
+        unsigned *ka = (unsigned *)c.rank, *kb = (unsigned *)c.aux2;  // both free until the ranks
+        launch_n(c, SetEdgeBases{c.e_off, segs->tbase, nT, nE, segs->ebase}, segs->K + 1);
+        launch_n(c, EntrySet{c.vals + 1, segs->tbase, segs->ebase, segs->K, nT, ka}, m);
+        int bits = 0;
+        while ((1ll << bits) < segs->K) bits++;
+        r = radix_sort_set_kv(c, ka, kb, c.keys + 1, c.vals + 1, c.keys2 + 1, c.vals2 + 1, m, bits);
         if (r) return r;
-        unsigned long long *tk = (unsigned long long *)c.spectrum;
-        launch_n(c, GatherEntries{c.keys + 1, c.vals + 1, c.vals2, ka, tk, c.rank, segs->seg}, m);
-        launch_n(c, CopyElems<unsigned long long>{c.keys + 1, tk}, m);
-        launch_n(c, CopyElems<int>{c.vals + 1, c.rank}, m);
+        launch_n(c, SetOfSorted{ka, segs->seg}, m);
     }
     // ranks
     int *nr = c.aux, *unc = c.list, *slow = c.list2, *slowflag = c.stamp;

@@ -371,7 +371,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     c.have_mesh = true;
     bh.alpha = false;
     if (withAlpha) {
-        AlphaSegs segs{H.bd.tset, K, H.bd.seg, H.bd.firstexcl, H.bd.nd, H.bd.spec_off};
+        AlphaSegs segs{H.bd.tset, K, H.bd.seg, H.bd.firstexcl, H.bd.nd, H.bd.spec_off, H.bd.tbase, H.bd.ebase};
         STAGE("alpha", stage_alpha(c, &segs));
         c.have_alpha = true;
         bh.alpha = true;

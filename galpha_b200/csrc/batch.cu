@@ -375,7 +375,7 @@ int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, 
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t need = al(sizeof(SetDesc) * (size_t)K) + 2 * al(4 * (size_t)(K + 1)) + al(4 * (size_t)N + 4) +
                   al(4 * (size_t)V + 4) + 3 * al(4 * (size_t)(K + 1)) + al(4 * (size_t)cap + 4) +
-                  al(4 * (size_t)(K + 1)) + al(4 * (size_t)nspec + 4) + 3 * al(4 * (size_t)(K + 1)) +
+                  al(4 * (size_t)(K + 1)) + al(4 * (size_t)nspec + 4) + 4 * al(4 * (size_t)(K + 1)) +
                   al(sizeof(gpudtTriangle) * (size_t)cap) + 2 * al(8 * (size_t)(K + 1)) + al(4 * (size_t)(K + 1)) +
                   al(48 * (size_t)(K + 1)) + al(4 * (size_t)(K + 1)) + al(8 * (size_t)(ntiles + 1));
     if (need > B.bytes) {
@@ -405,6 +405,7 @@ int batch_buffers(Ctx &c, BatchDev &B, int K, int N, int V, int cap, int nspec, 
     B.firstexcl = (int *)take(4 * (size_t)(K + 1));
     B.nd = (int *)take(4 * (size_t)(K + 1));
     B.spec_off = (int *)take(4 * (size_t)(K + 1));
+    B.ebase = (int *)take(4 * (size_t)(K + 1));
     B.otri = (gpudtTriangle *)take(sizeof(gpudtTriangle) * (size_t)cap);
     B.qparam = (double *)take(8 * (size_t)(K + 1));
     B.qalpha = (double *)take(8 * (size_t)(K + 1));

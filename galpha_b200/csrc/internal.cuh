@@ -404,7 +404,7 @@ struct BatchDev {
     SetDesc *sets = nullptr;
     int *vbases = nullptr, *fbases = nullptr, *vset = nullptr, *vsetall = nullptr, *first = nullptr,
         *offline = nullptr, *esc = nullptr, *tset = nullptr, *tbase = nullptr, *seg = nullptr,
-        *firstexcl = nullptr, *nd = nullptr, *spec_off = nullptr;
+        *firstexcl = nullptr, *nd = nullptr, *spec_off = nullptr, *ebase = nullptr;
     gpudtTriangle *otri = nullptr;  // [cap] set-local output triangles
     double *qparam = nullptr, *qalpha = nullptr;  // [K] per-set query values
     int *qR = nullptr, *qcounts = nullptr;        // [K], [12 K]
@@ -434,6 +434,8 @@ struct AlphaSegs {
     int *firstexcl;   // [K] global rank count before the set's first entry
     int *nd;          // [K] distinct values of the set
     int *spec_off;    // [K + 1] first spectrum slot of the set (its rank 0)
+    const int *tbase; // [K + 1] first compacted triangle of each set (non-decreasing; [K] = nT)
+    int *ebase;       // [K + 1] scratch: first edge of each set
 };
 int stage_alpha(Ctx &c, AlphaSegs *segs = nullptr);
 int alpha_query(Ctx &c, double alpha, double q, bool by_quantile);
@@ -466,6 +468,10 @@ int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *o
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n,
                bool *in_second);
 int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);
+// Stable sort by the low nbits of 32-bit set ids, moving (keys, vals) along;
+// the result ends in (skey, keys, vals).
+int radix_sort_set_kv(Ctx &c, unsigned *skey, unsigned *skey2, unsigned long long *keys, int *vals,
+                      unsigned long long *keys2, int *vals2, int n, int nbits);
 // Geometry of the compacted mesh for the alpha stage: triangles with the
 // mesh stages' vertex ids (cv holds input ids, which decide edge ownership
 // and index the point intervals; after a spatial numbering the internal ids

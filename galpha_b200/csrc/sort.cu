@@ -748,3 +748,155 @@ int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int
 }
 
 }  // namespace galpha
+
+namespace galpha {
+
+// ------------------------------------- set-key sort with a (key, value) payload
+// Stable LSD sort of 32-bit set ids that moves each entry's 64-bit key and int
+// value with it: the batched alpha stage turns its value-sorted entries into
+// (set, value) order in ceil(bits / 8) passes of coalesced reads and run-wise
+// writes, instead of sorting positions and gathering the entries afterwards.
+struct RsKvSmem {
+    unsigned key[kRsTile];
+    unsigned long long pk[kRsTile];
+    int pv[kRsTile];
+    int wcnt[kRsWarps][256];
+    int lstart[256];
+    int gbase[256];
+};
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter_kv(const unsigned *__restrict__ kin,
+                                                              const unsigned long long *__restrict__ pkin,
+                                                              const int *__restrict__ pvin, unsigned *__restrict__ kout,
+                                                              unsigned long long *__restrict__ pkout,
+                                                              int *__restrict__ pvout, int n, int shift,
+                                                              const int *__restrict__ hoff, int nblocks)
+{
+    extern __shared__ __align__(16) unsigned char rs_smem_kv[];
+    RsKvSmem &S = *reinterpret_cast<RsKvSmem *>(rs_smem_kv);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = lane; d < 256; d += 32) S.wcnt[w][d] = 0;
+    S.gbase[threadIdx.x] = hoff[threadIdx.x * nblocks + blockIdx.x];
+    __syncwarp();
+    const long long tile0 = (long long)blockIdx.x * kRsTile;
+    const long long base = tile0 + (long long)w * (kRsItems * 32);
+    unsigned key[kRsItems];
+    unsigned long long pk[kRsItems];
+    int pv[kRsItems], rk[kRsItems];
+    const unsigned lanemask_lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kRsItems; r++) {
+        const long long i = base + r * 32 + lane;
+        const bool ok = i < n;
+        key[r] = ok ? kin[i] : 0u;
+        pk[r] = ok ? pkin[i] : 0ull;
+        pv[r] = ok ? pvin[i] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kRsItems; r++) {
+        const bool ok = base + r * 32 + lane < n;
+        const int dg = (int)((key[r] >> shift) & 255);
+        unsigned peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const unsigned bb = __ballot_sync(0xffffffffu, (dg >> b) & 1);
+            peers &= ((dg >> b) & 1) ? bb : ~bb;
+        }
+        const int leader = ok ? __ffs(peers) - 1 : lane;
+        int before = 0;
+        if (ok && lane == leader) before = atomicAdd(&S.wcnt[w][dg], __popc(peers));
+        before = __shfl_sync(0xffffffffu, before, leader);
+        rk[r] = before + __popc(peers & lanemask_lt);
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x;
+        int s = 0;
+        for (int q = 0; q < kRsWarps; q++) {
+            const int c = S.wcnt[q][d];
+            S.wcnt[q][d] = s;
+            s += c;
+        }
+        S.lstart[d] = s;
+    }
+    __syncthreads();
+    if (w == 0) {
+        int carry = 0;
+        for (int d0 = 0; d0 < 256; d0 += 32) {
+            const int v = S.lstart[d0 + lane];
+            int incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            S.lstart[d0 + lane] = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRsItems; r++) {
+        const long long i = base + r * 32 + lane;
+        if (i < n) {
+            const int dg = (int)((key[r] >> shift) & 255);
+            const int p = S.lstart[dg] + S.wcnt[w][dg] + rk[r];
+            S.key[p] = key[r];
+            S.pk[p] = pk[r];
+            S.pv[p] = pv[r];
+        }
+    }
+    __syncthreads();
+    const int cnt = (int)min((long long)kRsTile, (long long)n - tile0);
+    for (int p = threadIdx.x; p < cnt; p += kRsThreads) {
+        const unsigned k = S.key[p];
+        const int d = (int)((k >> shift) & 255);
+        const long long g = (long long)S.gbase[d] + (p - S.lstart[d]);
+        kout[g] = k;
+        pkout[g] = S.pk[p];
+        pvout[g] = S.pv[p];
+    }
+}
+
+int radix_sort_set_kv(Ctx &c, unsigned *skey, unsigned *skey2, unsigned long long *keys, int *vals,
+                      unsigned long long *keys2, int *vals2, int n, int nbits)
+{
+    if (n <= 1 || nbits <= 0) return GPUDT_OK;
+    const int smem = (int)sizeof(RsKvSmem);
+    {
+        static std::mutex mu;
+        static bool attr_set[64];
+        std::lock_guard<std::mutex> lk(mu);
+        if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
+            GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter_kv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            GALPHA_CUDA(cudaFuncSetAttribute(k_rs_scatter_kv, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             cudaSharedmemCarveoutMaxShared));
+            if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+        }
+    }
+    const int nblocks = (n + kRsTile - 1) / kRsTile;
+    int *hist = c.rhist + 8;
+    unsigned *ki = skey, *ko = skey2;
+    unsigned long long *pki = keys, *pko = keys2;
+    int *pvi = vals, *pvo = vals2;
+    for (int shift = 0; shift < nbits; shift += 8) {
+        c.sort_passes++;
+        k_rs_hist<unsigned><<<nblocks, kRsThreads, 0, c.stream>>>(ki, n, shift, hist, nblocks);
+        count_launch();
+        int r = exclusive_scan_int(c, hist, hist, 256 * nblocks, nullptr);
+        if (r) return r;
+        k_rs_scatter_kv<<<nblocks, kRsThreads, smem, c.stream>>>(ki, pki, pvi, ko, pko, pvo, n, shift, hist, nblocks);
+        count_launch();
+        GALPHA_CUDA(cudaGetLastError());
+        std::swap(ki, ko);
+        std::swap(pki, pko);
+        std::swap(pvi, pvo);
+    }
+    if (pki != keys) {  // an odd number of passes: the result is in the second buffers
+        launch_n(c, CopyElems<unsigned long long>{keys, pki}, n);
+        launch_n(c, CopyElems<int>{vals, pvi}, n);
+        launch_n(c, CopyElems<unsigned>{skey, ki}, n);
+    }
+    return GPUDT_OK;
+}
+
+}  // namespace galpha
