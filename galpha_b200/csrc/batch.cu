@@ -331,19 +331,25 @@ struct FillEmptyBases {
 };
 
 // --------------------------------------------------------------- outputs
+// gpudtTriangle records with set-local indices, straight from the compacted
+// mesh (cv / cn), so compaction writes no record array of its own.
 struct LocalTriangles {
-    const gpudtTriangle *in;
+    const int4 *cv, *cn;
     const int *tset, *tbase;
     const SetDesc *sets;
     gpudtTriangle *out;
     __device__ void operator()(long long t) const
     {
-        gpudtTriangle g = in[t];
-        int s = tset[t], tb = tbase[s], vb = sets[s].vbase;
-        for (int k = 0; k < 3; k++) {
-            g.vtx[k] -= vb;
-            if (g.tri[k] >= 0) g.tri[k] -= tb << 2;
-        }
+        const int4 v = cv[t], n = cn[t];
+        const int s = tset[t], tb = tbase[s], vb = sets[s].vbase;
+        gpudtTriangle g;
+        g.vtx[0] = v.x - vb;
+        g.vtx[1] = v.y - vb;
+        g.vtx[2] = v.z - vb;
+        g.tri[0] = n.x >= 0 ? n.x - (tb << 2) : n.x;
+        g.tri[1] = n.y >= 0 ? n.y - (tb << 2) : n.y;
+        g.tri[2] = n.z >= 0 ? n.z - (tb << 2) : n.z;
+        g.tmp[0] = g.tmp[1] = g.tmp[2] = 0;
         out[t] = g;
     }
 };
@@ -696,7 +702,7 @@ int batch_compact(Ctx &c, BatchDev &B, BatchHost &bh)
     GALPHA_CUDA(cudaMemsetAsync(B.tbase, 0xff, sizeof(int) * (size_t)(bh.K + 1), c.stream));
     launch_n(c, NewIndex{ka, c.vals, c.aux2, B.tset, B.tbase, nalive, nt, bh.K}, nt);
     launch_n(c, FillEmptyBases{B.tbase, bh.K, nalive}, 1);
-    launch_compact_write(c, c.aux2, nt);
+    launch_compact_gather(c, c.vals, c.aux2, nalive);
     GALPHA_CUDA(cudaGetLastError());
     c.nT_out = nalive;
     bh.tbase.resize(bh.K + 1);
@@ -709,7 +715,7 @@ int batch_compact(Ctx &c, BatchDev &B, BatchHost &bh)
 // Triangles and edge intervals with set-local vertex and triangle indices.
 int batch_local_outputs(Ctx &c, BatchDev &B, gpudtTriangle *tris, galphaEdgeInterval *edges)
 {
-    if (tris && c.nT_out > 0) launch_n(c, LocalTriangles{c.outtri, B.tset, B.tbase, B.sets, tris}, c.nT_out);
+    if (tris && c.nT_out > 0) launch_n(c, LocalTriangles{c.cv, c.cn, B.tset, B.tbase, B.sets, tris}, c.nT_out);
     if (edges && c.nE > 0)
         launch_n(c, LocalEdges{c.edges, c.edge_ro, c.edge_nu, B.tset, B.tbase, edges}, c.nE);
     GALPHA_CUDA(cudaGetLastError());

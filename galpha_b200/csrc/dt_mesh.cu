@@ -2141,6 +2141,39 @@ struct CompactWrite {
     }
 };
 
+// The same compaction driven by the new order: new triangle j is slot
+// order[j] (alive slots sorted by set, slot order kept within a set), so the
+// writes are consecutive and only the reads follow the slots.
+struct CompactGather {
+    const int4 *tv, *tn;
+    const int *order, *newidx;
+    int4 *cv, *cn;
+    const int *perm;  // internal -> input vertex index (nullptr: identity)
+    int4 *cvi;        // with perm: the triangles with internal ids (alpha-stage geometry)
+    __device__ void operator()(long long jj) const
+    {
+        const int j = (int)jj, t = order[j];
+        int4 v = tv[t];
+        const int4 n = tn[t];
+        if (perm) {
+            cvi[j] = make_int4(v.x, v.y, v.z, 0);
+            v = make_int4(perm[v.x], perm[v.y], perm[v.z], 0);
+        }
+        int nn[3] = {n.x, n.y, n.z};
+        for (int q = 0; q < 3; q++)
+            if (nn[q] >= 0) nn[q] = enc(newidx[dtri(nn[q])], dori(nn[q]));
+        cv[j] = make_int4(v.x, v.y, v.z, 0);
+        cn[j] = make_int4(nn[0], nn[1], nn[2], 0);
+    }
+};
+
+void launch_compact_gather(Ctx &c, const int *order, const int *newidx, int nalive)
+{
+    launch_n(c, CompactGather{c.tv, c.tn, order, newidx, c.cv, c.cn, c.renumbered ? c.perm : nullptr, c.fwd},
+             nalive);
+    c.outtri_ready = false;
+}
+
 // gpudtTriangle records of the compacted mesh (tmp[] zero).
 struct SoaToAos {
     const int4 *cv, *cn;
@@ -2167,13 +2200,6 @@ int ensure_outtri(Ctx &c)
     GALPHA_CUDA(cudaGetLastError());
     c.outtri_ready = true;
     return GPUDT_OK;
-}
-
-void launch_compact_write(Ctx &c, const int *newidx, int nslots)
-{
-    launch_n(c, CompactWrite{c.tv, c.tn, newidx, c.cv, c.cn, c.outtri, c.renumbered ? c.perm : nullptr, c.fwd},
-             nslots);
-    c.outtri_ready = true;
 }
 
 int stage_compact(Ctx &c)

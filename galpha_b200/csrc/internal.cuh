@@ -413,7 +413,9 @@ struct BatchDev {
 };
 
 void grid_scaling(double minX, double minY, double maxX, double maxY, int T, double &scale, double &sx, double &sy);
-void launch_compact_write(Ctx &c, const int *newidx, int nslots);
+// Compaction in the new order: new triangle j is slot order[j], j < nalive
+// (cv / cn only).
+void launch_compact_gather(Ctx &c, const int *order, const int *newidx, int nalive);
 int batch_plan(BatchHost &bh, int K, const int *sizes, const double *bounds);
 int fused_tiles(int T);  // tiles of the fused colouring kernel per T x T cell
 // The mesh in the gpudtTriangle layout (outtri), built from cv / cn when a
