@@ -207,8 +207,9 @@ class GPUDTParams:
         self.minY = float(lo[1] if minY is None else minY)
         self.maxX = float(hi[0] if maxX is None else maxX)
         self.maxY = float(hi[1] if maxY is None else maxY)
-        self.constraints = constraints
-        self.nConstraints = 0 if constraints is None else len(constraints)
+        # constrained edges: (M, 2) point indices (gpudt.h: two per constraint)
+        self.constraints = None if constraints is None else np.ascontiguousarray(constraints, dtype=np.int32).reshape(-1, 2)
+        self.nConstraints = 0 if constraints is None else self.constraints.shape[0]
 
     def _c(self):
         p = _Params()
@@ -216,7 +217,7 @@ class GPUDTParams:
         p.nPoints = self.nPoints
         p.points = self.points.ctypes.data if self.nPoints else None
         p.nConstraints = self.nConstraints
-        p.constraints = None
+        p.constraints = self.constraints.ctypes.data if self.nConstraints else None
         p.fboSize = self.fboSize
         return p
 

@@ -260,6 +260,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
     c.host_reads = 0;
+    c.chash = nullptr;  // no constrained edges unless this call's constraint stage sets them
     for (int k = 0; k < 10; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
@@ -290,6 +291,7 @@ static int run_dt(HandleState &H, const double *d_xy, int n, double minX, double
     STAGE("missing", stage_missing(c));
     ev_record(c, 5);
     STAGE("boundary", stage_boundary(c));
+    STAGE("constraints", stage_constraints(c));
     ev_record(c, 6);
     STAGE("flip", stage_flip(c));
     ev_record(c, 7);
@@ -345,6 +347,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     if (r) return r;
     memset(&c.st, 0, sizeof(c.st));
     c.host_reads = 0;
+    c.chash = nullptr;  // no constrained edges unless this call's constraint stage sets them
     for (int k = 0; k < 10; k++) c.kev_rec[k] = false;
     c.have_mesh = c.have_alpha = c.have_master = false;
     ev_record(c, 1);
@@ -363,6 +366,7 @@ static int run_batch(HandleState &H, int K, const int *sizes, const double *d_xy
     STAGE("missing", stage_missing(c));
     ev_record(c, 5);
     STAGE("boundary", stage_boundary(c));
+    STAGE("constraints", stage_constraints(c));
     ev_record(c, 6);
     STAGE("flip", stage_flip(c));
     ev_record(c, 7);
@@ -443,7 +447,14 @@ static int check_params(const GPUDTPARAMS *p)
 {
     if (!p) return GPUDT_ERR_ARG;
     if (p->nPoints < 0 || (p->nPoints > 0 && !p->points)) return GPUDT_ERR_ARG;
-    if (p->nConstraints != 0) return GPUDT_ERR_ARG;
+    if (p->nConstraints < 0 || (p->nConstraints > 0 && !p->constraints)) return GPUDT_ERR_ARG;
+    for (int k = 0; k < p->nConstraints; k++) {
+        const int a = p->constraints[2 * k], b = p->constraints[2 * k + 1];
+        if (a < 0 || b < 0 || a >= p->nPoints || b >= p->nPoints || a == b) {
+            set_last_error("constraint with an endpoint out of range, or with equal endpoints");
+            return GPUDT_ERR_ARG;
+        }
+    }
     if (!fbo_ok(p->fboSize)) return GPUDT_ERR_ARG;
     if (p->nPoints >= (1 << 28)) return GPUDT_ERR_ARG;
     if (!(std::isfinite(p->minX) && std::isfinite(p->minY) && std::isfinite(p->maxX) && std::isfinite(p->maxY)))
@@ -534,6 +545,8 @@ int galphaDestroy(galphaHandle h)
     if (h->H.arena.base) cudaFree(h->H.arena.base);
     if (h->H.d_xy) cudaFree(h->H.d_xy);
     if (c.ml_buf) cudaFree(c.ml_buf);
+    if (c.cons_buf) cudaFree(c.cons_buf);
+    if (c.cons_pool) cudaFree(c.cons_pool);
     if (h->H.bd.buf) cudaFree(h->H.bd.buf);
     if (c.hctr) cudaFreeHost(c.hctr);
     for (int k = 0; k < GALPHA_STAGE_TOTAL + 2 && c.events; k++) cudaEventDestroy(c.ev[k]);
@@ -631,9 +644,13 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
     cudaGetLastError();  // clear an error left by unrelated runtime calls
     ev_record(c, 0);
     r = upload_points(h->H, params->points, params->nPoints);
+    c.n_cons = params->nConstraints;
+    c.h_cons = params->constraints;
     if (!r)
         r = run_dt(h->H, h->H.d_xy, params->nPoints, params->minX, params->minY, params->maxX, params->maxY,
                    params->fboSize);
+    c.n_cons = 0;
+    c.h_cons = nullptr;
     if (!r && out) {
         int n = params->nPoints;
         gpudtTriangle *tris = nullptr;
@@ -894,9 +911,13 @@ int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt,
     }
     ev_record(c, 0);
     r = upload_points(H, params->points, params->nPoints);
+    c.n_cons = params->nConstraints;
+    c.h_cons = params->constraints;
     if (!r)
         r = run_dt(H, H.d_xy, params->nPoints, params->minX, params->minY, params->maxX, params->maxY,
                    params->fboSize);
+    c.n_cons = 0;
+    c.h_cons = nullptr;
     gpudtTriangle *tris = nullptr;
     bool owned = false, copying = false;
     if (!r) {

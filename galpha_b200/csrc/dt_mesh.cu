@@ -1764,6 +1764,33 @@ constexpr int kFlipSync = 4;
 // so the two new triangles are listed with their outer edges marked
 // (eflag), and later rounds test marked edges only.  A candidate that loses
 // its vote keeps its marks (all three after the one-sided first round).
+// Set of constrained edges: open addressing over keys (min id << 32 | max id),
+// empty slots ~0 (constraints, section below).
+__device__ __forceinline__ unsigned long long cons_key(int a, int b)
+{
+    const unsigned lo = (unsigned)min(a, b), hi = (unsigned)max(a, b);
+    return ((unsigned long long)lo << 32) | hi;
+}
+
+__device__ __forceinline__ unsigned cons_slot(unsigned long long k, unsigned mask)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    return (unsigned)k & mask;
+}
+
+__device__ __forceinline__ bool cons_has(const unsigned long long *h, unsigned mask, int a, int b)
+{
+    const unsigned long long k = cons_key(a, b);
+    for (unsigned s = cons_slot(k, mask), n = 0; n <= mask; s = (s + 1) & mask, n++) {
+        const unsigned long long x = h[s];
+        if (x == k) return true;
+        if (x == ~0ull) return false;
+    }
+    return false;
+}
+
 struct FlipCheck {
     const int4 *tv, *tn;
     const double2 *pos;
@@ -1772,6 +1799,8 @@ struct FlipCheck {
     int *cand_n;
     Counters *ct;
     int8_t *eflag;
+    const unsigned long long *chash;  // constrained edges, never flipped (null: none)
+    unsigned cmask;
     __device__ void operator()(long long ii) const
     {
         const int t = act ? act[ii] : (int)ii;  // no list: every slot (the first round)
@@ -1795,6 +1824,7 @@ struct FlipCheck {
             for (int i = 0; i < 3; i++) {
                 const int e = nb[i];
                 want[i] = e >= 0 && ((fl >> i) & 1) && (act || dtri(e) >= t);  // first round: the lower slot tests
+                if (want[i] && chash && cons_has(chash, cmask, geti(v, p1(i)), geti(v, m1(i)))) want[i] = false;
                 tu[i] = want[i] ? tv[dtri(e)] : make_int4(0, 0, 0, 0);
             }
             double2 D[3];
@@ -2048,7 +2078,8 @@ int stage_flip(Ctx &c)
             const int p = rounds & 1;
             const int round0 = next_round(c);
             k_flip_tail<<<1, kTailThreads, 0, c.stream>>>(
-                FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr, c.eflag},
+                FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr, c.eflag,
+                          c.chash, c.cmask},
                 FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nullptr, nullptr, prop, target, cands,
                           c.rec, 0, c.ctr, c.eflag, false, &c.ctr->cand, 3ll * c.cap_tris},
                 Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, 0, c.ctr}, FlipReset{c.vote, target, cands},
@@ -2072,11 +2103,11 @@ int stage_flip(Ctx &c)
             launch_n(c, FlipRoundStart{p, c.ctr}, 1);
             if (rounds == 0)
                 launch_n(c, FlipCheck{c.tv, c.tn, c.pos, nullptr, c.vote, prop, target, cands, &c.ctr->cand, c.ctr,
-                                      c.eflag},
+                                      c.eflag, c.chash, c.cmask},
                          nt);
             else
                 launch_dev(c, FlipCheck{c.tv, c.tn, c.pos, lists[p], c.vote, prop, target, cands, &c.ctr->cand,
-                                        c.ctr, c.eflag},
+                                        c.ctr, c.eflag, c.chash, c.cmask},
                            &c.ctr->act[p], capn);
             launch_dev(c, FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, lists[1 - p],
                                     &c.ctr->act[1 - p], prop, target, cands, c.rec, round, c.ctr, c.eflag,
@@ -2095,6 +2126,593 @@ int stage_flip(Ctx &c)
     }
     c.st.nFlips = c.hctr->flips_total + c.hctr->nflips;
     c.st.flipRounds = rounds;
+    return GPUDT_OK;
+}
+
+// ------------------------------------------------------------ constraints
+// Constrained edges (GPUDTPARAMS.nConstraints > 0; the reference inserts them
+// in cudaConstraint, gpudt/Cuda/cudaConstraint.cu:828-939, and its flipping
+// never flips a marked edge, cudaFlipping.cu:111-220, gpudt.cpp:88-155).
+// Here they are inserted after the fake ring is gone and before the flip
+// stage, in rounds:
+//   1. each constraint (a, b) that is not yet an edge walks from a along the
+//      segment, counting the triangles it crosses, and claims them and their
+//      neighbours (atomicMin of its index on the vote words);
+//   2. a constraint that holds every claim records its walk: the crossed
+//      triangles (their slots are reused), the chains of vertices right and
+//      left of the segment, and the outer link of every chain edge;
+//   3. each winner re-triangulates the two cavities on either side of the
+//      segment (every chain vertex lies strictly on its side), each by the
+//      Delaunay choice of apex over the base (for the base (u, w), the chain
+//      vertex whose circle through u and w holds no other one) applied
+//      recursively; the segment becomes the edge shared by the two roots.
+//      A vertex whose whole star was crossed lies inside a cavity (the walk
+//      records it as a spike u, x, u): it is left out of the chain and put
+//      back afterwards by a split of the new triangle that holds it.
+// Winners own their crossed triangles and the neighbours around them, so their
+// writes never meet, and the constraint with the lowest index among those
+// left always wins: every round inserts at least one.  The flip stage then
+// leaves the constrained edges in place (FlipCheck looks them up in a hash
+// set), which yields the constrained Delaunay triangulation.  A segment that
+// passes through another vertex, or a vertex that is not in the mesh, is an
+// argument error (GPUDT_ERR_ARG); crossing constraints exhaust the round cap.
+constexpr int kConsWalkMax = 1 << 22;  // crossed edges of one constraint
+
+struct ConsWalker {
+    const int4 *tv, *tn;
+    const double2 *pos;
+    const int *vtri;
+    Counters *ct;
+    // The first crossed edge of (a, b): the triangle (a, p, q) whose corner at
+    // a holds the direction of b.  Returns 1 and (t, ja), 0 when (a, b) is an
+    // edge already, -1 on an error (recorded in the counters).
+    __device__ int start(int a, int b, int &t, int &ja, OrientTally &n) const
+    {
+        const int s0 = vtri[a];
+        if (s0 < 0) {
+            set_err(ct, GPUDT_ERR_ARG, 123);
+            return -1;
+        }
+        const double2 A = pos[a], B = pos[b];
+        int tt = dtri(s0), j = dori(s0), dir = 0;
+        for (int steps = 0; steps < kConsWalkMax; steps++) {
+            const int4 v = tv[tt];
+            const int p = geti(v, p1(j)), q = geti(v, m1(j));
+            if (p == b || q == b) return 0;
+            const int o1 = orient_staged(A, pos[p], B, ct, n), o2 = orient_staged(A, pos[q], B, ct, n);
+            if (o1 > 0 && o2 < 0) {
+                t = tt;
+                ja = j;
+                return 1;
+            }
+            if (o1 == 0) {
+                const double2 P = pos[p];
+                if ((P.x - A.x) * (B.x - A.x) + (P.y - A.y) * (B.y - A.y) > 0) {
+                    set_err(ct, GPUDT_ERR_ARG, 120);  // p lies on the segment
+                    return -1;
+                }
+            }
+            const int4 nb = tn[tt];
+            const int e = dir == 0 ? geti(nb, p1(j)) : geti(nb, m1(j));
+            if (e < 0) {
+                if (dir == 1) break;
+                dir = 1;
+                tt = dtri(s0);
+                j = dori(s0);
+                continue;
+            }
+            tt = dtri(e);
+            j = dir == 0 ? p1(dori(e)) : m1(dori(e));
+            if (enc(tt, j) == s0) break;
+        }
+        set_err(ct, GPUDT_ERR_TOPOLOGY, 122);
+        return -1;
+    }
+};
+
+__device__ __forceinline__ int index_of(const int4 &v, int x) { return v.x == x ? 0 : (v.y == x ? 1 : 2); }
+
+// Round step 1: walk, count the crossed triangles, claim them and their
+// neighbours.  size[k] = the record size of the constraint (0 when inserted).
+struct ConsClaim {
+    ConsWalker w;
+    const int2 *cons;
+    const unsigned long long *hash;
+    unsigned mask;
+    int *done, *size, *vote;
+    int m;
+    __device__ void operator()(long long kk) const
+    {
+        const int k = (int)kk;
+        size[k] = 0;
+        if (done[k]) return;
+        const int a = cons[k].x, b = cons[k].y;
+        OrientTally n;
+        int t, ja;
+        const int st = w.start(a, b, t, ja, n);
+        if (st <= 0) {
+            if (st == 0) done[k] = 1;
+            n.flush(w.ct);
+            return;
+        }
+        int p = geti(w.tv[t], p1(ja)), q = geti(w.tv[t], m1(ja)), jt = ja, cnt = 1;
+        const double2 A = w.pos[a], B = w.pos[b];
+        for (;;) {
+            atomicMin(&vote[t], k);
+            const int4 nb = w.tn[t];
+            if (nb.x >= 0) atomicMin(&vote[dtri(nb.x)], k);
+            if (nb.y >= 0) atomicMin(&vote[dtri(nb.y)], k);
+            if (nb.z >= 0) atomicMin(&vote[dtri(nb.z)], k);
+            const int e = geti(nb, jt);
+            if (e < 0 || cnt > kConsWalkMax) {
+                set_err(w.ct, GPUDT_ERR_TOPOLOGY, 124);
+                break;
+            }
+            if (cons_has(hash, mask, p, q)) {
+                set_err(w.ct, GPUDT_ERR_ARG, 130);  // crosses another constraint
+                break;
+            }
+            const int u = dtri(e);
+            const int4 uv = w.tv[u];
+            const int r = geti(uv, dori(e));
+            cnt++;
+            if (r == b) {
+                atomicMin(&vote[u], k);
+                const int4 un = w.tn[u];
+                if (un.x >= 0) atomicMin(&vote[dtri(un.x)], k);
+                if (un.y >= 0) atomicMin(&vote[dtri(un.y)], k);
+                if (un.z >= 0) atomicMin(&vote[dtri(un.z)], k);
+                break;
+            }
+            const int o = orient_staged(A, B, w.pos[r], w.ct, n);
+            if (o == 0) {
+                set_err(w.ct, GPUDT_ERR_ARG, 121);  // r lies on the segment
+                break;
+            }
+            if (o > 0) {
+                jt = index_of(uv, q);
+                q = r;
+            } else {
+                jt = index_of(uv, p);
+                p = r;
+            }
+            t = u;
+        }
+        n.flush(w.ct);
+        // slots (cnt), two chains (cnt + 2 each) with their edge links, the
+        // vertices inside the region (fewer than cnt) and the
+        // re-triangulation stack (4 ints per level)
+        size[k] = 12 * (cnt + 4);
+        atomicAdd(&w.ct->changed, 1);
+    }
+};
+
+// Round step 2: a constraint that holds all its claims records its walk at
+// rec = pool + off[k]: [0] crossed triangles n, [1] right chain length nr,
+// [2] left chain length nl, [3] unused, then slots[n], right chain[nr],
+// right links[nr - 1], left chain[nl], left links[nl - 1] (chain i: vertices
+// in order from a to b; link i: the neighbour across chain edge i), room for
+// the inner vertices and the stack of step 3.
+struct ConsRecord {
+    ConsWalker w;
+    const int2 *cons;
+    const int *done, *size, *off, *vote;
+    int *win, *pool;
+    long long pool_ints;
+    __device__ bool mine(int t, int k) const
+    {
+        if (vote[t] != k) return false;
+        const int4 nb = w.tn[t];
+        return (nb.x < 0 || vote[dtri(nb.x)] == k) && (nb.y < 0 || vote[dtri(nb.y)] == k) &&
+               (nb.z < 0 || vote[dtri(nb.z)] == k);
+    }
+    __device__ void operator()(long long kk) const
+    {
+        const int k = (int)kk;
+        win[k] = 0;
+        if (done[k] || size[k] == 0) return;
+        if ((long long)off[k] + size[k] > pool_ints) {
+            set_err(w.ct, GPUDT_ERR_NOMEM, 125);
+            return;
+        }
+        const int a = cons[k].x, b = cons[k].y;
+        OrientTally n;
+        int t, ja;
+        if (w.start(a, b, t, ja, n) <= 0) {
+            n.flush(w.ct);
+            return;
+        }
+        const int cap = size[k] / 12 - 4;  // crossed triangles the record holds
+        int *rec = pool + off[k];
+        int *slots = rec + 4;
+        int *R = slots + cap, *RL = R + cap + 2, *L = RL + cap + 1, *LL = L + cap + 2;
+        const double2 A = w.pos[a], B = w.pos[b];
+        bool ok = mine(t, k);
+        int4 tv0 = w.tv[t];
+        int p = geti(tv0, p1(ja)), q = geti(tv0, m1(ja)), jt = ja, cnt = 0, nr = 0, nl = 0;
+        const int4 tn0 = w.tn[t];
+        slots[cnt++] = t;
+        R[nr] = a;
+        RL[nr++] = geti(tn0, m1(ja));  // edge (a, p), opposite q
+        R[nr] = p;
+        L[nl] = a;
+        LL[nl++] = geti(tn0, p1(ja));  // edge (q, a), opposite p
+        L[nl] = q;
+        for (;;) {
+            const int e = geti(w.tn[t], jt);
+            const int u = dtri(e);
+            if (e < 0 || cnt >= cap) {
+                set_err(w.ct, GPUDT_ERR_TOPOLOGY, 126);
+                ok = false;
+                break;
+            }
+            const int4 uv = w.tv[u], un = w.tn[u];
+            const int r = geti(uv, dori(e));
+            ok = ok && mine(u, k);
+            slots[cnt++] = u;
+            if (r == b) {
+                RL[nr++] = geti(un, index_of(uv, q));  // edge (p, b), opposite q
+                R[nr] = b;
+                LL[nl++] = geti(un, index_of(uv, p));  // edge (q, b), opposite p
+                L[nl] = b;
+                break;
+            }
+            const int o = orient_staged(A, B, w.pos[r], w.ct, n);
+            if (o > 0) {  // r left: the boundary edge (q, r) is opposite p
+                LL[nl++] = geti(un, index_of(uv, p));
+                L[nl] = r;
+                jt = index_of(uv, q);
+                q = r;
+            } else {  // r right: the boundary edge (p, r) is opposite q
+                RL[nr++] = geti(un, index_of(uv, q));
+                R[nr] = r;
+                jt = index_of(uv, p);
+                p = r;
+            }
+            t = u;
+        }
+        n.flush(w.ct);
+        rec[0] = cnt;
+        rec[1] = nr + 1;
+        rec[2] = nl + 1;
+        win[k] = ok ? 1 : 0;
+    }
+};
+
+// Links edge ei of triangle t to the encoded neighbour o and o back to it.
+__device__ __forceinline__ void cons_link(int4 *tn, int t, int ei, int o)
+{
+    set_link(tn, enc(t, ei), o);
+    if (o >= 0) set_link(tn, o, enc(t, ei));
+}
+
+// Removes the dangling trees from a chain in place: a vertex whose whole star
+// is crossed lies inside the region of the crossed triangles, and the walk
+// passes round the edges to it in both directions (u, x, u).  Those vertices
+// go to orph[]; the remaining chain is the simple boundary of the region on
+// its side, and its links all lead to triangles outside it.  Returns the new
+// chain length.
+__device__ __forceinline__ int cons_reduce(int *c, int *cl, int len, int *orph, int &no)
+{
+    int top = 0;  // c[0..top] kept, cl[0..top) their links
+    for (int i = 1; i < len; i++) {
+        if (top >= 1 && c[top - 1] == c[i]) {
+            orph[no++] = c[top];  // (c[top-1], c[top]) and back: a spike
+            top--;
+        } else {
+            cl[top] = cl[i - 1];
+            c[++top] = c[i];
+        }
+    }
+    return top + 1;
+}
+
+// Round step 3: re-triangulate a winner's cavities.  Chain c[0..len) with
+// links cl[0..len-1) forms a counterclockwise polygon closed by the base edge
+// (c[len-1], c[0]); each sub-polygon (i, j) becomes the triangle
+// (c[i], c[x], c[j]) whose circle holds no other c[i+1..j-1], plus its two
+// sub-polygons.  Triangle edges: 0 = (c[x], c[j]), 1 = the base (c[j], c[i]),
+// 2 = (c[i], c[x]).  The vertices taken off the chains as dangling trees are
+// then put back, each by splitting the new triangle that holds it (or the two
+// on either side of the new edge through it); the slots of the crossed
+// triangles hold exactly the result.  The flip stage restores the Delaunay
+// property around them.
+struct ConsApply {
+    int4 *tv, *tn;
+    const double2 *pos;
+    int *vtri, *done;
+    const int *win, *off, *size;
+    int *pool;
+    Counters *ct;
+    __device__ int cavity(const int *c, const int *cl, int len, const int *slots, int &next, int *stack,
+                          int nstack) const
+    {
+        int sp = 0, root = -1;
+        stack[0] = 0;
+        stack[1] = len - 1;
+        stack[2] = -1;
+        stack[3] = -1;
+        sp = 1;
+        while (sp > 0) {
+            sp--;
+            const int i = stack[4 * sp], j = stack[4 * sp + 1], pt = stack[4 * sp + 2], pe = stack[4 * sp + 3];
+            int x = i + 1;
+            const double2 I = pos[c[i]], J = pos[c[j]];
+            for (int l = i + 2; l < j; l++) {
+                const double2 X = pos[c[x]], Lp = pos[c[l]];
+                double pa[2] = {I.x, I.y}, pb[2] = {X.x, X.y}, pc[2] = {J.x, J.y}, pd[2] = {Lp.x, Lp.y};
+                int s = incircle_filter32(pa, pb, pc, pd);
+                if (s == 2) s = incircle_filter(pa, pb, pc, pd);
+                if (s == 2) {
+                    atomicAdd(&ct->exact_incircle, 1ull);
+                    s = incircle_exact(pa, pb, pc, pd);
+                    if (s == EXACT_OVERFLOW) {
+                        set_err(ct, GPUDT_ERR_EXACT, 127);
+                        return -1;
+                    }
+                }
+                if (s > 0) x = l;
+            }
+            const int T = slots[next++];
+            tv[T] = make_int4(c[i], c[x], c[j], 0);
+            vtri[c[i]] = enc(T, 0);
+            vtri[c[x]] = enc(T, 1);
+            vtri[c[j]] = enc(T, 2);
+            if (pt >= 0) cons_link(tn, T, 1, enc(pt, pe));
+            else root = T;
+            if (x == i + 1) cons_link(tn, T, 2, cl[i]);
+            else if (sp < nstack) {
+                stack[4 * sp] = i;
+                stack[4 * sp + 1] = x;
+                stack[4 * sp + 2] = T;
+                stack[4 * sp + 3] = 2;
+                sp++;
+            } else {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 128);
+                return -1;
+            }
+            if (j == x + 1) cons_link(tn, T, 0, cl[x]);
+            else if (sp < nstack) {
+                stack[4 * sp] = x;
+                stack[4 * sp + 1] = j;
+                stack[4 * sp + 2] = T;
+                stack[4 * sp + 3] = 0;
+                sp++;
+            } else {
+                set_err(ct, GPUDT_ERR_TOPOLOGY, 128);
+                return -1;
+            }
+        }
+        return root;
+    }
+    // Writes triangle T = (a, b, c) with the links (na, nb, nc) of its edges
+    // opposite a, b, c; `ext` bit i: link i leads outside the triangles being
+    // written, so its far side is pointed back at T.
+    __device__ void put(int T, int a, int b, int c, int na, int nb, int nc, int ext) const
+    {
+        tv[T] = make_int4(a, b, c, 0);
+        tn[T] = make_int4(na, nb, nc, 0);
+        if ((ext & 1) && na >= 0) set_link(tn, na, enc(T, 0));
+        if ((ext & 2) && nb >= 0) set_link(tn, nb, enc(T, 1));
+        if ((ext & 4) && nc >= 0) set_link(tn, nc, enc(T, 2));
+        vtri[a] = enc(T, 0);
+        vtri[b] = enc(T, 1);
+        vtri[c] = enc(T, 2);
+    }
+    // Puts vertex v back into the triangles slots[0..next): a 1-3 split of the
+    // one that holds it, or a 2-4 split of the two beside the edge through it.
+    __device__ bool orphan(int v, const int *slots, int &next, OrientTally &n) const
+    {
+        const double2 V = pos[v];
+        for (int k = 0; k < next; k++) {
+            const int T = slots[k];
+            const int4 t = tv[T];
+            const double2 P0 = pos[t.x], P1 = pos[t.y], P2 = pos[t.z];
+            const int s0 = orient_staged(P1, P2, V, ct, n);
+            if (s0 < 0) continue;
+            const int s1 = orient_staged(P2, P0, V, ct, n);
+            if (s1 < 0) continue;
+            const int s2 = orient_staged(P0, P1, V, ct, n);
+            if (s2 < 0) continue;
+            const int4 nb = tn[T];
+            if (s0 > 0 && s1 > 0 && s2 > 0) {
+                const int B = slots[next++], C = slots[next++];
+                put(T, v, t.y, t.z, nb.x, enc(B, 2), enc(C, 1), 0);
+                put(B, v, t.z, t.x, nb.y, enc(C, 2), enc(T, 1), 1);
+                put(C, v, t.x, t.y, nb.z, enc(T, 2), enc(B, 1), 1);
+                return true;
+            }
+            if ((s0 == 0) + (s1 == 0) + (s2 == 0) != 1) break;
+            // v on the edge opposite corner i of T = (a, b, c): U = (u, c, b)
+            const int i = s0 == 0 ? 0 : (s1 == 0 ? 1 : 2);
+            const int a = geti(t, i), b = geti(t, p1(i)), c = geti(t, m1(i));
+            const int na = geti(nb, i), nbb = geti(nb, p1(i)), nc = geti(nb, m1(i));
+            if (na < 0) break;
+            const int U = dtri(na), j = dori(na);
+            bool ours = false;  // the edge through v is one of the new ones
+            for (int q = 0; q < next && !ours; q++) ours = slots[q] == U;
+            if (!ours) break;
+            const int4 uv = tv[U], un = tn[U];
+            const int u = geti(uv, j), ub = geti(un, p1(j)), uc = geti(un, m1(j));
+            const int T2 = slots[next++], U2 = slots[next++];
+            put(T, a, b, v, enc(U2, 0), enc(T2, 2), nc, 4);
+            put(T2, a, v, c, enc(U, 0), nbb, enc(T, 1), 2);
+            put(U, u, c, v, enc(T2, 0), enc(U2, 2), uc, 4);
+            put(U2, u, v, b, enc(T, 0), ub, enc(U, 1), 2);
+            return true;
+        }
+        set_err(ct, GPUDT_ERR_TOPOLOGY, 131);
+        return false;
+    }
+    __device__ void operator()(long long kk) const
+    {
+        const int k = (int)kk;
+        if (!win[k]) return;
+        int *rec = pool + off[k];
+        const int cnt = rec[0];
+        int nr = rec[1], nl = rec[2];
+        const int cap = size[k] / 12 - 4;
+        const int *slots = rec + 4;
+        int *R = (int *)slots + cap, *RL = R + cap + 2;
+        int *L = RL + cap + 1, *LL = L + cap + 2;
+        int *orph = LL + cap + 1;
+        int *stack = orph + cap;
+        const int nstack = (size[k] - (int)(stack - rec)) / 4;
+        if (nr + nl - 4 != cnt || nr > cap + 2 || nl > cap + 2) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 129);
+            return;
+        }
+        int no = 0;
+        nr = cons_reduce(R, RL, nr, orph, no);
+        nl = cons_reduce(L, LL, nl, orph, no);
+        if (nr < 3 || nl < 3 || nr + nl - 4 + 2 * no != cnt) {
+            set_err(ct, GPUDT_ERR_TOPOLOGY, 132);
+            return;
+        }
+        // the left chain, reversed (b ... a), is counterclockwise like the right one
+        for (int i = 0, j = nl - 1; i < j; i++, j--) {
+            const int x = L[i];
+            L[i] = L[j];
+            L[j] = x;
+        }
+        for (int i = 0, j = nl - 2; i < j; i++, j--) {
+            const int x = LL[i];
+            LL[i] = LL[j];
+            LL[j] = x;
+        }
+        int next = 0;
+        const int rr = cavity(R, RL, nr, slots, next, stack, nstack);
+        if (rr < 0) return;
+        const int rl = cavity(L, LL, nl, slots, next, stack, nstack);
+        if (rl < 0) return;
+        cons_link(tn, rr, 1, enc(rl, 1));  // the constraint: base of both roots
+        OrientTally n;
+        for (int o = 0; o < no; o++)
+            if (!orphan(orph[o], slots, next, n)) break;
+        n.flush(ct);
+        done[k] = 1;
+    }
+};
+
+struct ConsMap {
+    const int2 *in;
+    const int *iperm;  // input -> internal id (null: identity)
+    int2 *cons;
+    int *done;
+    __device__ void operator()(long long k) const
+    {
+        int2 c = in[k];
+        if (iperm) c = make_int2(iperm[c.x], iperm[c.y]);
+        cons[k] = c;
+        done[k] = 0;
+    }
+};
+
+struct InvPerm {
+    const int *perm;
+    int *iperm;
+    __device__ void operator()(long long i) const { iperm[perm[i]] = (int)i; }
+};
+
+struct VtriOfTris {
+    const int4 *tv;
+    int *vtri;
+    __device__ void operator()(long long t) const
+    {
+        const int4 v = tv[t];
+        if (v.x < 0) return;
+        vtri[v.x] = enc((int)t, 0);
+        vtri[v.y] = enc((int)t, 1);
+        vtri[v.z] = enc((int)t, 2);
+    }
+};
+
+struct ConsHashInsert {
+    const int2 *cons;
+    unsigned long long *h;
+    unsigned mask;
+    __device__ void operator()(long long k) const
+    {
+        const unsigned long long key = cons_key(cons[k].x, cons[k].y);
+        for (unsigned s = cons_slot(key, mask), n = 0; n <= mask; s = (s + 1) & mask, n++) {
+            const unsigned long long old = atomicCAS(&h[s], ~0ull, key);
+            if (old == ~0ull || old == key) return;
+        }
+    }
+};
+
+int stage_constraints(Ctx &c)
+{
+    const int m = c.n_cons;
+    c.chash = nullptr;
+    c.cons_rounds = 0;
+    if (m <= 0) return GPUDT_OK;
+    unsigned S = 64;
+    while (S < 2u * (unsigned)m + 2u) S <<= 1;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t need = al(sizeof(int2) * (size_t)m) * 2 + al(4 * (size_t)(m + 1)) * 4 + al(8 * (size_t)S) +
+                        al(4 * (size_t)c.N + 4);
+    if (need > c.cons_bytes) {
+        if (c.cons_buf) cudaFree(c.cons_buf);
+        c.cons_buf = nullptr;
+        c.cons_bytes = 0;
+        GALPHA_CUDA(cudaMalloc(&c.cons_buf, need));
+        c.cons_bytes = need;
+    }
+    char *p = c.cons_buf;
+    auto take = [&](size_t b) {
+        char *q = p;
+        p += al(b);
+        return q;
+    };
+    int2 *in = (int2 *)take(sizeof(int2) * (size_t)m);
+    int2 *cons = (int2 *)take(sizeof(int2) * (size_t)m);
+    int *done = (int *)take(4 * (size_t)(m + 1));
+    int *size = (int *)take(4 * (size_t)(m + 1));
+    int *off = (int *)take(4 * (size_t)(m + 1));
+    int *win = (int *)take(4 * (size_t)(m + 1));
+    unsigned long long *hash = (unsigned long long *)take(8 * (size_t)S);
+    int *iperm = (int *)take(4 * (size_t)c.N + 4);
+    GALPHA_CUDA(cudaMemcpyAsync(in, c.h_cons, sizeof(int2) * (size_t)m, cudaMemcpyHostToDevice, c.stream));
+    if (c.renumbered) launch_n(c, InvPerm{c.perm, iperm}, c.N);
+    launch_n(c, ConsMap{in, c.renumbered ? iperm : nullptr, cons, done}, m);
+    GALPHA_CUDA(cudaMemsetAsync(hash, 0xff, 8 * (size_t)S, c.stream));
+    launch_n(c, ConsHashInsert{cons, hash, S - 1}, m);
+    // one incident triangle per vertex of the mesh (vertices not in it: -1)
+    int r = read_counters(c);
+    if (r) return r;
+    const int nt = c.hctr->ntris;
+    GALPHA_CUDA(cudaMemsetAsync(c.vtri, 0xff, sizeof(int) * (size_t)c.V, c.stream));
+    launch_n(c, VtriOfTris{c.tv, c.vtri}, nt);
+    const ConsWalker w{c.tv, c.tn, c.pos, c.vtri, c.ctr};
+    int round = 0;
+    for (;; round++) {
+        if (round > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
+        GALPHA_CUDA(cudaMemsetAsync(c.vote, 0x7f, sizeof(int) * (size_t)c.cap_tris, c.stream));
+        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+        launch_n(c, ConsClaim{w, cons, hash, S - 1, done, size, c.vote, m}, m);
+        r = exclusive_scan_int(c, size, off, m, &c.ctr->nlist);
+        if (r) return r;
+        r = read_counters(c);
+        if (r) return r;
+        if (c.hctr->err) return c.hctr->err;
+        if (c.hctr->changed == 0) break;
+        const long long total = (long long)(unsigned)c.hctr->nlist;
+        if (total > c.cons_pool_ints) {
+            if (c.cons_pool) cudaFree(c.cons_pool);
+            c.cons_pool = nullptr;
+            c.cons_pool_ints = 0;
+            const long long ints = std::max(total + total / 2, 1ll << 16);
+            GALPHA_CUDA(cudaMalloc(&c.cons_pool, sizeof(int) * (size_t)ints));
+            c.cons_pool_ints = ints;
+        }
+        launch_n(c, ConsRecord{w, cons, done, size, off, c.vote, win, c.cons_pool, c.cons_pool_ints}, m);
+        launch_n(c, ConsApply{c.tv, c.tn, c.pos, c.vtri, done, win, off, size, c.cons_pool, c.ctr}, m);
+        GALPHA_CUDA(cudaGetLastError());
+    }
+    c.chash = hash;
+    c.cmask = S - 1;
+    c.cons_rounds = round;
     return GPUDT_OK;
 }
 

@@ -180,6 +180,17 @@ struct Ctx {
     int round_counter = 1;    // ids of operation rounds (per handle: stamps live in its arena)
     int host_reads = 0;       // device -> host reads (each a stream synchronisation) of the current call
 
+    // constrained edges of the current call (GPUDTPARAMS.nConstraints > 0)
+    int n_cons = 0;
+    const int *h_cons = nullptr;       // host pairs of input indices
+    char *cons_buf = nullptr;          // own allocation: constraint state + hash set
+    size_t cons_bytes = 0;
+    int *cons_pool = nullptr;          // own allocation: per-round walk records
+    long long cons_pool_ints = 0;
+    const unsigned long long *chash = nullptr;  // set of constrained vertex pairs (internal ids), or null
+    unsigned cmask = 0;                // its size - 1 (a power of two)
+    int cons_rounds = 0;               // insertion rounds of the last call
+
     // failure-detection limits (galphaSetLimits): the round cap of every
     // iterative stage, the spin bound of the single-pass look-back waits, and
     // a test switch under which tile 0 of each look-back kernel withholds its
@@ -368,6 +379,7 @@ int stage_shift(Ctx &c);
 int stage_missing(Ctx &c);
 int stage_boundary(Ctx &c);
 int stage_flip(Ctx &c);
+int stage_constraints(Ctx &c);
 int stage_compact(Ctx &c);
 // ------------------------------------------------------------------ batches
 // One point set of a batch: its grid scaling, its texture cell and its

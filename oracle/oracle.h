@@ -23,6 +23,12 @@ extern "C" {
  * Returns the triangle count or a negative ORACLE_ERR_*. */
 int oracle_dt(int npts, const double *xy, int cap, int *out_vtx, int *out_nbr, int *out_nkept);
 
+/* Constrained Delaunay triangulation: cons holds ncons pairs of point
+ * indices (non-crossing segments through no other point).  Same outputs as
+ * oracle_dt; every constraint is an edge, every other edge locally Delaunay. */
+int oracle_cdt(int npts, const double *xy, int ncons, const int *cons, int cap, int *out_vtx, int *out_nbr,
+               int *out_nkept);
+
 /* Validates a mesh; out[6]: link errors, non-CCW, non-Delaunay edges, hull
  * edges, non-convex hull edges, bad indices. */
 int oracle_check_mesh(int npts, const double *xy, int ntri, const int *vtx, const int *nbr, long long *out);

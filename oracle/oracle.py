@@ -51,7 +51,9 @@ def lib():
             build()
         L = ctypes.CDLL(_LIB)
         L.oracle_dt.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip]
+        L.oracle_cdt.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip, _ip, _ip]
         L.oracle_dt.restype = ctypes.c_int
+        L.oracle_cdt.restype = ctypes.c_int
         L.oracle_orient2d.argtypes = [_dp, _dp, _dp]
         L.oracle_incircle.argtypes = [_dp, _dp, _dp, _dp]
         L.oracle_exact_counts.argtypes = [ctypes.c_int]
@@ -86,6 +88,22 @@ def dt(points):
     nt = lib().oracle_dt(n, _d(pts), cap, _i(vtx), _i(nbr), _i(kept))
     if nt < 0:
         raise RuntimeError("oracle_dt failed with status %d" % nt)
+    return vtx[:nt].copy(), nbr[:nt].copy(), int(kept[0])
+
+
+def cdt(points, constraints):
+    """Exact constrained DT (oracle_cdt).  constraints: (M, 2) point indices.
+    Returns (vtx[T,3] int32, nbr[T,3] int32, n_distinct)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    cons = np.ascontiguousarray(constraints, dtype=np.int32).reshape(-1, 2)
+    n = pts.shape[0]
+    cap = max(2 * n, 8)
+    vtx = np.empty((cap, 3), dtype=np.int32)
+    nbr = np.empty((cap, 3), dtype=np.int32)
+    kept = np.zeros(1, dtype=np.int32)
+    nt = lib().oracle_cdt(n, _d(pts), cons.shape[0], _i(cons), cap, _i(vtx), _i(nbr), _i(kept))
+    if nt < 0:
+        raise RuntimeError("oracle_cdt failed with status %d" % nt)
     return vtx[:nt].copy(), nbr[:nt].copy(), int(kept[0])
 
 
