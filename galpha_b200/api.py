@@ -77,6 +77,7 @@ class Status(ctypes.Structure):
         ("ms", ctypes.c_float * 12),
         ("kernelMs", ctypes.c_float * 4),
         ("sortKeys", ctypes.c_longlong), ("sortPasses", ctypes.c_int), ("hostReads", ctypes.c_int),
+        ("constraintRounds", ctypes.c_int), ("reserved0", ctypes.c_int),
     ]
 
     def as_dict(self):

@@ -2713,6 +2713,7 @@ int stage_constraints(Ctx &c)
     c.chash = hash;
     c.cmask = S - 1;
     c.cons_rounds = round;
+    c.st.constraintRounds = round;
     return GPUDT_OK;
 }
 

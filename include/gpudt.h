@@ -22,9 +22,12 @@
  *     of them valid, counterclockwise, vtx[] are input indices; tri[i] =
  *     (t << 2) | j is the neighbour across the edge opposite vtx[i], -1 on the hull;
  *   - exact duplicates are dropped (the lowest input index survives);
- *   - nConstraints must be 0 (constrained edges are outside this engine).
+ *   - constraints[0..2*nConstraints) are pairs of input indices that become
+ *     edges of the result, which is then the constrained Delaunay triangulation
+ *     (gpudt.cpp:860 cudaConstraint).
  * Differences from the reference: errors are returned, not exit(-1); tmp[3]
- * is zero-filled instead of internal chain garbage.
+ * is zero-filled instead of internal chain garbage; constraints that cross
+ * each other or pass through a point are GPUDT_ERR_ARG (undefined there).
  */
 #ifndef GALPHA_GPUDT_H
 #define GALPHA_GPUDT_H
@@ -101,6 +104,8 @@ typedef struct {
     int sortPasses;          /* radix passes it took (8-bit digits) */
     int hostReads;           /* device -> host reads of the call, each one stream synchronisation
                                 (the host reads work-list sizes between stages) */
+    int constraintRounds;    /* segment-insertion rounds (0 without constraints) */
+    int reserved0;
 } gpudtStatus;
 
 #ifdef __cplusplus

@@ -171,6 +171,7 @@ def test_gpu_cdt_matches_oracle(engine, n, kind, seed):
     dt = engine.triangulate(G.GPUDTParams(pts, fboSize=1024 if n <= 5000 else 2048, constraints=cons))
     rep = check_cdt(pts, dt.vtx, dt.tri, cons)
     assert rep == dict(links=0, ccw=0, missing=0, non_delaunay_free=0), rep
+    assert 1 <= dt.status.constraintRounds < len(cons), dt.status.constraintRounds
     ov, _, _ = O.cdt(pts, cons)
     assert canon_set(dt.vtx) == canon_set(ov)
     # the alpha stage runs on the constrained mesh as on any triangulation
