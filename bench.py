@@ -6,10 +6,12 @@ FP64), discrete Voronoi texture 8192^2.  One step = one full Delaunay
 triangulation + alpha spectrum with per-simplex intervals.
 
   value  device-resident: points already in HBM, results left in HBM
-         (galphaRunDevice), timed with CUDA events on the engine's stream.
-  e2e    the same through the public host API (galphaTriangulate +
-         galphaComputeResident): pinned host points in, triangles and all alpha
-         arrays back to host memory, inside the timed region.
+         (galphaRunDevice, the gpudtTriangle records built too), timed with
+         CUDA events on the engine's stream.
+  e2e    the same through the public host API (galphaComputeAll): pinned
+         host points in, triangles and all alpha arrays back to host memory,
+         inside the timed region.
+The master list (compute_master_list) is timed on its own beside them.
 
 Between timed steps a 512 MiB buffer is written (L2 flush); the step's own
 working set (~3.5 GB) is far larger than L2 as well.
@@ -56,7 +58,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched (c4) and serving (c5) legs")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="arrival window of the serving leg")
     return ap.parse_args()
 
 
@@ -397,7 +399,7 @@ def main():
     L = G.load()
 
     def step():
-        return eng.run_device(d_xy.data_ptr(), n, bounds, fbo, True)
+        return eng.run_device(d_xy.data_ptr(), n, bounds, fbo, True, triangles=True)
 
     for _ in range(a.warmup):
         step()
@@ -424,6 +426,8 @@ def main():
                                              "nRepairTiles", "nEscalated",
                                              "nFlips", "flipRounds", "shiftRounds", "missingRounds", "hostReads")}
         stats["predicates"] = predicate_stages(st)
+        stats["hostReadsStage"] = dict(zip(["voronoi", "triangles", "shift", "missing", "boundary", "flip", "compact",
+                                            "alpha"], list(st.hostReadsStage)[1:9]))
     torch.cuda.synchronize()
     launches = L.galphaLaunchCount() - launches0
     clk = clocks.stop()
@@ -492,6 +496,16 @@ def main():
                      "ideal_ms": b_alg / (peak * 1e9) * 1e3},
     }
 
+    # the master list (Alpha_Shapes_2D::compute_master_list, part of the
+    # reference's computeAlphaShapes) on the same resident input: its own
+    # stage time, reported beside the step (the step and e2e leave it out, as
+    # the CPU arms do)
+    master_ms = []
+    for _ in range(3):
+        stm = eng.run_device_flags(d_xy.data_ptr(), n, bounds, fbo, 2 | 4)
+        master_ms.append(float(stm.ms[11]))
+    torch.cuda.synchronize()
+
     # end to end through the host API
     e2e = None
     if not a.no_e2e:
@@ -546,6 +560,7 @@ def main():
             "kernels_ms": {"vd_tri": row_ms, "column_pass": col_ms,
                            "emit": sum(k[2] for k in kernels) / len(kernels), "spectrum_sort": sort_ms},
             "counts": {"triangles": nt, "edges": ne, "spectrum": ns},
+            "master_list_ms": sum(master_ms) / len(master_ms),
             "pipeline_stats": stats,
             "batched": batched,
             "serving": serving,

@@ -78,12 +78,14 @@ class Status(ctypes.Structure):
         ("kernelMs", ctypes.c_float * 4),
         ("sortKeys", ctypes.c_longlong), ("sortPasses", ctypes.c_int), ("hostReads", ctypes.c_int),
         ("constraintRounds", ctypes.c_int), ("reserved0", ctypes.c_int),
+        ("hostReadsStage", ctypes.c_int * 12),
     ]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("ms", "kernelMs")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("ms", "kernelMs", "hostReadsStage")}
         d["ms"] = list(self.ms)
         d["kernelMs"] = list(self.kernelMs)
+        d["hostReadsStage"] = list(self.hostReadsStage)
         return d
 
 
@@ -401,12 +403,25 @@ class Engine:
                "galphaCompute")
         return self._alpha_result(out, bufs, copy)
 
-    def run_device(self, d_xy_ptr, n, bounds, fbo_size, with_alpha=True):
-        """Hot path on device-resident points (d_xy_ptr: device address of 2n doubles)."""
+    def run_device(self, d_xy_ptr, n, bounds, fbo_size, with_alpha=True, triangles=False):
+        """Hot path on device-resident points (d_xy_ptr: device address of 2n doubles).
+        ``triangles``: also build the gpudtTriangle records on the device."""
+        return self.run_device_flags(d_xy_ptr, n, bounds, fbo_size, (1 if with_alpha else 0) | (4 if triangles else 0))
+
+    def resident_triangles(self):
+        """The resident triangles as a TRIANGLE_DTYPE array (galphaCopyTriangles)."""
+        nt, _, _ = self.counts()
+        out = np.empty(nt, TRIANGLE_DTYPE)
+        _check(self._L.galphaCopyTriangles(self._h, out.ctypes.data if nt else None, nt), "galphaCopyTriangles")
+        return out
+
+    def run_device_flags(self, d_xy_ptr, n, bounds, fbo_size, flags):
+        """galphaRunDevice with its flag word: flags & 3 = 0 (DT only), 1 (+ alpha),
+        2 (+ alpha + master list); flags & 4: build the gpudtTriangle records."""
         self._batch_active = False
         st = Status()
         _check(self._L.galphaRunDevice(self._h, ctypes.c_void_p(d_xy_ptr), n, bounds[0], bounds[1], bounds[2],
-                                       bounds[3], fbo_size, 1 if with_alpha else 0, ctypes.byref(st)),
+                                       bounds[3], fbo_size, flags, ctypes.byref(st)),
                "galphaRunDevice")
         self._npoints = n
         return st

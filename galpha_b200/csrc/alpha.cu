@@ -769,15 +769,15 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     GALPHA_CUDA(cudaMemsetAsync(c.keys, 0, sizeof(unsigned long long), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vals, 0, sizeof(int), c.stream));
     launch_n(c, TriKeys{c.cv, c.cn, alpha_geom_tris(c), c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
-    r = read_counters(c);
-    if (r) return r;
-    if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
-    if (c.hctr->nlist2 > 0) launch_n(c, SliverKeys{alpha_geom_tris(c), c.opos, c.list, c.keys, c.ctr}, c.hctr->nlist2);
+    // the sliver list's length stays on the device; TriKeys' errors are read
+    // with the spectrum length below
+    launch_dev(c, SliverKeys{alpha_geom_tris(c), c.opos, c.list, c.keys, c.ctr}, &c.ctr->nlist2, nT);
     r = exclusive_scan_int(c, unatt, spos, nE, &c.ctr->nlist);
     if (r) return r;
     launch_n(c, EdgeKeys{c.edges, alpha_geom_tris(c), c.opos, unatt, spos, c.keys, c.vals, 1 + nT, nT}, nE);
     r = read_counters(c);
     if (r) return r;
+    if (c.hctr->err) return stage_fail(c, c.hctr->err, "alpha");
     const int nIn = 1 + nT + c.hctr->nlist;
     c.nSpecIn = nIn;
     c.sort_passes = 0;

@@ -229,6 +229,7 @@ static int ensure_sizes(HandleState &H, const Sizes &z)
 
 static void ev_record(Ctx &c, int k)
 {
+    c.reads_at[k] = c.host_reads;
     if (c.events) cudaEventRecord(c.ev[k], c.stream);
 }
 
@@ -410,6 +411,7 @@ static void fill_times(Ctx &c, int last)
     for (int k = 1; k < last; k++) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, c.ev[k], c.ev[k + 1]) == cudaSuccess && k < 12) c.st.ms[k] = ms;
+        if (k < 12) c.st.hostReadsStage[k] = c.reads_at[k + 1] - c.reads_at[k];
     }
     float tot = 0.f;
     if (cudaEventElapsedTime(&tot, c.ev[0], c.ev[last]) == cudaSuccess) c.st.ms[GALPHA_STAGE_TOTAL] = tot;
@@ -605,19 +607,24 @@ int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, doub
     Ctx &c = h->H.c;
     cudaSetDevice(c.device);
     cudaGetLastError();  // clear an error left by unrelated runtime calls
+    const int level = withAlpha & 3;
     ev_record(c, 0);
     int r = run_dt(h->H, d_xy, n, minX, minY, maxX, maxY, fboSize);
-    if (!r && withAlpha) {
+    if (!r && (withAlpha & GALPHA_RUN_TRIANGLES)) {
+        r = ensure_outtri(c);  // the gpudtTriangle records, timed with the compaction
+        ev_record(c, 8);
+    }
+    if (!r && level) {
         ev_record(c, 8);
         r = stage_alpha(c);
         if (!r) c.have_alpha = true;
         ev_record(c, 9);
-        if (!r && withAlpha >= 2) {
+        if (!r && level >= 2) {
             r = master_list(c);
             ev_record(c, 10);
         }
         if (!r) fill_times(c, 9);
-        if (!r && withAlpha >= 2 && c.events) {
+        if (!r && level >= 2 && c.events) {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, c.ev[9], c.ev[10]) == cudaSuccess) c.st.ms[GALPHA_STAGE_MASTER] = ms;
             if (cudaEventElapsedTime(&ms, c.ev[0], c.ev[10]) == cudaSuccess) c.st.ms[GALPHA_STAGE_TOTAL] = ms;

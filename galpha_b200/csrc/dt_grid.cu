@@ -412,7 +412,8 @@ int stage_setup(Ctx &c, const double *d_xy, int n, double minX, double minY, dou
     if (c.renumbered) {
         unsigned *k1 = (unsigned *)c.keys, *k2 = (unsigned *)c.keys2;
         launch_n(c, SpatialKeys{d_xy, k1, c.perm, c.scale, c.shiftX, c.shiftY, T - 2 * kMargin}, n);
-        int r = radix_sort32(c, k1, c.perm, k2, c.vals2, n, c.rhist);
+        // pixel coordinates below T: Morton codes of 2 logT bits
+        int r = radix_sort32(c, k1, c.perm, k2, c.vals2, n, c.rhist, 2 * c.logT);
         if (r) return r;
     }
     SetupSites s;

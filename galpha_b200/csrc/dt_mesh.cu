@@ -123,6 +123,17 @@ __device__ __forceinline__ int alloc_slot(int *freelist, Counters *ct, int cap)
     return s;
 }
 
+// After a round of allocations: a free-list count driven below zero by pops
+// that fell through to the tail is reset, so that a later free_slot appends
+// at index 0.
+struct ClampFree {
+    Counters *ct;
+    __device__ void operator()(long long) const
+    {
+        if (ct->nfree < 0) ct->nfree = 0;
+    }
+};
+
 __device__ __forceinline__ void free_slot(int4 *tv, int *freelist, Counters *ct, int t)
 {
     tv[t] = make_int4(-1, -1, -1, 0);
@@ -437,17 +448,22 @@ struct ShiftCheckFans {
 };
 
 // Takes the listed vertices out of the candidate set and appends them to the
-// list of all dropped vertices.
+// list of all dropped vertices (its order is immaterial: the priority rounds
+// decide by vertex priority, not by list position).
 struct ShiftDropList {
     const int *list;
     int8_t *cand;
-    int *drop, *all;
+    int *drop, *all, *total;
+    int cap;
+    Counters *ct;
     __device__ void operator()(long long i) const
     {
         const int v = list[i];
         drop[v] = 0;
         cand[v] = 0;
-        all[i] = v;
+        const int k = atomicAdd(total, 1);
+        if (k < cap) all[k] = v;
+        else set_err(ct, GPUDT_ERR_TOPOLOGY, 42);
     }
 };
 
@@ -649,92 +665,106 @@ struct CountState {
     }
 };
 
-static int run_counts(Ctx &c) { return read_counters(c); }
+// Rounds of the shifting loops run in groups of kShiftGroup between counter
+// reads: list lengths stay on the device (launch_dev), each round's count is
+// kept in ct->grp[], and a round after the loop's last one does nothing (an
+// empty list, or no site left in the state it acts on), so running past the
+// end of a loop changes no result.
+constexpr int kShiftGroup = 4;
 
 int stage_shift(Ctx &c)
 {
     int r;
     int shiftRounds = 0, badCount = 0;
     int *dropped = c.aux2;  // every site the optimistic phase dropped: the only undecided ones after it
-    int ndropped = 0;
     {
-        r = read_counters(c);
-        if (r) return r;
-        int nt = c.hctr->ntris;
         // candidate flags (bytes) and per-iteration drop flags (ints) share list2
         int8_t *cand = (int8_t *)c.list2;
         int *drop = c.list2 + ((c.V + 1023) >> 2) + 256;
         int *lists[2] = {c.list, c.aux};  // vertices dropped in an iteration (ping-pong)
         launch_n(c, ShiftCandidates{c.vstate, cand}, c.V);
         GALPHA_CUDA(cudaMemsetAsync(drop, 0, sizeof(int) * (size_t)c.V, c.stream));
-        int nprev = 0;
+        GALPHA_CUDA(cudaMemsetAsync(c.ctr->sh_n, 0, 3 * sizeof(int), c.stream));  // sh_n[2], sh_total
         bool settled = false;
-        for (int it = 0; it < c.max_rounds; it++) {
-            int *cur = lists[it & 1], *prev = lists[(it + 1) & 1];
-            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
-            if (it == 0)
-                launch_n(c, ShiftCheckTris{c.tv, c.pos, c.opos, cand, drop, cur, &c.ctr->nlist2, c.ctr}, nt);
-            else
-                launch_n(c, ShiftCheckFans{c.tv, c.tn, c.vtri, c.pos, c.opos, cand, prev, drop, cur, &c.ctr->nlist2,
-                                           c.ctr},
-                         nprev);
+        for (int it = 0; !settled;) {
+            for (int j = 0; j < kShiftGroup; j++, it++) {
+                int *cur = lists[it & 1], *prev = lists[(it + 1) & 1];
+                int *curn = &c.ctr->sh_n[it & 1], *prevn = &c.ctr->sh_n[(it + 1) & 1];
+                GALPHA_CUDA(cudaMemsetAsync(curn, 0, sizeof(int), c.stream));
+                if (it == 0)
+                    launch_dev(c, ShiftCheckTris{c.tv, c.pos, c.opos, cand, drop, cur, curn, c.ctr}, &c.ctr->ntris,
+                               c.cap_tris);
+                else
+                    launch_dev(c, ShiftCheckFans{c.tv, c.tn, c.vtri, c.pos, c.opos, cand, prev, drop, cur, curn,
+                                                 c.ctr},
+                               prevn, c.V);
+                launch_dev(c, ShiftDropList{cur, cand, drop, dropped, &c.ctr->sh_total, c.N, c.ctr}, curn, c.V);
+                launch_n(c, CopyElems<int>{&c.ctr->grp[j], curn}, 1);
+            }
             r = read_counters(c);
             if (r) return r;
             if (c.hctr->err) return c.hctr->err;
-            shiftRounds++;
-            const int nd = c.hctr->nlist2;
-            if (nd == 0) {
-                settled = true;
-                break;
+            for (int j = 0; j < kShiftGroup && !settled; j++) {
+                shiftRounds++;
+                settled = c.hctr->grp[j] == 0;
             }
-            if ((long long)ndropped + nd > c.N) return GPUDT_ERR_TOPOLOGY;
-            launch_n(c, ShiftDropList{cur, cand, drop, dropped + ndropped}, nd);
-            ndropped += nd;
-            nprev = nd;
+            if (!settled && shiftRounds >= c.max_rounds) return GPUDT_ERR_NOCONVERGE;
         }
-        if (!settled) return GPUDT_ERR_NOCONVERGE;
         launch_n(c, ShiftCommit{cand, c.pos, c.opos, c.vstate, c.vround}, c.V);
     }
     // vertices fixed from the start (fake ring) and the optimistic set count
     // as decided in the first shifting round (id 1); the rest go through
     // priority rounds
-    for (int round = 2;; round++) {
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, 2 * sizeof(int) + 0, c.stream));
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-        launch_n(c, ShiftRoundList{ShiftRound{c.tv, c.tn, c.pos, c.opos, c.vstate, c.vround, c.vtri, round, c.ctr},
-                                   dropped},
-                 ndropped);
-        r = run_counts(c);
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+    for (int round = 2, done = 0; !done;) {
+        for (int j = 0; j < kShiftGroup; j++, round++) {
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+            launch_dev(c,
+                       ShiftRoundList{ShiftRound{c.tv, c.tn, c.pos, c.opos, c.vstate, c.vround, c.vtri, round, c.ctr},
+                                      dropped},
+                       &c.ctr->sh_total, c.N);
+            launch_n(c, CopyElems<int>{&c.ctr->grp[j], &c.ctr->nlist}, 1);
+        }
+        r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        shiftRounds++;
-        badCount += c.hctr->changed;
-        if (c.hctr->nlist == 0) break;
-        if (shiftRounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
+        for (int j = 0; j < kShiftGroup && !done; j++) {
+            shiftRounds++;
+            done = c.hctr->grp[j] == 0;
+        }
+        if (!done && shiftRounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
+    badCount = c.hctr->changed;
     c.st.shiftRounds = shiftRounds;
     c.st.nBadShift = badCount;
     // remove the unshiftable sites in independent rounds
     int guard = 0;
+    const long long recn = 4LL * c.cap_tris;
     while (badCount > 0) {
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-        launch_n(c, BadSelectList{BadSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.ctr}, dropped}, ndropped);
-        r = run_counts(c);
-        if (r) return r;
-        int nsel = c.hctr->nlist;
-        if (nsel == 0) break;
-        int round = next_round(c);
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
-        launch_n(c, BadRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.anchor, c.list, c.pos, c.vstate,
-                              c.rec, round, c.N, c.ctr},
-                 nsel);
-        r = run_counts(c);
+        for (int j = 0; j < kShiftGroup; j++) {
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
+            launch_dev(c, BadSelectList{BadSelect{c.tv, c.tn, c.vstate, c.vtri, c.list, c.ctr}, dropped},
+                       &c.ctr->sh_total, c.N);
+            launch_n(c, CopyElems<int>{&c.ctr->grp[j], &c.ctr->nlist}, 1);
+            const int round = next_round(c);
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
+            launch_dev(c, BadRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.anchor, c.list, c.pos,
+                                    c.vstate, c.rec, round, c.N, c.ctr},
+                       &c.ctr->nlist, c.N);
+            launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
+        }
+        GALPHA_CUDA(cudaGetLastError());
+        r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        r = run_relink(c, round, c.hctr->nrec);
-        if (r) return r;
-        badCount -= nsel;
-        if (++guard > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
+        bool stuck = false;
+        for (int j = 0; j < kShiftGroup && !stuck; j++) {
+            stuck = c.hctr->grp[j] == 0;
+            badCount -= c.hctr->grp[j];
+        }
+        if (stuck) break;
+        guard += kShiftGroup;
+        if (guard > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
     }
     return GPUDT_OK;
 }
@@ -902,6 +932,7 @@ struct MissingInsert {
         if (k == 2) {
             vstate[p] = VS_DUP;
             atomicAdd(&ct->changed, 1);
+            atomicAdd(&ct->ndup, 1);
             return;
         }
         if (vote[t] != p) return;
@@ -1019,40 +1050,46 @@ int stage_missing(Ctx &c)
     c.st.nMissing = nmiss;
     if (nmiss == 0) return GPUDT_OK;
     int *loc = c.aux, *kind = c.aux2 + 0;
-    // aux2 holds kind at [0, nmiss) ; edge tags in list2
+    // aux2 holds kind at [0, nmiss) ; edge tags in list2.  Rounds run in
+    // groups of kMissingGroup between counter reads (a round after the last
+    // insertion finds no missing site and does nothing); each round's
+    // insertions are kept in ct->grp[].
+    constexpr int kMissingGroup = 2;
+    const long long recn = 4LL * c.cap_tris;
     int rounds = 0, remaining = nmiss, dups = 0;
+    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ndup, 0, sizeof(int), c.stream));
     while (remaining > 0) {
-        int round = next_round(c);
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
-        GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-        launch_n(c, MissingLocate{c.tv, c.tn, c.pos, c.opos, c.vtri, c.anchor, c.vstate, c.list, loc, kind, c.vote,
-                                  c.N, c.ctr},
-                 nmiss);
-        launch_n(c, EdgeTags{c.tn, loc, kind, c.list2, c.ctr}, nmiss);
-        launch_n(c, MissingInsert{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.vote, c.pos, c.opos, c.vstate,
-                                  c.list, loc, kind, c.rec, round, c.cap_tris, c.ctr},
-                 nmiss);
+        for (int j = 0; j < kMissingGroup; j++) {
+            int round = next_round(c);
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
+            GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
+            launch_n(c, MissingLocate{c.tv, c.tn, c.pos, c.opos, c.vtri, c.anchor, c.vstate, c.list, loc, kind,
+                                      c.vote, c.N, c.ctr},
+                     nmiss);
+            launch_n(c, EdgeTags{c.tn, loc, kind, c.list2, c.ctr}, nmiss);
+            launch_n(c, MissingInsert{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.vote, c.pos, c.opos,
+                                      c.vstate, c.list, loc, kind, c.rec, round, c.cap_tris, c.ctr},
+                     nmiss);
+            launch_n(c, ClampFree{c.ctr}, 1);  // a pop past the free list took tail slots
+            launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
+            launch_n(c, ResetVotes{c.vote, c.tn, loc, kind}, nmiss);
+            launch_dev(c, ResetVotesEdge{c.vote, c.list2}, &c.ctr->nlist2, c.cap_tris);
+            launch_n(c, CopyElems<int>{&c.ctr->grp[j], &c.ctr->changed}, 1);
+        }
+        GALPHA_CUDA(cudaGetLastError());
         r = read_counters(c);
         if (r) return r;
         if (c.hctr->err) return c.hctr->err;
-        if (c.hctr->nfree < 0) GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nfree, 0, sizeof(int), c.stream));
         if (c.hctr->ntris > c.cap_tris) return GPUDT_ERR_NOMEM;
-        r = run_relink(c, round, c.hctr->nrec);
-        if (r) return r;
-        launch_n(c, ResetVotes{c.vote, c.tn, loc, kind}, nmiss);
-        launch_n(c, ResetVotesEdge{c.vote, c.list2}, c.hctr->nlist2);
-        int done = c.hctr->changed;
-        remaining -= done;
-        rounds++;
-        if (done == 0 || rounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
+        for (int j = 0; j < kMissingGroup && remaining > 0; j++) {
+            const int done = c.hctr->grp[j];
+            remaining -= done;
+            rounds++;
+            if (done == 0 || rounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
+        }
     }
-    // count drops
-    GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist, 0, sizeof(int), c.stream));
-    launch_n(c, CountState{c.vstate, VS_DUP, nullptr, c.ctr}, c.N);
-    r = read_counters(c);
-    if (r) return r;
-    dups = c.hctr->nlist;
+    dups = c.hctr->ndup;
     c.st.nDuplicates = dups;
     c.st.missingRounds = rounds;
     return GPUDT_OK;

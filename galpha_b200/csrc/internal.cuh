@@ -71,6 +71,10 @@ struct Counters {
     int runstage;    // fake runs: staged fan entries
     int nlong;       // key sort: out-of-order pairs recorded in groups too long for one thread
     int nhuge;       // alpha ranks: runs too long for one block, listed for the multi-block merge
+    int sh_n[2];     // shift: sites dropped by the current / previous optimistic iteration
+    int sh_total;    // shift: all dropped sites listed so far
+    int grp[8];      // per-round counts of a group of rounds run between two counter reads
+    int ndup;        // missing sites found to be exact duplicates
 };
 
 // Relink record: an edge of a triangle created this round (loc = (t<<2)|i, or -1
@@ -170,6 +174,7 @@ struct Ctx {
 
     // events for stage timing
     cudaEvent_t ev[GALPHA_STAGE_TOTAL + 2];
+    int reads_at[GALPHA_STAGE_TOTAL + 2] = {};  // host_reads when event k was recorded
     cudaEvent_t kev[10];  // [2k, 2k+1] bracket single kernel k (see gpudtStatus.kernelMs)
     bool kev_rec[10];     // recorded during the current call
     bool events = false;
@@ -481,7 +486,8 @@ int launch_column_pass_cells(Ctx &c, int T, int W2, int cells, const uint32_t *o
 // LSD radix sort of (keys, vals) ascending (sort.cu)
 int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *keys2, int *vals2, int n,
                bool *in_second);
-int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch);
+int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch,
+                 int key_bits = 0);
 // Stable sort by the low nbits of 32-bit set ids, moving (keys, vals) along;
 // the result ends in (skey, keys, vals).
 int radix_sort_set_kv(Ctx &c, unsigned *skey, unsigned *skey2, unsigned long long *keys, int *vals,

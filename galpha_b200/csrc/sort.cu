@@ -169,9 +169,11 @@ long long radix_scratch_ints(long long n)
 // Sorts (keys, vals)[0..n) ascending (stable) on the key bits from min_shift
 // up; result in keys/vals.  Uses keys2/vals2 and `scratch`
 // (radix_scratch_ints(n) ints).
+// key_bits > 0: the keys are known to fit in key_bits bits, and every digit
+// below that is sorted without first reading which bits vary.
 template <typename K>
 static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int n, int *scratch, int min_shift = 0,
-                           bool *in_second = nullptr)
+                           bool *in_second = nullptr, int key_bits = 0)
 {
     if (in_second) *in_second = false;
     if (n <= 1) return GPUDT_OK;
@@ -188,18 +190,21 @@ static int radix_sort_keys(Ctx &c, K *keys, int *vals, K *keys2, int *vals2, int
             if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
         }
     }
-    K *acc = reinterpret_cast<K *>(scratch);
-    launch_n(c, CopyElems<K>{acc, keys}, 1);
-    GALPHA_CUDA(cudaMemsetAsync(acc + 1, 0, sizeof(K), c.stream));
-    {
+    unsigned long long varying;
+    if (key_bits > 0) {
+        varying = key_bits >= 64 ? ~0ull : (1ull << key_bits) - 1ull;
+    } else {
+        K *acc = reinterpret_cast<K *>(scratch);
+        launch_n(c, CopyElems<K>{acc, keys}, 1);
+        GALPHA_CUDA(cudaMemsetAsync(acc + 1, 0, sizeof(K), c.stream));
         long long blocks = std::min<long long>((n + 255) / 256, (long long)c.sm_count * 4);
         k_or_xor<K><<<(unsigned)blocks, 256, 0, c.stream>>>(keys, n, acc);
         count_launch();
+        K hv[2];
+        int rr = read_small(c, hv, acc, sizeof(hv));
+        if (rr) return rr;
+        varying = (unsigned long long)hv[1];
     }
-    K hv[2];
-    int rr = read_small(c, hv, acc, sizeof(hv));
-    if (rr) return rr;
-    const unsigned long long varying = (unsigned long long)hv[1];
     const int nblocks = (n + kRsTile - 1) / kRsTile;
     int *hist = scratch + 8;
     K *ki = keys, *ko = keys2;
@@ -742,9 +747,10 @@ int radix_sort(Ctx &c, unsigned long long *keys, int *vals, unsigned long long *
     return GPUDT_OK;
 }
 
-int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch)
+int radix_sort32(Ctx &c, unsigned int *keys, int *vals, unsigned int *keys2, int *vals2, int n, int *scratch,
+                 int key_bits)
 {
-    return radix_sort_keys<unsigned int>(c, keys, vals, keys2, vals2, n, scratch);
+    return radix_sort_keys<unsigned int>(c, keys, vals, keys2, vals2, n, scratch, 0, nullptr, key_bits);
 }
 
 }  // namespace galpha

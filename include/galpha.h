@@ -102,9 +102,12 @@ int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt,
 int galphaCompute(galphaHandle h, const GPUDTPARAMS *params, const GPUDTOUTPUT *dt, GAlphaOutput *out);
 
 /* Device-resident hot path: points already in device memory (d_xy: 2*n doubles).
- * Runs DT (+ alpha when withAlpha; + the master list when withAlpha = 2) and
- * leaves every result on the device.
+ * Runs DT (+ alpha when withAlpha & 3 is 1; + the master list when it is 2) and
+ * leaves every result on the device.  With GALPHA_RUN_TRIANGLES set in
+ * withAlpha the gpudtTriangle records are built on the device too (otherwise
+ * they are built by the first call that copies them out).
  * Returns the status; counts through galphaGetCounts. */
+#define GALPHA_RUN_TRIANGLES 4
 int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, double minY,
                     double maxX, double maxY, int fboSize, int withAlpha, gpudtStatus *st);
 

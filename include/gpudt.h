@@ -106,6 +106,7 @@ typedef struct {
                                 (the host reads work-list sizes between stages) */
     int constraintRounds;    /* segment-insertion rounds (0 without constraints) */
     int reserved0;
+    int hostReadsStage[12];  /* hostReads per stage, indexed like ms[] */
 } gpudtStatus;
 
 #ifdef __cplusplus

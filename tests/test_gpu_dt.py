@@ -218,3 +218,20 @@ def test_c1_through_reference_symbol_matches_handle(engine):
     a = G.gpudt_compute_dt(G.GPUDTParams(pts, fboSize=fbo))
     b = run(engine, pts, fbo)
     assert canon_set(a.vtx) == canon_set(b.vtx)
+
+
+@pytest.mark.parametrize("flags", [0, 4, 1 | 4, 2 | 4])
+def test_run_device_flags(engine, flags):
+    """galphaRunDevice on device-resident points: the gpudtTriangle records
+    (built inside the call with GALPHA_RUN_TRIANGLES = 4, else on the copy)
+    equal the oracle's triangulation."""
+    import torch
+
+    pts = D.uniform_points(50000, 77)
+    d = torch.from_numpy(pts).cuda()
+    engine.run_device_flags(d.data_ptr(), len(pts), (0.0, 0.0, 1.0, 1.0), 1024, flags)
+    tri = engine.resident_triangles()
+    vtx = tri["vtx"].reshape(-1, 3)
+    assert canon_set(vtx) == canon_set(O.dt(pts)[0])
+    ok, rep = compare_dt(pts, vtx, tri["tri"].reshape(-1, 3))
+    assert ok and rep["identical"], rep

@@ -45,6 +45,16 @@ def test_master_list_duplicates_and_lattice(engine):
     assert (ml[:74]["st"] == 2).all()
 
 
+def test_master_list_large_tie_runs(engine):
+    """A 256 x 256 lattice of dyadic spacing: every square's two triangles
+    share one exact circumradius, so ranks repeat over tens of thousands of
+    entries (runs sorted as sub-arrays), next to the short runs of a uniform
+    patch."""
+    g = np.stack(np.meshgrid(np.arange(256) / 256.0, np.arange(256) / 256.0), -1).reshape(-1, 2)
+    pts = np.concatenate([g * 0.5, 0.5 + 0.5 * D.uniform_points(20000, 12)])
+    _check(engine, pts, 2048)
+
+
 def test_master_list_tiny(engine):
     _check(engine, np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]), 256)
 
