@@ -13,13 +13,15 @@
 //
 // The keys are dense (one per spectrum rank), so the stable sort is a
 // counting sort: count the entries of every key, scan the counts into run
-// starts, drop each entry into its run by an atomic cursor, then put every
-// run back in entry order (runs are a few entries long: an insertion sort per
-// run; the rare long runs -- exact ties on lattices, dropped duplicates -- are
-// radix-sorted as sub-arrays).  The spectrum pointers are the run starts.
-// That is one read of the ranks per pass instead of four full passes of an
-// LSD sort.  Keys outside [0, nSpec] (a batch's segmented ranks) take the LSD
-// sort of the whole list instead.
+// starts, move each entry into its run (two levels, see k_ml_partition /
+// k_ml_place), then put every run back in entry order (runs are a few entries
+// long: an insertion sort per run; the rare long runs -- exact ties on
+// lattices, dropped duplicates -- are radix-sorted as sub-arrays).  The
+// spectrum pointers are the run starts.  Keys outside [0, nSpec] (a batch's
+// segmented ranks) take an LSD sort of the whole list instead.
+#include <algorithm>
+#include <mutex>
+
 #include "internal.cuh"
 
 namespace galpha {
@@ -146,60 +148,120 @@ struct MasterCount {
     }
 };
 
-// Entry k goes to the next free place of its run; cur[K] starts at the run's
-// start and ends at the next run's start.
-struct MasterPlace {
-    const int2 *pt;
-    const int *edge_ro;
-    const int2 *edge_nu;
-    const int *tri_ro;
-    int *cur, *slot;
-    int N, nE, nK;
-    __device__ void operator()(long long ii) const
-    {
-        const int k = (int)ii;
-        const int r = master_rank(k, pt, edge_ro, edge_nu, tri_ro, N, nE);
-        if (r == 0) return;
-        const int K = r + 1;
-        if (K < 0 || K >= nK) return;
-        slot[atomicAdd(&cur[K], 1)] = k;
-    }
+// Two-level placement.  Ranks are grouped into buckets of kBucket
+// consecutive keys; a bucket's entries occupy one contiguous range of the
+// list (its runs' starts come from the count scan).  k_ml_partition moves
+// every entry (key, index) into its bucket's range, a tile at a time (block
+// histogram, one reservation per bucket and tile), and k_ml_place then
+// places one bucket per block in shared memory, puts every run of it in
+// entry order and writes the bucket out in one coalesced pass.  The random
+// part of the permutation thus happens in shared memory, not as scattered
+// 4-byte stores to HBM.
+constexpr int kBucketBits = 13, kBucket = 1 << kBucketBits;
+constexpr int kPartTile = 8192, kPartThreads = 256;
+constexpr int kMaxBuckets = 4096;
+constexpr int kPlaceCap = 40960, kPlaceThreads = 512;  // entries of a bucket placed in shared memory
+
+struct BucketCursors {
+    const int *start;
+    int *gcur;
+    int nK;
+    __device__ void operator()(long long b) const { gcur[b] = start[min((long long)nK, b * kBucket)]; }
 };
 
-// Run K is slot[end[K-1] .. end[K]) (end[-1] = 0): short runs are put in entry
-// order here; long ones are listed (begin, end) for a sub-array sort.
-// nonempty[K] marks the runs that exist (their starts are the spectrum
-// pointers).
-struct MasterRuns {
-    const int *end;
-    int *slot, *nonempty, *longs;
-    int nK;
-    Counters *ct;
-    __device__ void operator()(long long ii) const
-    {
-        const int K = (int)ii;
-        const int b = K == 0 ? 0 : end[K - 1], e = end[K];
-        nonempty[K] = e > b ? 1 : 0;
-        if (e - b <= 1) return;
-        if (e - b > kMaxShortRun) {
-            const int q = atomicAdd(&ct->nlong, 1);
-            if (q < kMaxLongRuns) {
-                longs[2 * q] = b;
-                longs[2 * q + 1] = e;
-            }
-            return;
+__global__ void __launch_bounds__(kPartThreads) k_ml_partition(const int2 *__restrict__ pt,
+                                                               const int *__restrict__ edge_ro,
+                                                               const int2 *__restrict__ edge_nu,
+                                                               const int *__restrict__ tri_ro, int N, int nE,
+                                                               long long M, int nK, int nb, int *gcur, int2 *P)
+{
+    extern __shared__ int ml_part[];
+    int *Ks = ml_part, *loc = Ks + kPartTile, *h = loc + kPartTile, *gb = h + nb;
+    const long long t0 = (long long)blockIdx.x * kPartTile;
+    for (int i = threadIdx.x; i < nb; i += kPartThreads) h[i] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPartTile; i += kPartThreads) {
+        const long long k = t0 + i;
+        int K = -1;
+        if (k < M) {
+            const int r = master_rank((int)k, pt, edge_ro, edge_nu, tri_ro, N, nE);
+            if (r != 0 && r + 1 >= 0 && r + 1 < nK) K = r + 1;
         }
-        for (int i = b + 1; i < e; i++) {
-            const int x = slot[i];
-            int j = i - 1;
-            while (j >= b && slot[j] > x) {
-                slot[j + 1] = slot[j];
-                j--;
-            }
-            slot[j + 1] = x;
+        Ks[i] = K;
+        if (K >= 0) loc[i] = atomicAdd(&h[K >> kBucketBits], 1);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += kPartThreads)
+        if (h[b]) gb[b] = atomicAdd(&gcur[b], h[b]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPartTile; i += kPartThreads) {
+        const int K = Ks[i];
+        if (K >= 0) P[gb[K >> kBucketBits] + loc[i]] = make_int2(K, (int)(t0 + i));
+    }
+}
+
+// Puts run [bgn, end) of a (shared or global) array in entry order, or lists
+// it for a sub-array sort when it is longer than kMaxShortRun.
+__device__ __forceinline__ void ml_order_run(int *a, int bgn, int end, int gofs, int *longs, Counters *ct)
+{
+    if (end - bgn <= 1) return;
+    if (end - bgn > kMaxShortRun) {
+        const int q = atomicAdd(&ct->nlong, 1);
+        if (q < kMaxLongRuns) {
+            longs[2 * q] = gofs + bgn;
+            longs[2 * q + 1] = gofs + end;
+        }
+        return;
+    }
+    for (int i = bgn + 1; i < end; i++) {
+        const int x = a[i];
+        int j = i - 1;
+        while (j >= bgn && a[j] > x) {
+            a[j + 1] = a[j];
+            j--;
+        }
+        a[j + 1] = x;
+    }
+}
+
+__global__ void __launch_bounds__(kPlaceThreads) k_ml_place(const int2 *__restrict__ P, const int *__restrict__ start,
+                                                            int nK, int *slot, int *nonempty, int *gcurK,
+                                                            int *longs, Counters *ct)
+{
+    extern __shared__ int ml_place[];
+    int *cur = ml_place, *out = cur + kBucket;
+    const int K0 = blockIdx.x * kBucket, K1 = min(K0 + kBucket, nK);
+    const int s0 = start[K0], n = start[K1] - s0;
+    if (n <= kPlaceCap) {
+        for (int j = threadIdx.x; j < K1 - K0; j += kPlaceThreads) cur[j] = start[K0 + j] - s0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kPlaceThreads) {
+            const int2 e = P[s0 + i];
+            out[atomicAdd(&cur[e.x - K0], 1)] = e.y;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < K1 - K0; j += kPlaceThreads) {
+            const int bgn = start[K0 + j] - s0, end = cur[j];
+            nonempty[K0 + j] = end > bgn ? 1 : 0;
+            ml_order_run(out, bgn, end, s0, longs, ct);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kPlaceThreads) slot[s0 + i] = out[i];
+    } else {  // a bucket too large for shared memory: the same steps in HBM
+        for (int j = threadIdx.x; j < K1 - K0; j += kPlaceThreads) gcurK[K0 + j] = start[K0 + j];
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kPlaceThreads) {
+            const int2 e = P[s0 + i];
+            slot[atomicAdd(&gcurK[e.x], 1)] = e.y;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < K1 - K0; j += kPlaceThreads) {
+            const int bgn = start[K0 + j], end = gcurK[K0 + j];
+            nonempty[K0 + j] = end > bgn ? 1 : 0;
+            ml_order_run(slot, bgn, end, 0, longs, ct);
         }
     }
-};
+}
 
 struct MasterDecode {
     const int *slot;
@@ -209,13 +271,13 @@ struct MasterDecode {
 };
 
 struct RunPointers {
-    const int *end, *nonempty, *pos;
+    const int *start, *nonempty, *pos;
     int *sp;
     __device__ void operator()(long long ii) const
     {
         const int K = (int)ii;
         if (K == 0) sp[0] = -1;
-        if (nonempty[K]) sp[1 + pos[K]] = K == 0 ? 0 : end[K - 1];
+        if (nonempty[K]) sp[1 + pos[K]] = start[K];
     }
 };
 }  // namespace
@@ -278,13 +340,28 @@ int master_list(Ctx &c)
     const long long M = 2LL * c.N + 3LL * c.nE + c.nT_out;
     if (M > 0x7fffffffLL) return GPUDT_ERR_NOMEM;
     const long long nK = (long long)c.nSpec + 1;  // keys rank + 1 in [0, nSpec]
-    if (M == 0 || nK > 0x3fffffffLL) return master_list_radix(c);
-    // slot, sub-sort keys2 / vals / vals2 (int), cnt (run starts, then ends),
-    // nonempty, pos (int), long-run extents, out (12 B), sp (int), sort scratch
+    const long long nb = (nK + kBucket - 1) / kBucket;
+    if (M == 0 || nb > kMaxBuckets) return master_list_radix(c);
+    {
+        static std::mutex mu;
+        static bool attr_set[64];
+        std::lock_guard<std::mutex> lk(mu);
+        if (c.device < 0 || c.device >= 64 || !attr_set[c.device]) {
+            GALPHA_CUDA(cudaFuncSetAttribute(k_ml_partition, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(int) * (2 * kPartTile + 2 * kMaxBuckets)));
+            GALPHA_CUDA(cudaFuncSetAttribute(k_ml_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(int) * (kBucket + kPlaceCap)));
+            if (c.device >= 0 && c.device < 64) attr_set[c.device] = true;
+        }
+    }
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const long long scr = radix_scratch_ints(M);
-    const size_t need = al(4 * (size_t)M) * 4 + al(4 * (size_t)(nK + 1)) * 3 + al(8 * (size_t)kMaxLongRuns) +
-                        al(sizeof(galphaAlpha) * (size_t)M) + al(4 * (size_t)(nK + 2)) + al(4 * (size_t)scr);
+    // slot, P (2 ints per entry; later the sub-sorts' second keys and values),
+    // sval2 (int); start, nonempty, pos, gcurK (nK + 1 ints each); bucket
+    // cursors; long-run extents; out (12 B); sp; sort scratch
+    const size_t need = al(4 * (size_t)M) * 4 + al(4 * (size_t)(nK + 1)) * 4 + al(4 * (size_t)nb) +
+                        al(8 * (size_t)kMaxLongRuns) + al(sizeof(galphaAlpha) * (size_t)M) +
+                        al(4 * (size_t)(nK + 2)) + al(4 * (size_t)scr);
     if (need > c.ml_bytes) {
         if (c.ml_buf) cudaFree(c.ml_buf);
         c.ml_buf = nullptr;
@@ -299,31 +376,40 @@ int master_list(Ctx &c)
         return q;
     };
     int *slot = (int *)take(4 * (size_t)M);
-    int *skey2 = (int *)take(4 * (size_t)M);
-    int *sval = (int *)take(4 * (size_t)M);
+    int2 *P = (int2 *)take(8 * (size_t)M);
     int *sval2 = (int *)take(4 * (size_t)M);
-    int *cnt = (int *)take(4 * (size_t)(nK + 1));
+    int *start = (int *)take(4 * (size_t)(nK + 1));
     int *nonempty = (int *)take(4 * (size_t)(nK + 1));
     int *pos = (int *)take(4 * (size_t)(nK + 1));
+    int *gcurK = (int *)take(4 * (size_t)(nK + 1));
+    int *gcur = (int *)take(4 * (size_t)nb);
     int *longs = (int *)take(8 * (size_t)kMaxLongRuns);
     c.ml_out = (galphaAlpha *)take(sizeof(galphaAlpha) * (size_t)M);
     c.ml_sp = (int *)take(4 * (size_t)(nK + 2));
     int *scratch = (int *)take(4 * (size_t)scr);
 
-    GALPHA_CUDA(cudaMemsetAsync(cnt, 0, 4 * (size_t)(nK + 1), c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(start, 0, 4 * (size_t)(nK + 1), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlong, 0, sizeof(int), c.stream));
-    launch_n(c, MasterCount{c.pt_nu, c.edge_ro, c.edge_nu, c.tri_ro, cnt, c.N, c.nE, (int)nK, c.ctr}, M);
-    int r = exclusive_scan_int(c, cnt, cnt, (int)nK, &c.ctr->nlist);  // run starts; nlist = entries kept
+    launch_n(c, MasterCount{c.pt_nu, c.edge_ro, c.edge_nu, c.tri_ro, start, c.N, c.nE, (int)nK, c.ctr}, M);
+    // run starts (start[nK] = entries kept, also in nlist)
+    int r = exclusive_scan_int(c, start, start, (int)nK + 1, &c.ctr->nlist);
     if (r) return r;
-    launch_n(c, MasterPlace{c.pt_nu, c.edge_ro, c.edge_nu, c.tri_ro, cnt, slot, c.N, c.nE, (int)nK}, M);
-    launch_n(c, MasterRuns{cnt, slot, nonempty, longs, (int)nK, c.ctr}, nK);
+    launch_n(c, BucketCursors{start, gcur, (int)nK}, nb);
+    k_ml_partition<<<(unsigned)((M + kPartTile - 1) / kPartTile), kPartThreads,
+                     sizeof(int) * (2 * kPartTile + 2 * (size_t)nb), c.stream>>>(
+        c.pt_nu, c.edge_ro, c.edge_nu, c.tri_ro, c.N, c.nE, M, (int)nK, (int)nb, gcur, P);
+    count_launch();
+    k_ml_place<<<(unsigned)nb, kPlaceThreads, sizeof(int) * (kBucket + kPlaceCap), c.stream>>>(
+        P, start, (int)nK, slot, nonempty, gcurK, longs, c.ctr);
+    count_launch();
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
     if (r) return r;
     if (c.hctr->changed || c.hctr->nlong > kMaxLongRuns) return master_list_radix(c);
     const int nout = c.hctr->nlist, nlong = c.hctr->nlong;
     if (nlong > 0) {
+        int *skey2 = (int *)P, *sval = (int *)P + M;  // P is free after the placement
         int hl[2 * 64];
         for (int q0 = 0; q0 < nlong; q0 += 64) {  // the long runs' extents, 64 at a time
             const int qn = std::min(64, nlong - q0);
@@ -341,7 +427,7 @@ int master_list(Ctx &c)
     launch_n(c, MasterDecode{slot, c.ml_out, c.N, c.nE}, nout);
     r = exclusive_scan_int(c, nonempty, pos, (int)nK, &c.ctr->nlist2);
     if (r) return r;
-    launch_n(c, RunPointers{cnt, nonempty, pos, c.ml_sp}, nK);
+    launch_n(c, RunPointers{start, nonempty, pos, c.ml_sp}, nK);
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
     if (r) return r;
