@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched (c4) and serving (c5) legs")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default loop schedule")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="arrival window of the serving leg")
     return ap.parse_args()
 
@@ -192,7 +193,9 @@ def batched_leg(G, D, torch, stream, reps=3):
     from galpha_b200 import autotune
 
     tune_sets = D.c4_sets(seed=14)[:1024]
-    density, table = autotune.tune_batch_density(eng, tune_sets, bounds=G.Engine.batch_bounds(tune_sets))
+    tune_bounds = G.Engine.batch_bounds(tune_sets)
+    density, table = autotune.tune_batch_density(eng, tune_sets, bounds=tune_bounds)
+    sched, _ = autotune.tune_schedule(eng, lambda: eng.run_batch(tune_sets, bounds=tune_bounds), reps=2)
     st = eng.run_batch_device(d_xy.data_ptr(), sizes, bounds)  # warm-up (arena growth)
     torch.cuda.synchronize()
     ts = []
@@ -245,7 +248,7 @@ def batched_leg(G, D, torch, stream, reps=3):
         "value": value, "unit": UNIT, "ms_per_batch": ms, "gpu_launches": int(launches),
         "plain_per_set": {"value": plain, "unit": UNIT, "sets": len(sample), "points": npts, "ms": plain_ms},
         "speedup_vs_plain": value / plain,
-        "tuning": {"batch_density": density, "table_ms": table,
+        "tuning": {"batch_density": density, "table_ms": table, "schedule": sched,
                    "sample": "1024 sets of c4_sets(seed=14) (not the measured draw)"},
         "e2e": {"value": n / (min(te) / 1e3) / 1e6, "unit": UNIT, "ms": min(te), "h2d_bytes": int(xy.nbytes),
                 "d2h_bytes": int(d2h)},
@@ -293,8 +296,10 @@ def serving_leg(G, D, seconds, rate=2000.0, nslots=6):
 
     # texture density tuned on a batch of every 4th pool set, then set on every slot
     density, _ = autotune.tune_batch_density(slots[0], pool[::4], bounds=bounds[::4], reps=1)
+    sched, _ = autotune.tune_schedule(slots[0], lambda: slots[0].run_batch(pool[::4], bounds=bounds[::4]), reps=1)
     for e in slots[1:]:
         e.set_batch_density(density)
+        e.set_schedule(*(sched[k] for k in autotune.SCHEDULE_KEYS))
     reqs = [S.Request(i, t, pool[pick[i]], bounds=bounds[pick[i]]) for i, t in enumerate(arrivals)]
     srv = S.Server(slots, hbm_budget=120e9)
     # every slot grows its device arena and pinned staging buffers before the stream
@@ -307,12 +312,12 @@ def serving_leg(G, D, seconds, rate=2000.0, nslots=6):
     out["config"] = {"workload": "c5: Poisson %.0f req/s for %.1f s (of the 60 s stream), sizes log-uniform in "
                                  "[1000, 1048576], 50/50 uniform / Gaussian clusters, 3 quantile queries per request, "
                                  "120 GB admission budget" % (rate, seconds), "pool_sets": len(pool),
-                     "slots": nslots, "batch_density": density}
+                     "slots": nslots, "batch_density": density, "schedule": sched}
     out["offered_mpoints_per_s"] = float(sum(len(r.points) for r in reqs) / seconds / 1e6)
     return out
 
 
-def e2e_pipelined(G, params, n, steps, device, dist, world, nslots=6):
+def e2e_pipelined(G, params, n, steps, device, dist, world, nslots=6, schedule=None):
     """The same host-API call stream with several handles in flight (one host
     thread each): one call's uploads and downloads overlap the other's
     kernels.  Every call still uploads its points and downloads all of its
@@ -326,6 +331,8 @@ def e2e_pipelined(G, params, n, steps, device, dist, world, nslots=6):
     engines = [G.Engine(device=device) for _ in range(nslots)]
     try:
         for e in engines:
+            if schedule:
+                e.set_schedule(*(schedule[k] for k in G.Engine.SCHEDULE_KEYS))
             e.compute_all(params, copy=False)
         torch.cuda.synchronize()
         gate = threading.Barrier(nslots + 1)
@@ -401,6 +408,12 @@ def main():
     def step():
         return eng.run_device(d_xy.data_ptr(), n, bounds, fbo, True, triangles=True)
 
+    # loop schedule tuned on this workload before the warm-up (no result depends on it)
+    sched = None
+    if not a.no_tune:
+        from galpha_b200 import autotune
+
+        sched, _ = autotune.tune_schedule(eng, step, reps=3)
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
@@ -533,7 +546,7 @@ def main():
         e2e = {"value": world * n / (float(te.item()) / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": int(d2h), "ms_per_step": float(te.item()),
                "call": "galphaComputeAll (DT + alpha, pinned host buffers), one call at a time"}
-        e2e["pipelined"] = e2e_pipelined(G, params, n, a.steps, local, dist, world)
+        e2e["pipelined"] = e2e_pipelined(G, params, n, a.steps, local, dist, world, schedule=sched)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -560,6 +573,7 @@ def main():
             "kernels_ms": {"vd_tri": row_ms, "column_pass": col_ms,
                            "emit": sum(k[2] for k in kernels) / len(kernels), "spectrum_sort": sort_ms},
             "counts": {"triangles": nt, "edges": ne, "spectrum": ns},
+            "schedule": sched,
             "master_list_ms": sum(master_ms) / len(master_ms),
             "pipeline_stats": stats,
             "batched": batched,

@@ -171,6 +171,8 @@ def load(path=None):
     L.galphaRunBatchHost.argtypes = [vp, ip, vp, vp, vp, ip, ctypes.POINTER(Status)]
     L.galphaBatchSets.argtypes = [vp, vp]
     L.galphaSetBatchDensity.argtypes = [vp, ctypes.c_double]
+    L.galphaSetSchedule.argtypes = [vp, ip, ip, ip, ip, ip]
+    L.galphaGetSchedule.argtypes = [vp, ctypes.POINTER(ip)]
     L.galphaBatchCopy.argtypes = [vp, vp, vp, vp, vp, vp]
     L.galphaBatchQuery.argtypes = [vp, vp, ip, vp]
     L.galphaMasterList.argtypes = [vp, ctypes.POINTER(_MasterOut)]
@@ -484,6 +486,22 @@ class Engine:
         (galphaSetBatchDensity; default 10, tuned by galpha_b200.autotune)."""
         _check(self._L.galphaSetBatchDensity(self._h, float(pixels_per_point)), "galphaSetBatchDensity")
         self._density = float(pixels_per_point)
+
+    SCHEDULE_KEYS = ("shift_group", "missing_group", "flip_sync", "flip_tail_enter", "flip_tail_leave")
+
+    def set_schedule(self, shift_group=0, missing_group=0, flip_sync=0, flip_tail_enter=-1, flip_tail_leave=0):
+        """Loop schedule of later calls (galphaSetSchedule): rounds per counter
+        read of the shifting, missing-site and flip loops, and the flip-tail
+        hand-over lengths.  No value changes a result; 0 (-1 for
+        flip_tail_enter) keeps the default.  Tuned by galpha_b200.autotune."""
+        _check(self._L.galphaSetSchedule(self._h, int(shift_group), int(missing_group), int(flip_sync),
+                                         int(flip_tail_enter), int(flip_tail_leave)), "galphaSetSchedule")
+
+    def schedule(self):
+        """The schedule in force, as a dict (galphaGetSchedule)."""
+        out = (ctypes.c_int * 5)()
+        _check(self._L.galphaGetSchedule(self._h, out), "galphaGetSchedule")
+        return dict(zip(self.SCHEDULE_KEYS, list(out)))
 
     def batch_sets(self):
         k = self._batch[0]

@@ -1,6 +1,8 @@
-"""Autotuner for the batched pipeline: picks the texture density (pixels per
-point of each set's cell, galphaSetBatchDensity) that minimises the device
-time of a batch.
+"""Autotuner: picks the texture density of batches (pixels per point of each
+set's cell, galphaSetBatchDensity) and the loop schedule of a handle
+(galphaSetSchedule: rounds per counter read of the shifting, missing-site and
+flip loops, and the flip-tail hand-over lengths) that minimise the measured
+device time of a workload.
 
 Fewer pixels per point mean fewer pixels for the Voronoi colouring; more
 points then share a pixel and are inserted afterwards (missing sites), which
@@ -12,6 +14,17 @@ result does not depend on the density.
 
     best, table = tune_batch_density(engine, sample_sets)
     engine.set_batch_density(best)
+
+The schedule changes no result either (a round past the end of a loop does
+nothing; the in-block flip rounds run the launched rounds' functors); it
+trades counter reads, each a stream synchronisation, against rounds launched
+past a loop's end.  tune_schedule walks the five parameters one at a time
+(coordinate descent over SCHEDULE_CANDIDATES), timing `run()` -- any callable
+that runs the workload on the engine and returns its gpudtStatus -- by the
+median device time of `reps` runs, and moves off the value in force only for
+a gain above `min_gain`:
+
+    sched, table = tune_schedule(engine, lambda: engine.run_batch(sets))
 """
 import json
 
@@ -36,6 +49,54 @@ def tune_batch_density(engine, sets, bounds=None, candidates=DEFAULT_CANDIDATES,
     best = min(table, key=lambda t: (t[1], t[0]))[0]
     engine.set_batch_density(best)
     return best, table
+
+
+SCHEDULE_KEYS = ("shift_group", "missing_group", "flip_sync", "flip_tail_enter", "flip_tail_leave")
+SCHEDULE_CANDIDATES = {
+    "shift_group": (1, 2, 4, 8),
+    "missing_group": (1, 2, 4),
+    "flip_sync": (2, 4, 8, 16),
+    "flip_tail_enter": (0, 1024, 4096, 16384),
+    "flip_tail_leave": (8192, 32768, 131072),
+}
+
+
+def _valid(s):
+    return s["flip_tail_leave"] >= s["flip_tail_enter"]
+
+
+def tune_schedule(engine, run, candidates=None, reps=3, min_gain=0.01):
+    """Returns (best schedule dict, [(schedule, median device ms), ...]) and
+    leaves the engine set to the best schedule."""
+    cand = dict(SCHEDULE_CANDIDATES)
+    if candidates:
+        cand.update(candidates)
+    cur = dict(engine.schedule())
+    table = []
+    cache = {}
+
+    def measure(s):
+        key = tuple(s[k] for k in SCHEDULE_KEYS)
+        if key not in cache:
+            engine.set_schedule(*key)
+            run()  # first run of a schedule: untimed
+            ms = sorted(float(run().ms[STAGE_TOTAL]) for _ in range(max(1, reps)))
+            cache[key] = ms[len(ms) // 2]
+            table.append((dict(s), cache[key]))
+        return cache[key]
+
+    best_ms = measure(cur)
+    for k in SCHEDULE_KEYS:
+        for v in cand[k]:
+            trial = dict(cur)
+            trial[k] = v
+            if trial == cur or not _valid(trial):
+                continue
+            ms = measure(trial)
+            if ms < best_ms * (1.0 - min_gain):
+                cur, best_ms = trial, ms
+    engine.set_schedule(*(cur[k] for k in SCHEDULE_KEYS))
+    return cur, table
 
 
 def save(path, best, table, workload=""):

@@ -590,6 +590,40 @@ int galphaSetLimits(galphaHandle h, int maxRounds, int spinLimit, int holdFirstT
     return GPUDT_OK;
 }
 
+int galphaSetSchedule(galphaHandle h, int shiftGroup, int missingGroup, int flipSync, int flipTailEnter,
+                      int flipTailLeave)
+{
+    if (!h) return GPUDT_ERR_ARG;
+    const int sg = shiftGroup > 0 ? shiftGroup : kShiftGroupDefault;
+    const int mg = missingGroup > 0 ? missingGroup : kMissingGroupDefault;
+    const int fs = flipSync > 0 ? flipSync : kFlipSyncDefault;
+    const int te = flipTailEnter >= 0 ? flipTailEnter : kTailEnterDefault;
+    const int tl = flipTailLeave > 0 ? flipTailLeave : kTailLeaveDefault;
+    if (sg > kMaxGroup || mg > kMaxGroup || fs > 64 || te > (1 << 20) || tl > (1 << 22) || tl < te)
+        return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    Ctx &c = h->H.c;
+    c.shift_group = sg;
+    c.missing_group = mg;
+    c.flip_sync = fs;
+    c.tail_enter = te;
+    c.tail_leave = tl;
+    return GPUDT_OK;
+}
+
+int galphaGetSchedule(galphaHandle h, int *out5)
+{
+    if (!h || !out5) return GPUDT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mu);
+    const Ctx &c = h->H.c;
+    out5[0] = c.shift_group;
+    out5[1] = c.missing_group;
+    out5[2] = c.flip_sync;
+    out5[3] = c.tail_enter;
+    out5[4] = c.tail_leave;
+    return GPUDT_OK;
+}
+
 int galphaSetBlockRun(galphaHandle h, int entries)
 {
     if (!h) return GPUDT_ERR_ARG;

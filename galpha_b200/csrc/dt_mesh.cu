@@ -665,15 +665,15 @@ struct CountState {
     }
 };
 
-// Rounds of the shifting loops run in groups of kShiftGroup between counter
+// Rounds of the shifting loops run in groups of c.shift_group between counter
 // reads: list lengths stay on the device (launch_dev), each round's count is
 // kept in ct->grp[], and a round after the loop's last one does nothing (an
 // empty list, or no site left in the state it acts on), so running past the
 // end of a loop changes no result.
-constexpr int kShiftGroup = 4;
 
 int stage_shift(Ctx &c)
 {
+    const int kShiftGroup = c.shift_group;
     int r;
     int shiftRounds = 0, badCount = 0;
     int *dropped = c.aux2;  // every site the optimistic phase dropped: the only undecided ones after it
@@ -1051,10 +1051,10 @@ int stage_missing(Ctx &c)
     if (nmiss == 0) return GPUDT_OK;
     int *loc = c.aux, *kind = c.aux2 + 0;
     // aux2 holds kind at [0, nmiss) ; edge tags in list2.  Rounds run in
-    // groups of kMissingGroup between counter reads (a round after the last
+    // groups of c.missing_group between counter reads (a round after the last
     // insertion finds no missing site and does nothing); each round's
     // insertions are kept in ct->grp[].
-    constexpr int kMissingGroup = 2;
+    const int kMissingGroup = c.missing_group;
     const long long recn = 4LL * c.cap_tris;
     int rounds = 0, remaining = nmiss, dups = 0;
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->ndup, 0, sizeof(int), c.stream));
@@ -1792,8 +1792,7 @@ int stage_boundary(Ctx &c)
 
 // -------------------------------------------------------------------- flip
 // Rounds run back to back on device-side counts (ping-pong active lists);
-// the host looks at the counters only every kFlipSync rounds.
-constexpr int kFlipSync = 4;
+// the host looks at the counters only every c.flip_sync rounds.
 
 // The first round tests every edge once, from the triangle with the lower
 // slot.  A flip replaces edge (b, c) of the quad (a, b, d, c) by (a, d); only
@@ -2042,8 +2041,8 @@ struct FlipRoundStart {
 // empties, when a round's list exceeds `leave` (the host goes back to launched
 // rounds) or after max_rounds; no thread ever waits on another block.
 constexpr int kTailThreads = 1024;
-constexpr int kTailEnter = 4096;    // the host hands over at or below this many active triangles
-constexpr int kTailLeave = 32768;   // the block hands back above this many
+// c.tail_enter: the host hands over at or below this many active triangles;
+// c.tail_leave: the block hands back above this many.
 
 __global__ void __launch_bounds__(kTailThreads) k_flip_tail(FlipCheck ck, FlipApply ap, Relinker rl, FlipReset rs,
                                                              int *l0, int *l1, int p0, int round0,
@@ -2101,17 +2100,17 @@ int stage_flip(Ctx &c)
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nflips, 0, sizeof(int), c.stream));
     // the first launched round tests every slot directly; the in-block tail
     // (small meshes) starts from a list of the live slots
-    if (nt <= kTailEnter) launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
+    if (nt <= c.tail_enter) launch_n(c, AllAlive{c.tv, lists[0], &c.ctr->act[0]}, nt);
     // marked edges: none before the first launched round (it tests all), all
     // when the in-block rounds start from the list of live slots
-    GALPHA_CUDA(cudaMemsetAsync(c.eflag, nt <= kTailEnter ? 7 : 0, (size_t)c.cap_tris, c.stream));
+    GALPHA_CUDA(cudaMemsetAsync(c.eflag, nt <= c.tail_enter ? 7 : 0, (size_t)c.cap_tris, c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vote, 0xff, sizeof(int) * (size_t)nt, c.stream));  // unsigned votes start at max
     GALPHA_CUDA(cudaMemsetAsync(stamp, 0xff, sizeof(int) * (size_t)c.cap_tris, c.stream));
     const long long capn = c.cap_tris, recn = 4LL * c.cap_tris;
     int rounds = 0;
     long long known = nt;  // active-list length at `rounds`, as last read (nt bounds the first)
     while (known > 0) {
-        if (known <= kTailEnter) {
+        if (known <= c.tail_enter) {
             const int p = rounds & 1;
             const int round0 = next_round(c);
             k_flip_tail<<<1, kTailThreads, 0, c.stream>>>(
@@ -2120,7 +2119,7 @@ int stage_flip(Ctx &c)
                 FlipApply{c.tv, c.tn, c.fwd, c.epoch, c.vtri, c.vote, stamp, nullptr, nullptr, prop, target, cands,
                           c.rec, 0, c.ctr, c.eflag, false, &c.ctr->cand, 3ll * c.cap_tris},
                 Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, 0, c.ctr}, FlipReset{c.vote, target, cands},
-                lists[0], lists[1], p, round0, c.max_rounds + 1 - rounds, kTailLeave);
+                lists[0], lists[1], p, round0, c.max_rounds + 1 - rounds, c.tail_leave);
             count_launch();
             GALPHA_CUDA(cudaGetLastError());
             r = read_counters(c);
@@ -2132,9 +2131,9 @@ int stage_flip(Ctx &c)
             known = c.hctr->act[rounds & 1];
             if (known == 0) break;
             if (rounds > c.max_rounds) return GPUDT_ERR_NOCONVERGE;
-            if (known <= kTailLeave) return set_last_error("flip: in-block rounds stopped early"), GPUDT_ERR_TOPOLOGY;
+            if (known <= c.tail_leave) return set_last_error("flip: in-block rounds stopped early"), GPUDT_ERR_TOPOLOGY;
         }
-        for (int k = 0; k < kFlipSync; k++) {
+        for (int k = 0; k < c.flip_sync; k++) {
             int p = rounds & 1;
             int round = next_round(c);
             launch_n(c, FlipRoundStart{p, c.ctr}, 1);

@@ -24,7 +24,10 @@ constexpr int kMargin = kFakeSpacing / 2 + 1;    // real sites stay >= 17 pixels
 constexpr int kMaxFan = 64;                      // star holes / fans handled per thread
 constexpr int kMaxRounds = 100000;               // cap of every iterative stage (default)
 constexpr int kSpinLimit = 1 << 22;              // bound of every look-back wait (default)
-constexpr int kBlockRun = 1 << 16;               // longest exact-sort run for one block (default)
+constexpr int kBlockRun = 1 << 16;
+constexpr int kShiftGroupDefault = 4, kMissingGroupDefault = 2, kFlipSyncDefault = 4;
+constexpr int kTailEnterDefault = 4096, kTailLeaveDefault = 32768;
+constexpr int kMaxGroup = 8;  // Counters::grp holds one group's per-round counts               // longest exact-sort run for one block (default)
 
 // vertex states
 enum : int8_t {
@@ -207,6 +210,15 @@ struct Ctx {
     // the exact comparator by many blocks (one launch per merge level)
     // instead of by one block
     int block_run = kBlockRun;
+    // loop schedule (galphaSetSchedule): rounds per counter read of the
+    // shifting and missing-site loops and of the flip stage, and the active
+    // list lengths at which the flip stage hands its rounds to one block and
+    // takes them back.  None of them changes a result.
+    int shift_group = kShiftGroupDefault;
+    int missing_group = kMissingGroupDefault;
+    int flip_sync = kFlipSyncDefault;
+    int tail_enter = kTailEnterDefault;
+    int tail_leave = kTailLeaveDefault;
 };
 
 // ------------------------------------------------------------- error helpers

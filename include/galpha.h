@@ -278,6 +278,23 @@ int galphaSetLimits(galphaHandle h, int maxRounds, int spinLimit, int holdFirstT
  * order such runs without a size limit. */
 int galphaSetBlockRun(galphaHandle h, int entries);
 
+/* Loop schedule of the handle's later calls.  shiftGroup and missingGroup
+ * (1..8; defaults 4 and 2): rounds of the shifting loops and of missing-site
+ * insertion run between two device-to-host counter reads; flipSync (1..64,
+ * default 4): the same for the flip rounds; flipTailEnter (0..2^20, default
+ * 4,096): the active flip list length at or below which the remaining rounds
+ * run inside one block; flipTailLeave (>= flipTailEnter, up to 2^22, default
+ * 32,768): the length above which that block hands them back.  A round past
+ * the end of a loop does nothing and the in-block rounds are the launched
+ * rounds' functors, so no value changes a result, only the time and
+ * gpudtStatus.hostReads; 0 (-1 for flipTailEnter) restores a default, values
+ * out of range return GPUDT_ERR_ARG.  galphaGetSchedule fills out5 with the
+ * five values in force.  The autotuner (galpha_b200.autotune) picks them per
+ * workload.  No counterpart in the reference. */
+int galphaSetSchedule(galphaHandle h, int shiftGroup, int missingGroup, int flipSync, int flipTailEnter,
+                      int flipTailLeave);
+int galphaGetSchedule(galphaHandle h, int *out5);
+
 /* Text of the last error on the calling thread (cleared when a compute call
  * -- RunDevice, Triangulate, Compute*, RunBatch*, gpudtComputeDTEx -- starts). */
 const char *galphaLastError(void);

@@ -1,5 +1,5 @@
-"""CPU tests of the batch-density autotuner with a fake engine whose device
-time depends on the density."""
+"""CPU tests of the autotuner (batch density, loop schedule) with a fake
+engine whose device time depends on the settings."""
 import json
 
 import numpy as np
@@ -47,3 +47,41 @@ def test_ties_go_to_the_lower_density_and_roundtrip(tmp_path):
     assert A.load(str(p)) == 4.0 and json.load(open(p))["workload"] == "fake"
     with pytest.raises(ValueError):
         A.tune_batch_density(eng, [], candidates=())
+
+
+class FakeScheduleEngine:
+    DEFAULT = dict(shift_group=4, missing_group=2, flip_sync=4, flip_tail_enter=4096, flip_tail_leave=32768)
+
+    def __init__(self, cost):
+        self.cost = cost
+        self.s = dict(self.DEFAULT)
+        self.runs = 0
+
+    def schedule(self):
+        return dict(self.s)
+
+    def set_schedule(self, sg, mg, fs, te, tl):
+        assert tl >= te
+        self.s = dict(shift_group=sg, missing_group=mg, flip_sync=fs, flip_tail_enter=te, flip_tail_leave=tl)
+
+    def run(self):
+        self.runs += 1
+        return FakeStatus(self.cost(self.s))
+
+
+def test_schedule_descends_to_the_fastest_and_leaves_it_set():
+    want = dict(shift_group=8, missing_group=1, flip_sync=16, flip_tail_enter=16384, flip_tail_leave=131072)
+    eng = FakeScheduleEngine(lambda s: 100.0 + 10.0 * sum(abs(s[k] - want[k]) / max(1, want[k]) for k in want))
+    best, table = A.tune_schedule(eng, eng.run, reps=3)
+    assert best == want and eng.s == want
+    # every measured schedule is valid (tail leave >= enter) and measured once
+    assert all(t[0]["flip_tail_leave"] >= t[0]["flip_tail_enter"] for t in table)
+    keys = [tuple(sorted(t[0].items())) for t in table]
+    assert len(keys) == len(set(keys))
+    assert eng.runs == 4 * len(table)  # one untimed and three timed runs each
+
+
+def test_schedule_keeps_the_default_within_noise():
+    eng = FakeScheduleEngine(lambda s: 100.0 - 0.5 * (s["flip_sync"] == 8))  # 0.5 % better: below min_gain
+    best, _ = A.tune_schedule(eng, eng.run, reps=1)
+    assert best == FakeScheduleEngine.DEFAULT

@@ -235,3 +235,30 @@ def test_run_device_flags(engine, flags):
     assert canon_set(vtx) == canon_set(O.dt(pts)[0])
     ok, rep = compare_dt(pts, vtx, tri["tri"].reshape(-1, 3))
     assert ok and rep["identical"], rep
+
+
+@pytest.mark.parametrize("sched", [(1, 1, 1, 0, 1), (8, 4, 16, 16384, 131072), (2, 8, 64, 1 << 20, 1 << 22)])
+def test_schedule_changes_no_result(engine, sched):
+    """galphaSetSchedule moves only the counter reads: every schedule gives
+    the oracle's triangulation and the same alpha result."""
+    pts = D.uniform_points(60000, 91)
+    base = engine.triangulate(G.GPUDTParams(pts, fboSize=1024))
+    a0 = engine.alpha_resident()
+    try:
+        engine.set_schedule(*sched)
+        dt = engine.triangulate(G.GPUDTParams(pts, fboSize=1024))
+        a1 = engine.alpha_resident()
+        assert engine.schedule()["flip_sync"] == sched[2]
+    finally:
+        engine.set_schedule()
+    assert canon_set(dt.vtx) == canon_set(base.vtx) == canon_set(O.dt(pts)[0])
+    np.testing.assert_array_equal(a1["spectrum"], a0["spectrum"])
+    assert dt.status.hostReads != base.status.hostReads or sched[2] == 4
+
+
+def test_schedule_rejects_out_of_range(engine):
+    for bad in [(9, 0, 0, -1, 0), (0, 0, 65, -1, 0), (0, 0, 0, 5000, 4096)]:
+        with pytest.raises(G.GpudtError):
+            engine.set_schedule(*bad)
+    assert engine.schedule() == dict(shift_group=4, missing_group=2, flip_sync=4, flip_tail_enter=4096,
+                                     flip_tail_leave=32768)
