@@ -643,11 +643,9 @@ int galphaRunDevice(galphaHandle h, const double *d_xy, int n, double minX, doub
     cudaGetLastError();  // clear an error left by unrelated runtime calls
     const int level = withAlpha & 3;
     ev_record(c, 0);
+    c.want_outtri = (withAlpha & GALPHA_RUN_TRIANGLES) != 0;  // written by the compaction
     int r = run_dt(h->H, d_xy, n, minX, minY, maxX, maxY, fboSize);
-    if (!r && (withAlpha & GALPHA_RUN_TRIANGLES)) {
-        r = ensure_outtri(c);  // the gpudtTriangle records, timed with the compaction
-        ev_record(c, 8);
-    }
+    c.want_outtri = false;
     if (!r && level) {
         ev_record(c, 8);
         r = stage_alpha(c);
@@ -687,9 +685,11 @@ int galphaTriangulate(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *ou
     r = upload_points(h->H, params->points, params->nPoints);
     c.n_cons = params->nConstraints;
     c.h_cons = params->constraints;
+    c.want_outtri = out != nullptr;
     if (!r)
         r = run_dt(h->H, h->H.d_xy, params->nPoints, params->minX, params->minY, params->maxX, params->maxY,
                    params->fboSize);
+    c.want_outtri = false;
     c.n_cons = 0;
     c.h_cons = nullptr;
     if (!r && out) {
@@ -954,9 +954,11 @@ int galphaComputeAll(galphaHandle h, const GPUDTPARAMS *params, GPUDTOUTPUT *dt,
     r = upload_points(H, params->points, params->nPoints);
     c.n_cons = params->nConstraints;
     c.h_cons = params->constraints;
+    c.want_outtri = true;
     if (!r)
         r = run_dt(H, H.d_xy, params->nPoints, params->minX, params->minY, params->maxX, params->maxY,
                    params->fboSize);
+    c.want_outtri = false;
     c.n_cons = 0;
     c.h_cons = nullptr;
     gpudtTriangle *tris = nullptr;

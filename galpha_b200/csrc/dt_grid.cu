@@ -317,7 +317,9 @@ struct FirstDistinct {
     int *out;
     __device__ void operator()(long long i) const
     {
-        if (xy[2 * i] != xy[0] || xy[2 * i + 1] != xy[1]) atomicMin(out, (int)i);
+        // one atomic per point below the smallest index found so far (a plain
+        // read filters the rest; usually point 1 already differs)
+        if ((xy[2 * i] != xy[0] || xy[2 * i + 1] != xy[1]) && (int)i < *(volatile int *)out) atomicMin(out, (int)i);
     }
 };
 
@@ -332,7 +334,7 @@ struct CountOffLine {
         if (j >= n) return;  // every point equals point 0: nothing is off the line
         int s = orient2d_filter(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
         if (s == 2) s = orient2d_exact(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
-        if (s != 0) atomicAdd(&ct->changed, 1);
+        if (s != 0 && *(volatile int *)&ct->changed == 0) ct->changed = 1;  // any one point off the line
     }
 };
 

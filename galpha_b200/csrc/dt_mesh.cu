@@ -2865,9 +2865,12 @@ int stage_compact(Ctx &c)
     launch_n(c, MarkAlive{c.tv, c.aux}, nt);
     r = exclusive_scan_int(c, c.aux, c.aux2, nt, &c.ctr->nlist);
     if (r) return r;
-    // cv / cn only: the gpudtTriangle records are built when a download asks for them
-    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, nullptr, c.renumbered ? c.perm : nullptr, c.fwd}, nt);
-    c.outtri_ready = false;
+    // cv / cn, and the gpudtTriangle records when the call will return them
+    // (otherwise they are built when a download asks for them)
+    launch_n(c, CompactWrite{c.tv, c.tn, c.aux2, c.cv, c.cn, c.want_outtri ? c.outtri : nullptr,
+                             c.renumbered ? c.perm : nullptr, c.fwd},
+             nt);
+    c.outtri_ready = c.want_outtri;
     GALPHA_CUDA(cudaGetLastError());
     r = read_counters(c);
     if (r) return r;

@@ -170,6 +170,7 @@ struct Ctx {
     long long rhist_ints = 0;  // its size
     gpudtTriangle *outtri = nullptr;  // [cap] AoS output staging
     bool outtri_ready = false;          // outtri holds the current mesh (built on the first download)
+    bool want_outtri = false;           // this call needs outtri: compaction writes it directly
     galphaEdgeInterval *edge_aos = nullptr;  // [2*cap] edge records for download
 
     DevBuf bufs[64];
