@@ -4,7 +4,7 @@
 //   computeScalingFactors (gpudt.cpp:722-769)      grid_scaling: power-of-two aligned
 //                                                  scale/shift so every snapped
 //                                                  coordinate shift + g*scale is exact
-//   fake boundary circle (gpudt.cpp:810-832) and   fake ring: sites every <= 32 pixels on
+//   fake boundary circle (gpudt.cpp:810-832) and   fake ring: sites every <= 16 pixels on
 //   gpudtFixConvexHull (gpudt.cpp:349-647)          the texture border, inside the texture,
 //                                                  so the dual is closed by construction
 //                                                  and no host hull walk is needed

@@ -19,8 +19,8 @@
 namespace galpha {
 
 // ------------------------------------------------------------- constants
-constexpr int kFakeSpacing = 32;                 // fake ring site every <= 32 pixels
-constexpr int kMargin = kFakeSpacing / 2 + 1;    // real sites stay >= 17 pixels from the border
+constexpr int kFakeSpacing = 16;                 // fake ring site every <= 16 pixels
+constexpr int kMargin = kFakeSpacing / 2 + 1;    // real sites stay >= 9 pixels from the border
 constexpr int kMaxFan = 64;                      // star holes / fans handled per thread
 constexpr int kMaxRounds = 100000;               // cap of every iterative stage (default)
 constexpr int kSpinLimit = 1 << 22;              // bound of every look-back wait (default)
