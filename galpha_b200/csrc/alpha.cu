@@ -122,6 +122,15 @@ struct EdgeCount {
     }
 };
 
+// The exact attached test, called with coordinates by value: the caller then
+// keeps its operands in registers (an array argument would have to live in
+// local memory on the hot path, for a call that almost never happens).
+__device__ __noinline__ int attached_exact_v(double ix, double iy, double jx, double jy, double kx, double ky)
+{
+    const double i[2] = {ix, iy}, j[2] = {jx, jy}, k[2] = {kx, ky};
+    return attached_exact(i, j, k);
+}
+
 // Triangle keys + owned edges + attached test.
 struct TriKeys {
     const int4 *cv, *cn;
@@ -162,7 +171,7 @@ struct TriKeys {
             int att = attached_filter(qa, qb, qk);
             if (att == 2) {
                 atomicAdd(&ct->exact_attached, 1ull);
-                att = attached_exact(qa, qb, qk);
+                att = attached_exact_v(pa.x, pa.y, pb.x, pb.y, pk.x, pk.y);
             }
             if (att == 0 && nb >= 0) {
                 double2 po = P[geti(gv[dtri(nb)], dori(nb))];
@@ -170,7 +179,7 @@ struct TriKeys {
                 att = attached_filter(qa, qb, qo);
                 if (att == 2) {
                     atomicAdd(&ct->exact_attached, 1ull);
-                    att = attached_exact(qa, qb, qo);
+                    att = attached_exact_v(pa.x, pa.y, pb.x, pb.y, po.x, po.y);
                 }
             }
             if (att == EXACT_OVERFLOW) set_err(ct, GPUDT_ERR_EXACT, 100);
@@ -768,7 +777,7 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nlist2, 0, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.keys, 0, sizeof(unsigned long long), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(c.vals, 0, sizeof(int), c.stream));
-    launch_n(c, TriKeys{c.cv, c.cn, alpha_geom_tris(c), c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
+    launch_occ<4>(c, TriKeys{c.cv, c.cn, alpha_geom_tris(c), c.opos, e_off, c.keys, c.vals, c.edges, unatt, c.edge_ro, c.list, c.ctr}, nT);
     // the sliver list's length stays on the device; TriKeys' errors are read
     // with the spectrum length below
     launch_dev(c, SliverKeys{alpha_geom_tris(c), c.opos, c.list, c.keys, c.ctr}, &c.ctr->nlist2, nT);

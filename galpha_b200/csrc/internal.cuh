@@ -261,6 +261,17 @@ __global__ void __launch_bounds__(256) k_for_each(F f, long long n)
     for (; i < n; i += stride) f(i);
 }
 
+// The same with at least MINB resident blocks of 256 threads per SM asked of
+// the register allocator (for latency-bound functors whose rare exact paths
+// would otherwise set the register count of the common one).
+template <class F, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_for_each_occ(F f, long long n)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) f(i);
+}
+
 // Grid-stride launch over [0, *n) with the count read on the device, so a
 // round of kernels can run without the host learning its size.
 template <class F>
@@ -280,6 +291,17 @@ inline void launch_dev(const Ctx &c, F f, const int *n_dev, long long max_n)
     long long maxb = (long long)c.sm_count * 8;
     if (blocks > maxb) blocks = maxb;
     k_for_each_dev<<<(unsigned)blocks, 256, 0, c.stream>>>(f, n_dev);
+    count_launch();
+}
+
+template <int MINB, class F>
+inline void launch_occ(const Ctx &c, F f, long long n)
+{
+    if (n <= 0) return;
+    long long blocks = (n + 255) / 256;
+    long long maxb = (long long)c.sm_count * 8;
+    if (blocks > maxb) blocks = maxb;
+    k_for_each_occ<F, MINB><<<(unsigned)blocks, 256, 0, c.stream>>>(f, n);
     count_launch();
 }
 
