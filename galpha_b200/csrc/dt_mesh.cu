@@ -748,9 +748,11 @@ int stage_shift(Ctx &c)
             launch_n(c, CopyElems<int>{&c.ctr->grp[j], &c.ctr->nlist}, 1);
             const int round = next_round(c);
             GALPHA_CUDA(cudaMemsetAsync(&c.ctr->nrec, 0, sizeof(int), c.stream));
+            // a round selects at most the bad sites left (the grid is sized by them:
+            // an empty round of this local-memory-heavy kernel then stays cheap)
             launch_dev(c, BadRemove{c.tv, c.tn, c.fwd, c.epoch, c.freelist, c.vtri, c.anchor, c.list, c.pos,
                                     c.vstate, c.rec, round, c.N, c.ctr},
-                       &c.ctr->nlist, c.N);
+                       &c.ctr->nlist, badCount);
             launch_dev(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, &c.ctr->nrec, recn);
         }
         GALPHA_CUDA(cudaGetLastError());
@@ -1385,10 +1387,18 @@ struct ZeroInts {
 
 
 // Removal of the selected fake sites, one warp per fake: the lanes load the
-// stored fan, the chain U[0..d] and its positions into shared memory; lane 0
-// runs the stack rule (the ccw > 0 rule of cudaBoundary.cu:278) on that copy;
-// the lanes then write the remaining hull edges, the boundary candidates and
-// the released slots.
+// stored fan, the chain U[0..d] and its positions into shared memory, then
+// patch the pocket with the stack rule (the ccw > 0 rule of
+// cudaBoundary.cu:278): for each chain vertex in order, while the last two
+// stack vertices and it turn left, they and it become a triangle and the top
+// is popped.  The chain is cut into up to 32 pieces that share their end
+// vertices; each lane runs the rule on its piece (its pops are pops of the
+// whole chain too: a vertex inside the hull of a piece is inside the hull of
+// the chain), then lane 0 runs it once more over the pieces' leftover stacks
+// in order.  The triangles differ from one sequential pass but fill the same
+// pocket (the chain is star-shaped from the removed site), and the flip stage
+// makes the mesh Delaunay either way.  The lanes then write the remaining
+// hull edges, the boundary candidates and the released slots.
 struct FakeRemoveArgs {
     int4 *tv, *tn, *fwd;
     int *epoch, *freelist, *vtri;
@@ -1402,19 +1412,77 @@ struct FakeRemoveArgs {
     Counters *ct;
 };
 
-// Dynamic shared memory for fans of up to M triangles.
+constexpr int kFrPieces = 32;    // one piece per lane
+constexpr int kFrMinPiece = 16;  // chain edges per piece at least
+
+// Dynamic shared memory for fans of up to M triangles: Fs, Fi, O (M ints),
+// U (M + 1), the stacks S, SO (M + 1 + kFrPieces each: each piece's stack
+// starts at its first chain position plus its lane), positions P (M + 1).
+__host__ __device__ constexpr size_t fake_remove_ints(int M) { return (size_t)(6 * M + 3 + 2 * kFrPieces); }
 __host__ __device__ constexpr size_t fake_remove_smem(int M)
 {
-    return ((size_t)(3 * M + 3 * (M + 1)) * sizeof(int) + 15) / 16 * 16 + (size_t)(M + 1) * sizeof(double2);
+    return (fake_remove_ints(M) * sizeof(int) + 15) / 16 * 16 + (size_t)(M + 1) * sizeof(double2);
 }
+
+// One step of the stack rule: chain position k arrives through the edge owned
+// by wown (-2 - j: original chain edge j; >= 0: an edge of a new triangle;
+// -1: none).  Pops (and makes triangles) while the turn is left; returns the
+// new stack height.  Slots come from take().
+struct FrRule {
+    const FakeRemoveArgs &a;
+    const int *Fs, *Fi, *O, *U;
+    const double2 *P;
+    int rbase;
+    int *nrec_orig;  // original chain edges linked so far (this lane)
+    __device__ void owner_link(int ownv, int loc) const
+    {
+        if (ownv <= -2) {
+            const int q = -2 - ownv;
+            set_fwd(a.fwd, Fs[q], Fi[q], loc);
+            a.rec[rbase + q] = Relink{loc, O[q]};
+            (*nrec_orig)++;
+        } else {
+            set_link(a.tn, loc, ownv);
+            set_link(a.tn, ownv, loc);
+        }
+    }
+    template <class Take>
+    __device__ int push(int *S, int *SO, int top, int k, int wown, Take take, OrientTally &tally) const
+    {
+        const int wv = U[k];
+        while (top >= 2 && orient_staged(P[S[top - 2]], P[S[top - 1]], P[k], a.ct, tally) > 0) {
+            const int s = take();
+            if (s < 0) {  // more triangles than chain edges: not a pocket
+                set_err(a.ct, GPUDT_ERR_TOPOLOGY, 75);
+                break;
+            }
+            const int A = U[S[top - 2]], B = U[S[top - 1]];
+            a.tv[s] = make_int4(A, B, wv, 0);
+            a.tn[s] = make_int4(-1, -1, -1, 0);
+            // opp wv (2): A->B owned by SO[top-1]; opp A (0): B->wv owned by wown;
+            // opp B (1): wv->A, the new chain edge A->wv
+            owner_link(SO[top - 1], enc(s, 2));
+            owner_link(wown, enc(s, 0));
+            wown = enc(s, 1);
+            a.vtri[A] = enc(s, 0);
+            a.vtri[B] = enc(s, 1);
+            a.vtri[wv] = enc(s, 2);
+            top--;
+        }
+        S[top] = k;
+        SO[top] = wown;
+        return top + 1;
+    }
+};
 
 // Items whose fan has dmin..M triangles (the short and the long launch).
 __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int *n_dev, int M, int dmin)
 {
     extern __shared__ __align__(16) unsigned char fr_smem[];
-    int *Fs = (int *)fr_smem, *Fi = Fs + M, *O = Fi + M, *U = O + M, *S = U + M + 1, *SO = S + M + 1;
-    double2 *P = (double2 *)(fr_smem + ((size_t)(3 * M + 3 * (M + 1)) * sizeof(int) + 15) / 16 * 16);
-    __shared__ int s_top, s_used, s_rbase, s_rn;
+    int *Fs = (int *)fr_smem, *Fi = Fs + M, *O = Fi + M, *U = O + M, *S = U + M + 1, *SO = S + M + 1 + kFrPieces;
+    double2 *P = (double2 *)(fr_smem + (fake_remove_ints(M) * sizeof(int) + 15) / 16 * 16);
+    __shared__ int s_top[kFrPieces], s_used[kFrPieces];
+    __shared__ int s_top2, s_cl, s_co;
     const int lane = threadIdx.x;
     const int n = *n_dev;
     for (int item = blockIdx.x; item < n; item += gridDim.x) {
@@ -1439,88 +1507,98 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
         }
         __syncwarp();
         for (int k = lane; k <= d; k += 32) P[k] = a.pos[U[k]];
+        // every one of the d chain edges ends with exactly one relink record,
+        // at rbase + its index (linked to a new triangle, or left as a hull edge)
+        int rbase = 0;
+        if (lane == 0 && d > 0) rbase = atomicAdd(&a.ct->nrec, d);
+        rbase = __shfl_sync(0xffffffffu, rbase, 0);
         __syncwarp();
+        const int G = max(1, min(kFrPieces, d / kFrMinPiece));
+        int nrec_orig = 0;
+        OrientTally tally;
+        const FrRule rule{a, Fs, Fi, O, U, P, rbase, &nrec_orig};
+        // 1. each lane's piece [b0, b1]; its stack at S + b0 + lane
+        const int b0 = (int)((long long)lane * d / G), b1 = (int)((long long)(lane + 1) * d / G);
+        if (lane < G) {
+            int *LS = S + b0 + lane, *LSO = SO + b0 + lane;
+            int top = 0, used = 0;
+            for (int k = b0; k <= b1; k++)
+                top = rule.push(LS, LSO, top, k, k > b0 ? -2 - (k - 1) : -1, [&] { return Fs[b0 + used++]; },
+                                tally);
+            s_top[lane] = top;
+            s_used[lane] = used;
+        }
+        __syncwarp();
+        // 2. lane 0: the leftover stacks in order (a piece's first vertex is the
+        // previous piece's last); the stack is rebuilt in place at S[0..)
+        // (it never passes the entry being read).  Slots: the pieces' unused
+        // ones, in piece order.
         if (lane == 0) {
-            // every one of the d chain edges ends with exactly one relink
-            // record (linked to a new triangle, or left as a hull edge)
-            const int rbase = d > 0 ? atomicAdd(&a.ct->nrec, d) : 0;
-            int rn = 0, top = 0, used = 0;
-            auto owner_link = [&](int ownv, int loc) {
-                if (ownv <= -2) {
-                    const int k = -2 - ownv;
-                    set_fwd(a.fwd, Fs[k], Fi[k], loc);
-                    a.rec[rbase + rn++] = Relink{loc, O[k]};
-                } else {
-                    set_link(a.tn, loc, ownv);
-                    set_link(a.tn, ownv, loc);
+            int cl = 0, co = 0;  // next free slot: piece cl, offset co past its used ones
+            auto take = [&]() {
+                for (; cl < G; cl++, co = 0) {
+                    const int pb0 = (int)((long long)cl * d / G), pb1 = (int)((long long)(cl + 1) * d / G);
+                    if (pb0 + s_used[cl] + co < pb1) return Fs[pb0 + s_used[cl] + co++];
                 }
+                return -1;
             };
-            OrientTally tally;
-            for (int k = 0; k <= d; k++) {
-                const int wv = U[k];
-                int wown = k > 0 ? -2 - (k - 1) : -1;  // chain edge U[k-1] -> U[k]: fan triangle k-1
-                while (top >= 2 && orient_staged(P[S[top - 2]], P[S[top - 1]], P[k], a.ct, tally) > 0) {
-                    const int s = Fs[used++];
-                    const int A = U[S[top - 2]], B = U[S[top - 1]];
-                    a.tv[s] = make_int4(A, B, wv, 0);
-                    a.tn[s] = make_int4(-1, -1, -1, 0);
-                    // opp wv (2): A->B owned by SO[top-1]; opp A (0): B->wv owned by wown;
-                    // opp B (1): wv->A, the new chain edge A->wv
-                    owner_link(SO[top - 1], enc(s, 2));
-                    owner_link(wown, enc(s, 0));
-                    wown = enc(s, 1);
-                    a.vtri[A] = enc(s, 0);
-                    a.vtri[B] = enc(s, 1);
-                    a.vtri[wv] = enc(s, 2);
-                    top--;
+            int top2 = 0;
+            for (int L = 0; L < G; L++) {
+                const int pb0 = (int)((long long)L * d / G);
+                for (int j = L == 0 ? 0 : 1; j < s_top[L]; j++) {
+                    const int idx = pb0 + L + j;
+                    top2 = rule.push(S, SO, top2, S[idx], SO[idx], take, tally);
                 }
-                S[top] = k;  // stack of chain positions
-                SO[top] = wown;
-                top++;
             }
-            tally.flush(a.ct);
-            s_top = top;
-            s_used = used;
-            s_rbase = rbase;
-            s_rn = rn;
+            s_top2 = top2;
+            s_cl = cl;
+            s_co = co;
         }
         __syncwarp();
-        const int top = s_top, used = s_used, rbase = s_rbase;
-        // remaining chain edges are hull edges now (records after the rn
-        // written by the stack rule, in stack order)
-        {
-            int before = 0;  // chain-owned stack edges before this lane's
-            for (int k = 1 + lane; k < top; k += 32) {
-                const int ownv = SO[k];
-                if (ownv > -2) set_link(a.tn, ownv, -1);
+        tally.flush(a.ct);
+        const int top = s_top2, cl = s_cl, co = s_co;
+        // 3. the remaining chain edges are hull edges now
+        for (int k = 1 + lane; k < top; k += 32) {
+            const int ownv = SO[k];
+            if (ownv > -2) {
+                set_link(a.tn, ownv, -1);
+            } else {
+                const int q = -2 - ownv;
+                set_fwd(a.fwd, Fs[q], Fi[q], -1);
+                a.rec[rbase + q] = Relink{-1, O[q]};
+                nrec_orig++;
             }
-            int rn = s_rn;
-            for (int k0 = 1; k0 < top; k0 += 32) {
-                const int k = k0 + lane;
-                const bool own = k < top && SO[k] <= -2;
-                const unsigned m = __ballot_sync(0xffffffffu, own);
-                if (own) {
-                    const int q = -2 - SO[k];
-                    set_fwd(a.fwd, Fs[q], Fi[q], -1);
-                    a.rec[rbase + rn + __popc(m & ((1u << lane) - 1u))] = Relink{-1, O[q]};
-                }
-                rn += __popc(m);
-            }
-            (void)before;
-            if (lane == 0 && rn != d) set_err(a.ct, GPUDT_ERR_TOPOLOGY, 74);
         }
         {
+            int tot = nrec_orig;
+            for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            if (lane == 0 && tot != d) set_err(a.ct, GPUDT_ERR_TOPOLOGY, 74);
+        }
+        {
+            // released slots: each piece's unused ones past what step 2 took
+            int mine = 0, from = 0;
+            if (lane < G && lane >= cl) {
+                from = b0 + s_used[lane] + (lane == cl ? co : 0);
+                mine = max(0, b1 - from);
+            }
+            int incl = mine;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int nrel = __shfl_sync(0xffffffffu, incl, 31);
             int cb = 0, fb = 0;
             if (lane == 0) {
                 cb = atomicAdd(&a.ct->nlist2, top);
-                fb = used < d || nsh ? atomicAdd(&a.ct->nfree, d - used + nsh) : 0;
+                fb = nrel || nsh ? atomicAdd(&a.ct->nfree, nrel + nsh) : 0;
             }
             cb = __shfl_sync(0xffffffffu, cb, 0);
             fb = __shfl_sync(0xffffffffu, fb, 0);
             for (int k = lane; k < top; k += 32) a.cand[cb + k] = U[S[k]];
-            for (int k = used + lane; k < d; k += 32) {
-                a.tv[Fs[k]] = make_int4(-1, -1, -1, 0);
-                a.freelist[fb + k - used] = Fs[k];
+            for (int k = 0; k < mine; k++) {
+                const int t = Fs[from + k];
+                a.tv[t] = make_int4(-1, -1, -1, 0);
+                a.freelist[fb + incl - mine + k] = t;
             }
             // triangles shared by consecutive members of a run: inside the removed
             // region.  Both members are marked here: a middle member whose fan is
@@ -1534,7 +1612,7 @@ __global__ void __launch_bounds__(32) k_fake_remove(FakeRemoveArgs a, const int 
                 a.vtri[m2] = -1;
                 a.vstate[m2] = VS_GONE;
                 a.tv[t] = make_int4(-1, -1, -1, 0);
-                a.freelist[fb + d - used + k] = t;
+                a.freelist[fb + nrel + k] = t;
             }
         }
         if (lane == 0) {
