@@ -21,7 +21,7 @@ Two more legs share the JSON line (rank 0, N = 1):
            (galphaRunBatch), against plain per-set galphaRunDevice calls on
            a sample, plus end to end through galphaRunBatchHost.
   serving  c5: a Poisson request stream served by continuous batching on
-           six handles (streams) with quantile alpha queries on the
+           eight handles (streams) with quantile alpha queries on the
            resident meshes; p50 / p99 latency.
 
 Multi-GPU: a single DT does not shard (the flip, insertion and sort stages are
@@ -274,7 +274,7 @@ def predicate_stages(st):
     return out
 
 
-def serving_leg(G, D, seconds, rate=2000.0, nslots=6):
+def serving_leg(G, D, seconds, rate=2000.0, nslots=8):
     """c5: Poisson requests (rate per s) over `seconds`, sizes log-uniform in
     [1000, 1048576], half uniform and half Gaussian clusters (the c3 blob
     recipe), each followed by alpha queries at spectrum quantiles 0.1 / 0.5 /
@@ -553,8 +553,15 @@ def main():
         cpu = cpu_baseline()
     batched = serving = None
     if rank == 0 and world == 1 and not a.no_batch:
-        batched = batched_leg(G, D, torch, stream)
-        serving = serving_leg(G, D, a.serve_seconds)
+        # the extra legs report a failure in the line instead of losing it
+        try:
+            batched = batched_leg(G, D, torch, stream)
+        except Exception as x:  # recorded below
+            batched = {"error": "%s: %s" % (type(x).__name__, x)}
+        try:
+            serving = serving_leg(G, D, a.serve_seconds)
+        except Exception as x:  # recorded below
+            serving = {"error": "%s: %s" % (type(x).__name__, x)}
 
     if rank == 0:
         line = {
