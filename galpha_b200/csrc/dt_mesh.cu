@@ -2425,7 +2425,7 @@ struct ConsRecord {
         const int k = (int)kk;
         win[k] = 0;
         if (done[k] || size[k] == 0) return;
-        if ((long long)off[k] + size[k] > pool_ints) {
+        if (off[k] < 0 || (long long)off[k] + size[k] > pool_ints) {  // (a wrapped offset scan included)
             set_err(w.ct, GPUDT_ERR_NOMEM, 125);
             return;
         }
