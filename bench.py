@@ -360,11 +360,10 @@ def e2e_pipelined(G, params, n, steps, device, dist, world, nslots=6, schedule=N
     finally:
         for e in engines:
             e.close()
-    tw = torch.tensor([wall], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(tw, op=dist.ReduceOp.MAX)
-    wall = float(tw.item())
-    return {"value": world * nslots * steps * n / wall / 1e6, "unit": UNIT, "handles": nslots,
+    from galpha_b200 import replicas as R
+
+    wall = R.max_over_ranks(wall, dist, "cuda")
+    return {"value": R.job_throughput(world, nslots * steps * n, wall * 1e3) / 1e6, "unit": UNIT, "handles": nslots,
             "calls": nslots * steps, "ms_per_call": wall / (nslots * steps) * 1e3,
             "timing": "wall clock over all calls (host API, pinned buffers)"}
 
@@ -385,6 +384,7 @@ def main():
 
     import galpha_b200 as G
     from galpha_b200 import datasets as D
+    from galpha_b200 import replicas as R
 
     torch.cuda.set_device(local)
     dist = None
@@ -446,13 +446,9 @@ def main():
     clk = clocks.stop()
     ms = [s.elapsed_time(e) for s, e in ev]
     mean_ms = sum(ms) / len(ms)
-    t = torch.tensor([mean_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = R.max_over_ranks(mean_ms, dist, "cuda")  # replicas: the slowest rank times the job
     nt, ne, ns = eng.counts()
-    value = world * n / (max_ms / 1e3) / 1e6
+    value = R.job_throughput(world, n, max_ms) / 1e6
 
     # rooflines.  The sort of the spectrum keys is the largest HBM-bound kernel
     # of the step (the FlipCheck share is gather/latency-bound in-circle work).
@@ -539,12 +535,9 @@ def main():
         h2d = 16 * n
         d2h = (36 * dt.nTris + al["spectrum"].nbytes + al["point_list"].nbytes + al["edge_list"].nbytes
                + al["tri_list"].nbytes)
-        em = sum(tms) / len(tms)
-        te = torch.tensor([em], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * n / (float(te.item()) / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": float(te.item()),
+        em = R.max_over_ranks(sum(tms) / len(tms), dist, "cuda")
+        e2e = {"value": R.job_throughput(world, n, em) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": em,
                "call": "galphaComputeAll (DT + alpha, pinned host buffers), one call at a time"}
         e2e["pipelined"] = e2e_pipelined(G, params, n, a.steps, local, dist, world, schedule=sched)
 

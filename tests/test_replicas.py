@@ -1,0 +1,65 @@
+"""The N > 1 path of the bench on CPU: two ranks over gloo (127.0.0.1).
+Replicas only -- the ranks share no data; they meet to time the job (the
+slowest rank's time, every rank's units) -- and the reference arm runs on
+rank 0 alone."""
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+from galpha_b200 import replicas as R
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, times, out):
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    try:
+        m = R.max_over_ranks(times[rank], dist)
+        out.put((rank, m, R.job_throughput(world, 1000, m)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_job_time_is_the_slowest_rank_on_every_rank():
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    times = [2.5, 4.0]
+    ps = [ctx.Process(target=_rank, args=(r, 2, port, times, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [g[0] for g in got] == [0, 1]
+    for _, m, thr in got:
+        assert m == 4.0
+        assert thr == pytest.approx(2 * 1000 / 4.0e-3)
+
+
+def test_single_process_and_bad_time():
+    assert R.max_over_ranks(3.0) == 3.0
+    assert R.job_throughput(1, 500, 2.0) == pytest.approx(250000.0)
+    with pytest.raises(ValueError):
+        R.job_throughput(2, 1, 0.0)
+
+
+def test_reference_arm_does_no_work_off_rank_zero():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == ""
