@@ -744,10 +744,13 @@ __global__ void k_redo_collect(const unsigned char *redo, int ntiles, const int2
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles || !redo[t]) return;
     list[atomicAdd(&ct->nlist, 1)] = t;
-    int2 ch = chunk[t];
+    const int2 ch = chunk[t];
+    // the tile's triangles go to the free list in one reservation (one atomic
+    // per tile on the shared counter, not one per triangle)
+    const int base = ch.y > 0 ? atomicAdd(&ct->nfree, ch.y) : 0;
     for (int q = 0; q < ch.y; q++) {
         tv[ch.x + q] = make_int4(-1, -1, -1, 0);
-        freelist[atomicAdd(&ct->nfree, 1)] = ch.x + q;
+        freelist[base + q] = ch.x + q;
     }
 }
 
