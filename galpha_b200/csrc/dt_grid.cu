@@ -146,7 +146,7 @@ struct SetupSites {
         pos[v] = p;
         gpix[v] = make_short2((short)px, (short)py);
         vtri[v] = -1;
-        vround[v] = v < N ? 0 : 1;  // fake ring sites never move: decided before round 2
+        vround[v] = v < N ? 0 : 1;  // fake ring sites never move: decided before the first priority round (id 2)
         anchor[v] = -1;
         size_t pix = ((size_t)py << logT) + px;
         idmap[pix] = v;

@@ -427,7 +427,7 @@ struct ShiftCheckTris {
 };
 
 // Later iterations: only a triangle with a vertex dropped in the previous
-// iteration can change its verdict, so the fans of those vertices are checked.
+// iteration can change its outcome, so the fans of those vertices are checked.
 struct ShiftCheckFans {
     const int4 *tv, *tn;
     const int *vtri;
