@@ -679,23 +679,54 @@ struct SetEdgeBases {
 // Set of each value-sorted entry, by binary search of its id in the per-set
 // bases (triangles and edges are each grouped by set, bases non-decreasing;
 // the last set whose base is at most the id owns it) -- no gather by id.
+// A coarse table gives the owner of every kEntryBlock-th id, so the search
+// runs only over the sets that start inside the entry's block.
+constexpr int kEntryBlockBits = 10;
+
+__device__ __forceinline__ int set_owner(const int *b, int lo, int hi, int x)
+{
+    // the answer lies in [lo, hi): b[lo] <= x < b[hi]
+    while (hi - lo > 1) {
+        const int m = (lo + hi) >> 1;
+        if (b[m] <= x) lo = m;
+        else hi = m;
+    }
+    return lo;
+}
+
+// coarse[j]: owner of id j << kEntryBlockBits, for the triangle ids (j <
+// nbt) and then the edge ids
+struct EntryBlocks {
+    const int *tbase, *ebase;
+    int K, nbt;
+    int *coarse;
+    __device__ void operator()(long long jj) const
+    {
+        const int j = (int)jj;
+        const bool tri = j < nbt;
+        const int x = (tri ? j : j - nbt) << kEntryBlockBits;
+        coarse[j] = set_owner(tri ? tbase : ebase, 0, K, x);
+    }
+};
+
 struct EntrySet {
     const int *vals;
     const int *tbase, *ebase;
-    int K, nT;
+    const int *coarse;
+    int K, nT, nbt, nbe;
     unsigned *key;
     __device__ void operator()(long long i) const
     {
         const int v = vals[i];
-        const int *b = v < nT ? tbase : ebase;
-        const int x = v < nT ? v : v - nT;
-        int lo = 0, hi = K;  // the answer lies in [lo, hi): b[lo] <= x < b[hi]
-        while (hi - lo > 1) {
-            const int m = (lo + hi) >> 1;
-            if (b[m] <= x) lo = m;
-            else hi = m;
-        }
-        key[i] = (unsigned)lo;
+        const bool tri = v < nT;
+        const int *b = tri ? tbase : ebase;
+        const int x = tri ? v : v - nT;
+        const int j = x >> kEntryBlockBits;
+        const int *cb = tri ? coarse : coarse + nbt;
+        const int nb = tri ? nbt : nbe;
+        // the owner of the block's first id, up to the owner of the next block's
+        const int lo = cb[j], hi = j + 1 < nb ? min(K, cb[j + 1] + 1) : K;
+        key[i] = (unsigned)set_owner(b, lo, hi, x);
     }
 };
 
@@ -817,7 +848,11 @@ int stage_alpha(Ctx &c, AlphaSegs *segs)
         const int m = nIn - 1;
         unsigned *ka = (unsigned *)c.rank, *kb = (unsigned *)c.aux2;  // both free until the ranks
         launch_n(c, SetEdgeBases{c.e_off, segs->tbase, nT, nE, segs->ebase}, segs->K + 1);
-        launch_n(c, EntrySet{c.vals + 1, segs->tbase, segs->ebase, segs->K, nT, ka}, m);
+        // c.list is free here (the sliver list has been consumed)
+        const int nbt = (nT >> kEntryBlockBits) + 1, nbe = (nE >> kEntryBlockBits) + 1;
+        int *coarse = c.list;
+        launch_n(c, EntryBlocks{segs->tbase, segs->ebase, segs->K, nbt, coarse}, nbt + nbe);
+        launch_n(c, EntrySet{c.vals + 1, segs->tbase, segs->ebase, coarse, segs->K, nT, nbt, nbe, ka}, m);
         int bits = 0;
         while ((1ll << bits) < segs->K) bits++;
         r = radix_sort_set_kv(c, ka, kb, c.keys + 1, c.vals + 1, c.keys2 + 1, c.vals2 + 1, m, bits);
