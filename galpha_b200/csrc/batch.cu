@@ -292,7 +292,7 @@ struct AliveBySet {
         bool alive = v.x >= 0;
         key[t] = alive ? (unsigned)vsetall[v.x] : 0xffffffffu;
         val[t] = (int)t;
-        if (alive) atomicAdd(&ct->nlist, 1);
+        warp_reserve(&ct->nlist, alive ? 1 : 0);  // one atomic per warp on the shared count
     }
 };
 

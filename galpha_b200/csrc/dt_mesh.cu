@@ -658,10 +658,9 @@ struct CountState {
     Counters *ct;
     __device__ void operator()(long long i) const
     {
-        if (vstate[i] == s) {
-            int k = atomicAdd(&ct->nlist, 1);
-            if (list) list[k] = (int)i;
-        }
+        const bool hit = vstate[i] == s;
+        const int k = warp_reserve(&ct->nlist, hit ? 1 : 0);  // one atomic per warp
+        if (hit && list) list[k] = (int)i;
     }
 };
 
