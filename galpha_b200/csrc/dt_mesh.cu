@@ -291,13 +291,6 @@ struct Relinker {
     }
 };
 
-static int run_relink(Ctx &c, int round, int nrec)
-{
-    launch_n(c, Relinker{c.tn, c.fwd, c.epoch, c.rec, c.tv, c.vtri, round, c.ctr}, nrec);
-    GALPHA_CUDA(cudaGetLastError());
-    return GPUDT_OK;
-}
-
 // Every operation round gets a fresh id from the handle's counter (the
 // round-stamped arrays belong to the handle's arena, so ids must not repeat
 // on a handle, whichever thread drives it).
