@@ -1,4 +1,5 @@
-"""The N > 1 path of the bench on CPU: two ranks over gloo (127.0.0.1).
+"""The N > 1 path of the bench on CPU: two ranks over gloo (127.0.0.1); and the
+reference arm's line on a small problem.
 Replicas only -- the ranks share no data; they meet to time the job (the
 slowest rank's time, every rank's units) -- and the reference arm runs on
 rank 0 alone."""
@@ -63,3 +64,20 @@ def test_reference_arm_does_no_work_off_rank_zero():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
                         "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_reference_arm_line_on_a_small_problem():
+    """The reference arm's JSON line (oracle port, all host cores busy): the
+    fields the comparison reads, on a 20,000-point sample of the workload."""
+    import json
+
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                        "--warmup", "0", "--n", "20000"], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == (os.cpu_count() or 1)
+    assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["config"]["same_config"] is False and line["config"]["points"] == 20000
+    assert line["ms_per_step"] == pytest.approx(20000 / (line["value"] * 1e6) * 1e3)
