@@ -222,3 +222,25 @@ def test_gpu_cdt_lattice(engine, seed):
     rep = check_cdt(pts, dt.vtx, dt.tri, cons)
     assert rep == dict(links=0, ccw=0, missing=0, non_delaunay_free=0), rep
     assert len(dt.vtx) == len(O.cdt(pts, cons)[0])
+
+
+@pytest.mark.gpu
+def test_gpu_cdt_through_compute_all(engine):
+    """Constraints through galphaComputeAll (DT + alpha with host buffers):
+    the same triangles as galphaTriangulate, and the alpha result of that
+    constrained mesh."""
+    import galpha_b200 as G
+    from galpha_b200 import datasets as D
+    from alphacheck import compare_alpha
+
+    pts = D.uniform_points(5000, 621)
+    cons = without_crossings(pts, sheared_constraints(pts, 500, 3), chord_constraints(pts, 8))
+    p = G.GPUDTParams(pts, fboSize=1024, constraints=cons)
+    ref = engine.triangulate(p)
+    dt, al = engine.compute_all(p)
+    assert canon_set(dt.vtx) == canon_set(ref.vtx) == canon_set(O.cdt(pts, cons)[0])
+    ok, rep = compare_alpha(pts, dt.vtx, dt.tri, al, 4)
+    assert ok, rep
+    # the next call without constraints is the plain Delaunay triangulation again
+    dt2, _ = engine.compute_all(G.GPUDTParams(pts, fboSize=1024))
+    assert canon_set(dt2.vtx) == canon_set(O.dt(pts)[0])
