@@ -147,3 +147,18 @@ def test_batch_density_keeps_results(engine, density):
     finally:
         beng.close()
     _compare(engine, sets, res)
+
+
+@pytest.mark.parametrize("sched", [(1, 1, 1, 0, 1), (8, 8, 64, 1 << 20, 1 << 22)])
+def test_batch_schedule_keeps_results(engine, sched):
+    """The loop schedule (rounds per counter read, flip-tail hand-over)
+    changes when the host reads counters, not the result of a batch."""
+    sets = _mixed_sets(5)[:12]
+    beng = G.Engine()
+    try:
+        beng.set_schedule(*sched)
+        beng.run_batch(sets)
+        res = beng.batch_results()
+    finally:
+        beng.close()
+    _compare(engine, sets, res)
