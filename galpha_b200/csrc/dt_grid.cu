@@ -312,31 +312,72 @@ struct IslandApply {
 // ------------------------------------------------- degenerate input check
 // An input with fewer than 3 distinct points, or with all points collinear,
 // has no triangle; the pipeline is skipped for it.
-struct FirstDistinct {
-    const double *xy;
-    int *out;
-    __device__ void operator()(long long i) const
-    {
-        // one atomic per point below the smallest index found so far (a plain
-        // read filters the rest; usually point 1 already differs)
-        if ((xy[2 * i] != xy[0] || xy[2 * i + 1] != xy[1]) && (int)i < *(volatile int *)out) atomicMin(out, (int)i);
-    }
-};
+constexpr int kPrecheckPrefix = 1024;
 
-struct CountOffLine {
-    const double *xy;
-    const int *b;
-    long long n;
-    Counters *ct;
-    __device__ void operator()(long long i) const
-    {
-        int j = *b;
-        if (j >= n) return;  // every point equals point 0: nothing is off the line
+// The first kPrecheckPrefix points in one block, with no shared-address
+// traffic: the smallest index of a point distinct from point 0 into *first
+// (left alone when there is none) and ct->changed = 1 when one of them is
+// off the line through point 0 and that point. This decides general input;
+// the grid-wide scans below then return at once.
+__global__ void __launch_bounds__(kPrecheckPrefix) k_precheck_prefix(const double *xy, int n, int *first, Counters *ct)
+{
+    __shared__ int wmin[kPrecheckPrefix / 32];
+    __shared__ int jsh;
+    const int i = threadIdx.x, lane = i & 31, w = i >> 5;
+    const bool in = i < n;
+    const double x0 = xy[0], y0 = xy[1];
+    double xi = x0, yi = y0;
+    if (in) {
+        xi = xy[2 * i];
+        yi = xy[2 * i + 1];
+    }
+    const int cand = __reduce_min_sync(0xffffffffu, (xi != x0 || yi != y0) ? i : 0x7fffffff);
+    if (lane == 0) wmin[w] = cand;
+    __syncthreads();
+    if (w == 0) {
+        const int v = __reduce_min_sync(0xffffffffu, lane < kPrecheckPrefix / 32 ? wmin[lane] : 0x7fffffff);
+        if (lane == 0) jsh = v;
+    }
+    __syncthreads();
+    const int j = jsh;
+    if (j == 0x7fffffff) return;  // the prefix is all point 0: the grid scans decide
+    if (i == 0) *first = j;
+    int s = 0;
+    if (in) {
+        const double xj = xy[2 * j], yj = xy[2 * j + 1];
+        s = orient2d_filter(x0, y0, xj, yj, xi, yi);
+        if (s == 2) s = orient2d_exact(x0, y0, xj, yj, xi, yi);
+    }
+    if (__syncthreads_or(s != 0) && i == 0) ct->changed = 1;
+}
+
+// The smallest index of a point distinct from point 0 into *first, over all
+// points, when the prefix found none (*first still above every index). One
+// atomic per point below the smallest index found so far (a plain read
+// filters the rest).
+__global__ void __launch_bounds__(256) k_first_distinct(const double *xy, long long n, int *first)
+{
+    if (*first < n) return;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if ((xy[2 * i] != xy[0] || xy[2 * i + 1] != xy[1]) && (int)i < *(volatile int *)first) atomicMin(first, (int)i);
+}
+
+// ct->changed = 1 when some point is off the line through point 0 and point
+// *first, over all points, when the prefix found none (*first >= n: every
+// point equals point 0 and nothing is off the line).
+__global__ void __launch_bounds__(256) k_count_off_line(const double *xy, const int *first, long long n, Counters *ct)
+{
+    if (ct->changed) return;
+    const int j = *first;
+    if (j >= n) return;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         int s = orient2d_filter(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
         if (s == 2) s = orient2d_exact(xy[0], xy[1], xy[2 * j], xy[2 * j + 1], xy[2 * i], xy[2 * i + 1]);
-        if (s != 0 && *(volatile int *)&ct->changed == 0) ct->changed = 1;  // any one point off the line
+        if (s != 0 && *(volatile int *)&ct->changed == 0) ct->changed = 1;
     }
-};
+}
 
 // Returns 1 when the input has at least one triangle.
 int has_triangles(Ctx &c, const double *d_xy, int n)
@@ -345,10 +386,16 @@ int has_triangles(Ctx &c, const double *d_xy, int n)
     int *first = c.aux;
     GALPHA_CUDA(cudaMemsetAsync(first, 0x7f, sizeof(int), c.stream));
     GALPHA_CUDA(cudaMemsetAsync(&c.ctr->changed, 0, sizeof(int), c.stream));
-    launch_n(c, FirstDistinct{d_xy, first}, n);
+    k_precheck_prefix<<<1, kPrecheckPrefix, 0, c.stream>>>(d_xy, n, first, c.ctr);
+    count_launch();
+    long long blocks = ((long long)n + 255) / 256;
+    if (blocks > (long long)c.sm_count * 8) blocks = (long long)c.sm_count * 8;
+    k_first_distinct<<<(unsigned)blocks, 256, 0, c.stream>>>(d_xy, n, first);
+    count_launch();
     // the line through point 0 and the first point distinct from it (none:
     // `first` stays above every index and no point counts), one host read
-    launch_n(c, CountOffLine{d_xy, first, n, c.ctr}, n);
+    k_count_off_line<<<(unsigned)blocks, 256, 0, c.stream>>>(d_xy, first, n, c.ctr);
+    count_launch();
     int r = read_counters(c);
     if (r) return r;
     return c.hctr->changed > 0 ? 1 : 0;

@@ -109,6 +109,24 @@ def test_tiny_and_degenerate(engine, pts, ntri):
         assert_parity(pts, dt, True)
 
 
+def test_precheck_past_first_pass(engine):
+    # the input precheck stops once a distinct point (then an off-line point)
+    # is found; these sets put the answer, or no answer, beyond the first
+    # pass of its grid (148 SMs x 8 blocks x 256 threads = 303,104 points)
+    n = 400000
+    t = np.arange(n, dtype=np.float64) / (1 << 19)
+    line = np.stack([t, 0.25 + 0.5 * t], 1)               # collinear, exactly representable
+    assert run(engine, line, 2048).nTris == 0
+    dup = np.full((n, 2), 0.375)
+    dup[-1] = (0.625, 0.125)                                # two distinct points, the second last
+    assert run(engine, dup, 2048).nTris == 0
+    rng = np.random.default_rng(21)
+    late = np.concatenate([np.full((320000, 2), 0.5), rng.random((2000, 2))])
+    dt = run(engine, late, 2048)
+    assert_parity(late, dt, True)
+    assert dt.status.nDuplicates == 320000 - 1
+
+
 def test_deterministic_and_reusable(engine):
     rng = np.random.default_rng(9)
     a = rng.random((30000, 2))
