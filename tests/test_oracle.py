@@ -71,6 +71,26 @@ def test_dt_degenerate_inputs():
     assert len(v) == 0
 
 
+def test_dt_long_degenerate_runs():
+    # exactly collinear (dyadic coordinates), and two distinct points with
+    # the second one last: no triangle either way
+    t = np.arange(5000, dtype=np.float64) / 8192
+    assert len(O.dt(np.stack([t, 0.25 + 0.5 * t], 1))[0]) == 0
+    dup = np.full((5000, 2), 0.375)
+    dup[-1] = (0.625, 0.125)
+    assert len(O.dt(dup)[0]) == 0
+    # a long run of copies of point 0 ahead of the other points: the mesh is
+    # that of the distinct points, with point 0 standing for its copies
+    rng = np.random.default_rng(21)
+    rest = rng.random((500, 2))
+    late = np.concatenate([np.full((4000, 2), 0.5), rest])
+    v, nb, kept = O.dt(late)
+    assert kept == 501
+    v0, _, _ = O.dt(np.concatenate([[[0.5, 0.5]], rest]))
+    remap = np.concatenate([[0], np.arange(4000, 4500)])  # distinct set index -> input index
+    assert canon_set(v) == canon_set(remap[v0])
+
+
 def test_dt_rejects_nan():
     with pytest.raises(RuntimeError):
         O.dt(np.array([[0, 0], [1, np.nan], [0, 1.0]]))
