@@ -138,18 +138,44 @@ def cpu_baseline(sample_n=1 << 22):
             "sample": "one c2 problem: %d uniform points, oracle DT + alpha spectrum, 1 thread, %.1f s" % (n, dt)}
 
 
+def reference_processes(n, avail_bytes=None, cores=None):
+    """Worker processes for the reference arm: one per core this process may
+    run on, capped so that their problems fit in half the available host
+    memory (one c2 problem of 4,194,304 points peaks at about 1.24 GB
+    resident in a worker: 1.5 GB is budgeted per 4M points, 0.25 GB at
+    least)."""
+    if cores is None:
+        try:
+            cores = len(os.sched_getaffinity(0))
+        except (AttributeError, OSError):
+            cores = os.cpu_count() or 1
+    if avail_bytes is None:
+        try:
+            import psutil
+
+            avail_bytes = psutil.virtual_memory().available
+        except Exception:  # no reading: the core count alone
+            avail_bytes = None
+    procs = max(1, cores)
+    if avail_bytes:
+        per_proc = max(0.25e9, 1.5e9 * n / (1 << 22))
+        procs = min(procs, max(1, int(0.5 * avail_bytes // per_proc)))
+    return procs
+
+
 def reference_arm(a):
     """The reference's CPU path on the host cores: every step is one full c2
     problem (4,194,304 uniform points, DT + alpha spectrum) through the CPU
-    oracle port, on one process per host core.  K + P problems go to P
+    oracle port, on one process per host core (fewer where host memory is
+    short: `reference_processes`).  K + P problems go to P
     workers; the first K to finish ran while every worker was busy (the
     queue empties only at the K-th completion), so their times are times under
     full load, and value = P problems' points / their mean time: the
     throughput of all host cores, with no partly idle last wave."""
     import multiprocessing as mp
 
-    procs = max(1, os.cpu_count() or 1)
     per = a.n if a.n else (1 << 22)
+    procs = reference_processes(per)
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
         if a.warmup:

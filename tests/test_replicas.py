@@ -77,7 +77,24 @@ def test_reference_arm_line_on_a_small_problem():
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == (os.cpu_count() or 1)
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == bench.reference_processes(20000)
     assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["config"]["same_config"] is False and line["config"]["points"] == 20000
     assert line["ms_per_step"] == pytest.approx(20000 / (line["value"] * 1e6) * 1e3)
+
+
+def test_reference_processes_fit_host_memory():
+    """One worker per usable core, as many as half the available memory holds
+    at 1.5 GB per 4,194,304-point problem."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    n = 1 << 22
+    assert bench.reference_processes(n, avail_bytes=62e9, cores=16) == 16
+    assert bench.reference_processes(n, avail_bytes=64e9, cores=224) == 21
+    assert bench.reference_processes(n, avail_bytes=1e9, cores=16) == 1
+    assert bench.reference_processes(20000, avail_bytes=8e9, cores=64) == 16  # 0.25 GB floor per worker
+    assert bench.reference_processes(n, avail_bytes=None, cores=7) in range(1, 8)
